@@ -1,0 +1,538 @@
+// hpccg_cg.cu -- FP64 conjugate gradient as one CUDA graph (MPI/src/numerics.F90:41-162).
+//
+// Schedule (one rank; exchange_externals is a no-op, SparseMatrix.F90:643-645):
+//   prepare   k_cg_residual   r = b - A x, rtrans = r.r, normr, condition
+//   while (condition)          -- device-side graph while node --
+//     K_P  k_cg_update_p       k==1: p = r ; else x += alpha_{k-1} p, p = r + beta p
+//     K_A  k_cg_spmv_dot       Ap = A p, pAp = p.Ap, alpha = rtrans/pAp
+//     K_B  k_cg_update_r       r = r - alpha Ap, rr = r.r, then the top of the next
+//                              iteration's scalar work and the condition
+//   tail      k_cg_finish      x += alpha p for the last iteration
+// The x update of iteration k is deferred into K_P of iteration k+1 (same
+// operands, same rounding), which saves one pass over p per iteration.
+// Scalars never leave the device; the host reads niters/normr/history once.
+#include <stdlib.h>
+
+#include <algorithm>
+
+#include "hpccg_rows.cuh"
+
+namespace hpccg {
+
+struct CgArgs {
+  double *x, *r, *p, *Ap;
+  const double *b;
+  CgState *st;
+  double *hist;
+  int hist_cap;
+  int n;
+  Reduction red;
+  cudaGraphConditionalHandle cond;
+  int use_cond;
+};
+
+__device__ __forceinline__ void set_condition(const CgArgs &g, int v) {
+  g.st->cont = v;
+  if (g.use_cond) cudaGraphSetConditional(g.cond, (unsigned)v);
+}
+
+// Prepare phase, MPI/src/numerics.F90:91-104 (vcopy x->p; spmv; waxpby; ddot1).
+template <class S>
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_cg_residual(SpmvArgs a, CgArgs g) {
+  __shared__ double smem[32];
+  EpiResidual epi{g.b, g.r};
+  const double part = S::rows(a, g.x, epi);
+  const double tot = block_sum<kBlock>(part, smem);
+  if (arrive_last(g.red, tot)) {
+    const double rr = finish_sum<kBlock>(g.red, smem);
+    if (threadIdx.x == 0) {
+      CgState &st = *g.st;
+      st.rtrans = rr;
+      st.oldrtrans = 0.0;
+      st.normr = sqrt(rr);
+      st.k = 1;
+      st.niters = 0;
+      st.status = HPCCG_OK;
+      st.x_pending = 0;
+      if (g.hist_cap > 0) g.hist[0] = st.normr;
+      // Top of iteration 1 (:109-126): stop test, then normr = sqrt(rtrans).
+      const int cont = (st.max_iter >= 1) && !(st.normr < st.tolerance);
+      if (cont && g.hist_cap > 1) g.hist[1] = st.normr;
+      set_condition(g, cont);
+    }
+  }
+}
+
+// K_P: MPI/src/numerics.F90:114-120 (vcopy / wxbw) plus the deferred x update
+// of :140 (wwpby x += alpha p) from the previous iteration.
+__global__ void __launch_bounds__(kBlock) k_cg_update_p(CgArgs g) {
+  const CgState *st = g.st;
+  if (st->status) return;
+  const int k = st->k;
+  const double alpha = st->alpha, beta = st->beta;
+  const int xp = st->x_pending;
+  const int n = g.n;
+  const int stride = gridDim.x * blockDim.x;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n2 = n >> 1;
+  double2 *p2 = reinterpret_cast<double2 *>(g.p);
+  double2 *x2 = reinterpret_cast<double2 *>(g.x);
+  const double2 *r2 = reinterpret_cast<const double2 *>(g.r);
+  if (k == 1) {
+    for (int i = tid; i < n2; i += stride) p2[i] = __ldcs(r2 + i);
+    if (tid == 0 && (n & 1)) g.p[n - 1] = g.r[n - 1];
+    return;
+  }
+  for (int i = tid; i < n2; i += stride) {
+    const double2 pi = p2[i], ri = __ldcs(r2 + i);
+    if (xp) {
+      double2 xi = __ldcs(x2 + i);
+      xi.x = __dadd_rn(xi.x, __dmul_rn(alpha, pi.x));
+      xi.y = __dadd_rn(xi.y, __dmul_rn(alpha, pi.y));
+      __stcs(x2 + i, xi);
+    }
+    double2 po;
+    po.x = __dadd_rn(ri.x, __dmul_rn(beta, pi.x));
+    po.y = __dadd_rn(ri.y, __dmul_rn(beta, pi.y));
+    p2[i] = po;
+  }
+  if (tid == 0 && (n & 1)) {
+    const int i = n - 1;
+    const double pi = g.p[i];
+    if (xp) g.x[i] = __dadd_rn(g.x[i], __dmul_rn(alpha, pi));
+    g.p[i] = __dadd_rn(g.r[i], __dmul_rn(beta, pi));
+  }
+}
+
+// K_A: MPI/src/numerics.F90:133-138 (spmv; ddot; alpha = rtrans/alpha).
+template <class S>
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_cg_spmv_dot(SpmvArgs a, CgArgs g) {
+  __shared__ double smem[32];
+  if (g.st->status) return;
+  EpiDot epi{g.p, g.Ap};
+  const double part = S::rows(a, g.p, epi);
+  const double tot = block_sum<kBlock>(part, smem);
+  if (arrive_last(g.red, tot)) {
+    const double pAp = finish_sum<kBlock>(g.red, smem);
+    if (threadIdx.x == 0) {
+      CgState &st = *g.st;
+      st.pAp = pAp;
+      st.x_pending = 0;  // K_P of this iteration has applied it
+      const double alpha = st.rtrans / pAp;
+      if (!isfinite(alpha)) st.status = HPCCG_ERR_BREAKDOWN;
+      else st.alpha = alpha;
+    }
+  }
+}
+
+// K_B: MPI/src/numerics.F90:139 (wwpby r -= alpha Ap) fused with the ddot1
+// of the next iteration's :118, followed by the next iteration's stop test
+// (:109), beta (:117-119) and normr (:123).
+__global__ void __launch_bounds__(kBlock) k_cg_update_r(CgArgs g) {
+  __shared__ double smem[32];
+  if (g.st->status) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_condition(g, 0);
+    return;
+  }
+  const double nalpha = -g.st->alpha;
+  const int n = g.n, n2 = n >> 1;
+  const int stride = gridDim.x * blockDim.x;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  double2 *r2 = reinterpret_cast<double2 *>(g.r);
+  const double2 *a2 = reinterpret_cast<const double2 *>(g.Ap);
+  double part = 0.0;
+  for (int i = tid; i < n2; i += stride) {
+    double2 ri = r2[i];
+    const double2 ai = __ldcs(a2 + i);
+    ri.x = __dadd_rn(ri.x, __dmul_rn(nalpha, ai.x));
+    ri.y = __dadd_rn(ri.y, __dmul_rn(nalpha, ai.y));
+    r2[i] = ri;
+    part = __dadd_rn(part, __dmul_rn(ri.x, ri.x));
+    part = __dadd_rn(part, __dmul_rn(ri.y, ri.y));
+  }
+  if (tid == 0 && (n & 1)) {
+    const double ri = __dadd_rn(g.r[n - 1], __dmul_rn(nalpha, g.Ap[n - 1]));
+    g.r[n - 1] = ri;
+    part = __dadd_rn(part, __dmul_rn(ri, ri));
+  }
+  const double tot = block_sum<kBlock>(part, smem);
+  if (arrive_last(g.red, tot)) {
+    const double rr = finish_sum<kBlock>(g.red, smem);
+    if (threadIdx.x == 0) {
+      CgState &st = *g.st;
+      st.rr_last = rr;
+      st.niters = st.k;
+      st.x_pending = 1;
+      const int next = st.k + 1;
+      const int cont = (next <= st.max_iter) && !(st.normr < st.tolerance);
+      if (cont) {
+        st.oldrtrans = st.rtrans;
+        st.rtrans = rr;
+        st.beta = st.rtrans / st.oldrtrans;
+        st.normr = sqrt(st.rtrans);
+        st.k = next;
+        if (next < g.hist_cap) g.hist[next] = st.normr;
+      }
+      set_condition(g, cont);
+    }
+  }
+}
+
+// Tail: the x update (:140) of the last executed iteration.
+__global__ void __launch_bounds__(kBlock) k_cg_finish(CgArgs g) {
+  const CgState *st = g.st;
+  if (st->status || !st->x_pending) return;
+  const double alpha = st->alpha;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x)
+    g.x[i] = __dadd_rn(g.x[i], __dmul_rn(alpha, g.p[i]));
+}
+
+// Plain y = A x (op-level drop-in and timing).
+template <class S>
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_spmv(SpmvArgs a, const double *x, double *y) {
+  EpiStore epi{y};
+  S::rows(a, x, epi);
+}
+
+static CgArgs cg_args(hpccg_ctx *c, cudaGraphConditionalHandle h, int use_cond) {
+  CgArgs g;
+  g.x = c->d_x;
+  g.r = c->d_r;
+  g.p = c->d_p;
+  g.Ap = c->d_Ap;
+  g.b = c->d_b;
+  g.st = c->d_state;
+  g.hist = c->d_hist;
+  g.hist_cap = c->hist_cap;
+  g.n = c->nrow;
+  g.red = reduction_of(c);
+  g.cond = h;
+  g.use_cond = use_cond;
+  return g;
+}
+
+static int launch_prepare(hpccg_ctx *c, const SpmvArgs &a, const CgArgs &g, cudaStream_t s) {
+  return dispatch_strategy(a, [&](auto strat) {
+    using St = decltype(strat);
+    k_cg_residual<St><<<c->grid, kBlock, 0, s>>>(a, g);
+    return (int)cudaGetLastError();
+  });
+}
+
+static int launch_body(hpccg_ctx *c, const SpmvArgs &a, const CgArgs &g, cudaStream_t s) {
+  k_cg_update_p<<<c->grid, kBlock, 0, s>>>(g);
+  int rc = dispatch_strategy(a, [&](auto strat) {
+    using St = decltype(strat);
+    k_cg_spmv_dot<St><<<c->grid, kBlock, 0, s>>>(a, g);
+    return (int)cudaGetLastError();
+  });
+  if (rc) return rc;
+  k_cg_update_r<<<c->grid, kBlock, 0, s>>>(g);
+  return (int)cudaGetLastError();
+}
+
+int launch_spmv(hpccg_ctx *c, const double *x, double *y, cudaStream_t s) {
+  const SpmvArgs a = spmv_args(c);
+  return dispatch_strategy(a, [&](auto strat) {
+    using St = decltype(strat);
+    k_spmv<St><<<c->grid, kBlock, 0, s>>>(a, x, y);
+    return (int)cudaGetLastError();
+  });
+}
+
+static void drop_graph(hpccg_ctx *c) {
+  if (c->cg_exec) cudaGraphExecDestroy(c->cg_exec);
+  if (c->cg_graph) cudaGraphDestroy(c->cg_graph);
+  c->cg_exec = nullptr;
+  c->cg_graph = nullptr;
+}
+
+// Captures prepare -> while(K_P, K_A, K_B) -> tail into one executable graph.
+static int build_cg_graph(hpccg_ctx *c) {
+  drop_graph(c);
+  const SpmvArgs a = spmv_args(c);
+  cudaStream_t s = c->stream;
+  cudaStream_t bs = nullptr;
+  cudaGraph_t g = nullptr;
+  cudaGraphNode_t cnode = nullptr;
+  cudaGraphConditionalHandle h = 0;
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  HPCCG_CUDA(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
+  int rc = HPCCG_OK;
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &ndeps);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
+  CgArgs ga = cg_args(c, h, 1);
+  if (e == cudaSuccess) e = (cudaError_t)launch_prepare(c, a, ga, s);
+  if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &ndeps);
+  cudaGraphNodeParams cp = {};
+  if (e == cudaSuccess) {
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    e = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp);
+  }
+  if (e == cudaSuccess) {
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      const cudaError_t e1 = (cudaError_t)launch_body(c, a, ga, bs);
+      const cudaError_t e2 = cudaStreamEndCapture(bs, &body);
+      e = e1 != cudaSuccess ? e1 : e2;
+    }
+  }
+  if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies);
+  if (e == cudaSuccess) {
+    k_cg_finish<<<c->grid, kBlock, 0, s>>>(ga);
+    e = cudaGetLastError();
+  }
+  cudaGraph_t out = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(s, &out);
+  if (e == cudaSuccess) e = ee;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&c->cg_exec, out, 0);
+  if (e != cudaSuccess) {
+    rc = set_cuda_error(e, "build CG graph", __FILE__, __LINE__);
+    if (out) cudaGraphDestroy(out);
+    cudaGetLastError();
+  } else {
+    c->cg_graph = out;
+    c->cg_graph_kind = a.kind;
+    c->cg_graph_param = a.param;
+    c->cg_graph_hist_cap = c->hist_cap;
+  }
+  cudaStreamDestroy(bs);
+  return rc;
+}
+
+// Host-driven loop with the same kernels (HPCCG_EAGER=1): for debugging and
+// for drivers without graph support.
+static int run_cg_eager(hpccg_ctx *c) {
+  const SpmvArgs a = spmv_args(c);
+  const CgArgs g = cg_args(c, 0, 0);
+  int rc = launch_prepare(c, a, g, c->stream);
+  if (rc) return set_cuda_error((cudaError_t)rc, "prepare", __FILE__, __LINE__);
+  for (;;) {
+    int cont = 0;
+    HPCCG_CUDA(cudaMemcpyAsync(&cont, &c->d_state->cont, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+    if (!cont) break;
+    rc = launch_body(c, a, g, c->stream);
+    if (rc) return set_cuda_error((cudaError_t)rc, "iteration", __FILE__, __LINE__);
+  }
+  k_cg_finish<<<c->grid, kBlock, 0, c->stream>>>(g);
+  HPCCG_CUDA(cudaGetLastError());
+  return HPCCG_OK;
+}
+
+}  // namespace hpccg
+
+using namespace hpccg;
+
+static int cg_common(hpccg_ctx *c, int32_t max_iter, double tolerance, int32_t *niters,
+                     double *normr, double *resid_hist) {
+  int rc = ensure_workspace(c, std::max<int32_t>(max_iter + 1, 2));
+  if (rc) return rc;
+  if ((rc = autotune_spmv(c))) return rc;
+  CgState h0 = {};
+  h0.max_iter = max_iter;
+  h0.tolerance = tolerance;
+  HPCCG_CUDA(cudaMemcpyAsync(c->d_state, &h0, sizeof(CgState), cudaMemcpyHostToDevice, c->stream));
+  const bool eager = getenv("HPCCG_EAGER") && atoi(getenv("HPCCG_EAGER")) != 0;
+  if (eager) {
+    HPCCG_CUDA(cudaEventRecord(c->solve0, c->stream));
+    if ((rc = run_cg_eager(c))) return rc;
+    HPCCG_CUDA(cudaEventRecord(c->solve1, c->stream));
+  } else {
+    const SpmvArgs a = spmv_args(c);
+    if (!c->cg_exec || c->cg_graph_kind != a.kind || c->cg_graph_param != a.param ||
+        c->cg_graph_hist_cap != c->hist_cap)
+      if ((rc = build_cg_graph(c))) return rc;
+    HPCCG_CUDA(cudaEventRecord(c->solve0, c->stream));
+    HPCCG_CUDA(cudaGraphLaunch(c->cg_exec, c->stream));
+    HPCCG_CUDA(cudaEventRecord(c->solve1, c->stream));
+  }
+  CgState hs;
+  HPCCG_CUDA(cudaMemcpyAsync(&hs, c->d_state, sizeof(CgState), cudaMemcpyDeviceToHost, c->stream));
+  HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+  HPCCG_CUDA(cudaEventElapsedTime(&c->last_solve_ms, c->solve0, c->solve1));
+  if (niters) *niters = hs.niters;
+  if (normr) *normr = hs.normr;
+  if (resid_hist) {
+    HPCCG_CUDA(cudaMemcpyAsync(resid_hist, c->d_hist, sizeof(double) * ((size_t)hs.niters + 1),
+                               cudaMemcpyDeviceToHost, c->stream));
+    HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return hs.status;
+}
+
+extern "C" int hpccg_gpu_cg(hpccg_ctx *c, const double *b, double *x, int32_t max_iter,
+                            double tolerance, int32_t *niters, double *normr, double *resid_hist) {
+  if (!c || !b || !x || max_iter < 0) return HPCCG_ERR_INVALID_ARG;
+  const size_t bytes = sizeof(double) * (size_t)c->nrow;
+  HPCCG_CUDA(cudaMemcpyAsync(c->d_b, b, bytes, cudaMemcpyHostToDevice, c->stream));
+  HPCCG_CUDA(cudaMemcpyAsync(c->d_x, x, bytes, cudaMemcpyHostToDevice, c->stream));
+  const int rc = cg_common(c, max_iter, tolerance, niters, normr, resid_hist);
+  if (rc != HPCCG_OK && rc != HPCCG_ERR_BREAKDOWN) return rc;
+  HPCCG_CUDA(cudaMemcpyAsync(x, c->d_x, bytes, cudaMemcpyDeviceToHost, c->stream));
+  HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
+extern "C" int hpccg_gpu_cg_device(hpccg_ctx *c, const double *d_b, double *d_x, int32_t max_iter,
+                                   double tolerance, int32_t *niters, double *normr,
+                                   double *resid_hist) {
+  if (!c || !d_b || !d_x || max_iter < 0) return HPCCG_ERR_INVALID_ARG;
+  const size_t bytes = sizeof(double) * (size_t)c->nrow;
+  HPCCG_CUDA(cudaMemcpyAsync(c->d_b, d_b, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  HPCCG_CUDA(cudaMemcpyAsync(c->d_x, d_x, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  const int rc = cg_common(c, max_iter, tolerance, niters, normr, resid_hist);
+  if (rc != HPCCG_OK && rc != HPCCG_ERR_BREAKDOWN) return rc;
+  HPCCG_CUDA(cudaMemcpyAsync(d_x, c->d_x, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
+// ---- SpMV selection, op-level SpMV and timing ------------------------------
+
+extern "C" int hpccg_gpu_set_spmv(hpccg_ctx *c, int32_t kind, int32_t param) {
+  if (!c) return HPCCG_ERR_INVALID_ARG;
+  if (kind < HPCCG_SPMV_AUTO || kind > HPCCG_SPMV_CSR_VECTOR) return HPCCG_ERR_INVALID_ARG;
+  if ((kind == HPCCG_SPMV_ELL || kind == HPCCG_SPMV_ELL2) && !c->d_ell_col) return HPCCG_ERR_UNSUPPORTED;
+  if (kind == HPCCG_SPMV_ELL2 && c->ell_width != 27) return HPCCG_ERR_UNSUPPORTED;
+  if (kind == HPCCG_SPMV_CSR_VECTOR && param != 4 && param != 8 && param != 16 && param != 32)
+    return HPCCG_ERR_INVALID_ARG;
+  if ((kind == HPCCG_SPMV_ELL || kind == HPCCG_SPMV_ELL2) && param != 0 && param != 2 && param != 3 &&
+      param != 4 && param != 8)
+    return HPCCG_ERR_INVALID_ARG;
+  c->spmv_kind = kind;
+  c->spmv_param = (kind != HPCCG_SPMV_CSR_VECTOR && param == 0) ? 4 : param;
+  c->spmv_tuned = kind != HPCCG_SPMV_AUTO;
+  return HPCCG_OK;
+}
+
+extern "C" int hpccg_gpu_get_spmv(const hpccg_ctx *c, int32_t *kind, int32_t *param) {
+  if (!c) return HPCCG_ERR_INVALID_ARG;
+  const SpmvArgs a = spmv_args(c);
+  if (kind) *kind = a.kind;
+  if (param) *param = a.param;
+  return HPCCG_OK;
+}
+
+static int time_current(hpccg_ctx *c, const double *x, double *y, int reps, float *ms) {
+  int rc = launch_spmv(c, x, y, c->stream);  // warm-up
+  if (rc) return set_cuda_error((cudaError_t)rc, "spmv", __FILE__, __LINE__);
+  HPCCG_CUDA(cudaEventRecord(c->ev0, c->stream));
+  for (int i = 0; i < reps; ++i) launch_spmv(c, x, y, c->stream);
+  HPCCG_CUDA(cudaEventRecord(c->ev1, c->stream));
+  HPCCG_CUDA(cudaEventSynchronize(c->ev1));
+  float t = 0.f;
+  HPCCG_CUDA(cudaEventElapsedTime(&t, c->ev0, c->ev1));
+  *ms = t / (float)reps;
+  return HPCCG_OK;
+}
+
+namespace hpccg {
+// AUTO: time the bit-exact ELL strategies on this matrix and keep the faster.
+int autotune_spmv(hpccg_ctx *c) {
+  if (c->spmv_tuned) return HPCCG_OK;
+  c->spmv_tuned = true;
+  if (!c->d_ell_col || c->ell_width != 27) {
+    c->spmv_kind = c->d_ell_col ? HPCCG_SPMV_ELL : HPCCG_SPMV_CSR_VECTOR;
+    c->spmv_param = c->d_ell_col ? 4 : 32;
+    return HPCCG_OK;
+  }
+  // Candidates share the thread-per-row mapping, so the choice never changes
+  // a single bit of the CG results; only the register/occupancy trade-off.
+  float best = 1e30f;
+  int best_param = 4;
+  const int reps = c->nrow > (1 << 20) ? 5 : 20;
+  for (int minb : kEllMinBlocks) {
+    c->spmv_kind = HPCCG_SPMV_ELL;
+    c->spmv_param = minb;
+    float ms = 0.f;
+    const int rc = time_current(c, c->d_p, c->d_Ap, reps, &ms);
+    if (rc) return rc;
+    if (ms < best) {
+      best = ms;
+      best_param = minb;
+    }
+  }
+  c->spmv_kind = HPCCG_SPMV_ELL;
+  c->spmv_param = best_param;
+  return HPCCG_OK;
+}
+}  // namespace hpccg
+
+extern "C" int hpccg_gpu_spmv(hpccg_ctx *c, const double *d_x, double *d_y) {
+  if (!c || !d_x || !d_y || d_x == d_y) return HPCCG_ERR_INVALID_ARG;
+  int rc = autotune_spmv(c);
+  if (rc) return rc;
+  rc = launch_spmv(c, d_x, d_y, c->stream);
+  if (rc) return set_cuda_error((cudaError_t)rc, "spmv", __FILE__, __LINE__);
+  HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+  return HPCCG_OK;
+}
+
+extern "C" int hpccg_gpu_time_spmv(hpccg_ctx *c, const double *d_x, double *d_y, int32_t reps,
+                                   float *ms_per_call) {
+  if (!c || !d_x || !d_y || reps < 1 || !ms_per_call) return HPCCG_ERR_INVALID_ARG;
+  int rc = autotune_spmv(c);
+  if (rc) return rc;
+  return time_current(c, d_x, d_y, reps, ms_per_call);
+}
+
+extern "C" int hpccg_gpu_last_solve_ms(const hpccg_ctx *c, float *ms) {
+  if (!c || !ms) return HPCCG_ERR_INVALID_ARG;
+  *ms = c->last_solve_ms;
+  return HPCCG_OK;
+}
+
+extern "C" int hpccg_gpu_time_cg_kernels(hpccg_ctx *c, int32_t reps, float *ms) {
+  if (!c || reps < 1 || !ms) return HPCCG_ERR_INVALID_ARG;
+  int rc = ensure_workspace(c, 2);
+  if (rc) return rc;
+  if ((rc = autotune_spmv(c))) return rc;
+  const size_t bytes = sizeof(double) * (size_t)c->nrow;
+  // Benign operands: p = r = x = 0 keeps every scalar finite.
+  HPCCG_CUDA(cudaMemsetAsync(c->d_p, 0, bytes, c->stream));
+  HPCCG_CUDA(cudaMemsetAsync(c->d_r, 0, bytes, c->stream));
+  HPCCG_CUDA(cudaMemsetAsync(c->d_x, 0, bytes, c->stream));
+  CgState h0 = {};
+  h0.k = 2;
+  h0.max_iter = 1 << 30;
+  h0.rtrans = 1.0;
+  h0.alpha = 0.5;
+  h0.beta = 0.5;
+  h0.x_pending = 1;
+  HPCCG_CUDA(cudaMemcpyAsync(c->d_state, &h0, sizeof(CgState), cudaMemcpyHostToDevice, c->stream));
+  const SpmvArgs a = spmv_args(c);
+  const CgArgs g = cg_args(c, 0, 0);
+  for (int which = 0; which < 3; ++which) {
+    for (int rep = -1; rep < reps; ++rep) {  // rep -1 is the warm-up launch
+      if (rep == 0) HPCCG_CUDA(cudaEventRecord(c->ev0, c->stream));
+      // the spmv/dot kernel sets status on 0/0; reset it before every launch
+      HPCCG_CUDA(cudaMemsetAsync(&c->d_state->status, 0, sizeof(int), c->stream));
+      if (which == 0) {
+        k_cg_update_p<<<c->grid, kBlock, 0, c->stream>>>(g);
+      } else if (which == 1) {
+        rc = dispatch_strategy(a, [&](auto strat) {
+          using St = decltype(strat);
+          k_cg_spmv_dot<St><<<c->grid, kBlock, 0, c->stream>>>(a, g);
+          return 0;
+        });
+      } else {
+        k_cg_update_r<<<c->grid, kBlock, 0, c->stream>>>(g);
+      }
+      HPCCG_CUDA(cudaGetLastError());
+    }
+    HPCCG_CUDA(cudaEventRecord(c->ev1, c->stream));
+    HPCCG_CUDA(cudaEventSynchronize(c->ev1));
+    float t = 0.f;
+    HPCCG_CUDA(cudaEventElapsedTime(&t, c->ev0, c->ev1));
+    ms[which] = t / (float)reps;
+  }
+  return HPCCG_OK;
+}

@@ -1,0 +1,247 @@
+// hpccg_rows.cuh -- row strategies of the FP64 SpMV (MPI/src/SparseMatrix.F90:213-232).
+//
+// Every strategy walks the rows of A, forms rowsum_i = sum_k val_k * x[col_k],
+// and hands (i, rowsum_i) to an epilogue functor that stores the result and
+// returns this row's contribution to a fused dot product.
+//
+//  * ell_rows<W,RPT>: one thread per row (RPT = 1) or per row pair (RPT = 2)
+//    over the column-major ELL copy.  Slot k of 32 consecutive rows is one
+//    256-byte (RPT=1) or 512-byte (RPT=2) coalesced load; the x gather for a
+//    stencil slot hits 32 consecutive x entries.  The sum runs k = 0..W-1 in
+//    order with separately rounded multiply and add, exactly the reference's
+//    `rowsum = rowsum + values(k)*x(colindex(k))`, so y is bit-identical to
+//    the reference's spmv.  Matrix streams use evict-first loads so that L2
+//    keeps x.
+//  * csr_vector_rows<LPR>: LPR lanes per CSR row (LPR = 32 is warp-per-row),
+//    lane-strided loads, butterfly shuffle reduction.  Reassociates the sum.
+#pragma once
+#include "hpccg_internal.cuh"
+
+namespace hpccg {
+
+__device__ __forceinline__ double mul_add(double s, double v, double x) {
+  return __dadd_rn(s, __dmul_rn(v, x));  // no contraction: reference rounding
+}
+
+template <int W, int RPT, int U, class Epi>
+__device__ __forceinline__ double ell_rows(int n, int npad, const int32_t *__restrict__ col,
+                                           const double *__restrict__ val,
+                                           const double *__restrict__ x, Epi &epi) {
+  static_assert(W % U == 0, "slot chunk must divide the ELL width");
+  double part = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  if constexpr (RPT == 1) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+      double s = 0.0;
+#pragma unroll
+      for (int k0 = 0; k0 < W; k0 += U) {
+        int32_t c[U];
+        double v[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+          c[k] = __ldcs(col + (size_t)(k0 + k) * npad + i);
+          v[k] = __ldcs(val + (size_t)(k0 + k) * npad + i);
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) s = mul_add(s, v[k], __ldg(x + c[k]));
+      }
+      part = __dadd_rn(part, epi(i, s));
+    }
+  } else {
+    const int half = npad >> 1;
+    const int npairs = (n + 1) >> 1;
+    const int2 *col2 = reinterpret_cast<const int2 *>(col);
+    const double2 *val2 = reinterpret_cast<const double2 *>(val);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += stride) {
+      double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+      for (int k0 = 0; k0 < W; k0 += U) {
+        int2 c[U];
+        double2 v[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+          c[k] = __ldcs(col2 + (size_t)(k0 + k) * half + t);
+          v[k] = __ldcs(val2 + (size_t)(k0 + k) * half + t);
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+          s0 = mul_add(s0, v[k].x, __ldg(x + c[k].x));
+          s1 = mul_add(s1, v[k].y, __ldg(x + c[k].y));
+        }
+      }
+      const int i0 = 2 * t;
+      part = __dadd_rn(part, epi(i0, s0));
+      if (i0 + 1 < n) part = __dadd_rn(part, epi(i0 + 1, s1));
+    }
+  }
+  return part;
+}
+
+// Runtime-width variant for ELL widths other than the compiled ones.
+template <class Epi>
+__device__ __forceinline__ double ell_rows_dyn(int n, int npad, int W,
+                                               const int32_t *__restrict__ col,
+                                               const double *__restrict__ val,
+                                               const double *__restrict__ x, Epi &epi) {
+  double part = 0.0;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double s = 0.0;
+#pragma unroll 4
+    for (int k = 0; k < W; ++k)
+      s = mul_add(s, __ldcs(val + (size_t)k * npad + i), __ldg(x + __ldcs(col + (size_t)k * npad + i)));
+    part = __dadd_rn(part, epi(i, s));
+  }
+  return part;
+}
+
+template <int LPR, class Epi>
+__device__ __forceinline__ double csr_vector_rows(int n, const int32_t *__restrict__ rowptr,
+                                                  const int32_t *__restrict__ col,
+                                                  const double *__restrict__ val,
+                                                  const double *__restrict__ x, Epi &epi) {
+  constexpr int RPW = 32 / LPR;  // rows per warp
+  double part = 0.0;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane / LPR, sl = lane % LPR;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int base = warp * RPW; base < n; base += nwarps * RPW) {  // warp-uniform trip count
+    const int row = base + sub;
+    double s = 0.0;
+    if (row < n) {
+      const int a = __ldg(rowptr + row), e = __ldg(rowptr + row + 1);
+      for (int j = a + sl; j < e; j += LPR) s = mul_add(s, __ldcs(val + j), __ldg(x + __ldcs(col + j)));
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, o));
+    if (sl == 0 && row < n) part = __dadd_rn(part, epi(row, s));
+  }
+  return part;
+}
+
+// ---- epilogues --------------------------------------------------------------
+struct EpiStore {  // y = A x
+  double *y;
+  __device__ __forceinline__ double operator()(int i, double s) const {
+    y[i] = s;
+    return 0.0;
+  }
+};
+struct EpiDot {  // Ap = A p, contribution p_i * Ap_i
+  const double *p;
+  double *y;
+  __device__ __forceinline__ double operator()(int i, double s) const {
+    y[i] = s;
+    return __dmul_rn(__ldg(p + i), s);
+  }
+};
+struct EpiResidual {  // r = 1*b + (-1)*(A x), contribution r_i^2
+  const double *b;
+  double *r;
+  __device__ __forceinline__ double operator()(int i, double s) const {
+    const double ri = __dsub_rn(__ldg(b + i), s);
+    r[i] = ri;
+    return __dmul_rn(ri, ri);
+  }
+};
+
+// Arguments every row strategy may need.
+struct SpmvArgs {
+  int kind;   // HPCCG_SPMV_ELL / ELL2 / CSR_VECTOR
+  int param;  // lanes per row for CSR_VECTOR
+  int n, npad, W;
+  const int32_t *rowptr, *col, *ell_col;
+  const double *val, *ell_val;
+};
+
+// Strategy tags: each kernel is compiled once per strategy and the host picks
+// the instantiation.  kMinBlocks feeds __launch_bounds__: with 2 resident
+// blocks per SM ptxas keeps all 27 slot loads of a row in flight (~120
+// registers); with 8 it interleaves loads and gathers at 32 registers and
+// relies on occupancy instead.  Strategies with the same RPT map rows to
+// threads identically, so they give bit-identical results (fused dots too).
+template <int MINB>
+struct StratEll1 {
+  static constexpr int kMinBlocks = MINB;
+  template <class Epi>
+  static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
+    return ell_rows<27, 1, 27>(a.n, a.npad, a.ell_col, a.ell_val, x, e);
+  }
+};
+template <int MINB>
+struct StratEll2 {
+  static constexpr int kMinBlocks = MINB;
+  template <class Epi>
+  static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
+    return ell_rows<27, 2, 9>(a.n, a.npad, a.ell_col, a.ell_val, x, e);
+  }
+};
+struct StratEllDyn {
+  static constexpr int kMinBlocks = 4;
+  template <class Epi>
+  static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
+    return ell_rows_dyn(a.n, a.npad, a.W, a.ell_col, a.ell_val, x, e);
+  }
+};
+template <int LPR>
+struct StratCsr {
+  static constexpr int kMinBlocks = 4;
+  template <class Epi>
+  static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
+    return csr_vector_rows<LPR>(a.n, a.rowptr, a.col, a.val, x, e);
+  }
+};
+
+// Resident-block hints offered for the ELL strategies (the `param` of
+// hpccg_gpu_set_spmv for HPCCG_SPMV_ELL / HPCCG_SPMV_ELL2).
+constexpr int kEllMinBlocks[4] = {2, 3, 4, 8};
+
+// Calls f(Strat{}) with the strategy the arguments select (host side).
+template <class F>
+inline int dispatch_strategy(const SpmvArgs &a, F &&f) {
+  if (a.kind == HPCCG_SPMV_CSR_VECTOR) {
+    switch (a.param) {
+      case 4: return f(StratCsr<4>{});
+      case 8: return f(StratCsr<8>{});
+      case 16: return f(StratCsr<16>{});
+      default: return f(StratCsr<32>{});
+    }
+  }
+  if (a.W != 27) return f(StratEllDyn{});
+  if (a.kind == HPCCG_SPMV_ELL2) {
+    switch (a.param) {
+      case 2: return f(StratEll2<2>{});
+      case 3: return f(StratEll2<3>{});
+      case 8: return f(StratEll2<8>{});
+      default: return f(StratEll2<4>{});
+    }
+  }
+  switch (a.param) {
+    case 2: return f(StratEll1<2>{});
+    case 3: return f(StratEll1<3>{});
+    case 8: return f(StratEll1<8>{});
+    default: return f(StratEll1<4>{});
+  }
+}
+
+inline SpmvArgs spmv_args(const hpccg_ctx *c) {
+  SpmvArgs a;
+  a.kind = c->spmv_kind == HPCCG_SPMV_AUTO ? HPCCG_SPMV_ELL : c->spmv_kind;
+  a.param = c->spmv_kind == HPCCG_SPMV_AUTO ? 4 : c->spmv_param;
+  if (!c->d_ell_col && a.kind != HPCCG_SPMV_CSR_VECTOR) {
+    a.kind = HPCCG_SPMV_CSR_VECTOR;
+    a.param = 32;
+  }
+  a.n = c->nrow;
+  a.npad = c->npad;
+  a.W = c->ell_width;
+  a.rowptr = c->d_rowptr;
+  a.col = c->d_col;
+  a.val = c->d_val;
+  a.ell_col = c->d_ell_col;
+  a.ell_val = c->d_ell_val;
+  return a;
+}
+
+}  // namespace hpccg

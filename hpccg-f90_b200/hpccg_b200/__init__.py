@@ -1,0 +1,269 @@
+"""Python host mirror of the reference HPCCG interface over the B200 C-ABI.
+
+Every call goes through ``libhpccg_b200.so`` (include/hpccg_gpu.h) with
+ctypes; there is no CPU fallback.  If the library is missing, importing this
+package raises.  Names follow the reference (MPI/src): ``generate_matrix``
+(SparseMatrix.F90:68-185), ``Matrix.cg`` (numerics.F90:41-162), ``spmv``
+(SparseMatrix.F90:213-232) and the BLAS-1 routines of vector_operations.F90.
+
+Device arrays are torch CUDA tensors (torch is used for device memory only);
+host arrays are numpy arrays.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(PKG_DIR), "libhpccg_b200.so")
+
+HPCCG_OK = 0
+HPCCG_ERR_INVALID_ARG = 1
+HPCCG_ERR_CUDA = 2
+HPCCG_ERR_OOM = 3
+HPCCG_ERR_BREAKDOWN = 4
+HPCCG_ERR_TIMEOUT = 5
+HPCCG_ERR_NOT_CONVERGED = 6
+HPCCG_ERR_UNSUPPORTED = 7
+HPCCG_ERR_NO_DEVICE = 8
+
+SPMV_AUTO, SPMV_ELL, SPMV_ELL2, SPMV_CSR_VECTOR = 0, 1, 2, 3
+
+
+class HpccgError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        super().__init__(f"{what}: {strerror(code)} (code {code})")
+
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"libhpccg_b200.so not built ({LIB_PATH}); run `make -C hpccg-f90_b200`")
+
+_lib = ctypes.CDLL(LIB_PATH)
+_c = ctypes
+_vp = _c.c_void_p
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32 = _c.c_int32
+_i64 = _c.c_int64
+_f64 = _c.c_double
+
+_SIGS = {
+    "hpccg_strerror": (_c.c_char_p, [_c.c_int]),
+    "hpccg_generate_matrix": (_c.c_int, [_i32, _i32, _i32, _i32p, _i32p, _f64p, _f64p, _f64p, _f64p,
+                                          _c.POINTER(_i64)]),
+    "hpccg_gpu_create": (_c.c_int, [_i32, _i64, _i32p, _i32p, _f64p, _c.POINTER(_vp)]),
+    "hpccg_gpu_create_generated": (_c.c_int, [_i32, _i32, _i32, _vp, _vp, _vp, _c.POINTER(_vp)]),
+    "hpccg_gpu_destroy": (None, [_vp]),
+    "hpccg_gpu_info": (_c.c_int, [_vp, _c.POINTER(_i32), _c.POINTER(_i64), _c.POINTER(_i32)]),
+    "hpccg_gpu_download_csr": (_c.c_int, [_vp, _i32p, _i32p, _f64p]),
+    "hpccg_gpu_set_spmv": (_c.c_int, [_vp, _i32, _i32]),
+    "hpccg_gpu_get_spmv": (_c.c_int, [_vp, _c.POINTER(_i32), _c.POINTER(_i32)]),
+    "hpccg_gpu_cg": (_c.c_int, [_vp, _f64p, _f64p, _i32, _f64, _c.POINTER(_i32), _c.POINTER(_f64), _vp]),
+    "hpccg_gpu_cg_device": (_c.c_int, [_vp, _vp, _vp, _i32, _f64, _c.POINTER(_i32), _c.POINTER(_f64), _vp]),
+    "hpccg_gpu_spmv": (_c.c_int, [_vp, _vp, _vp]),
+    "hpccg_gpu_ddot": (_c.c_int, [_vp, _i32, _vp, _vp, _c.POINTER(_f64)]),
+    "hpccg_gpu_ddot1": (_c.c_int, [_vp, _i32, _vp, _c.POINTER(_f64)]),
+    "hpccg_gpu_waxpby": (_c.c_int, [_vp, _i32, _f64, _vp, _f64, _vp, _vp]),
+    "hpccg_gpu_wwpby": (_c.c_int, [_vp, _i32, _f64, _vp, _vp]),
+    "hpccg_gpu_wxbw": (_c.c_int, [_vp, _i32, _vp, _f64, _vp]),
+    "hpccg_gpu_vcopy": (_c.c_int, [_vp, _i32, _vp, _vp]),
+    "hpccg_gpu_time_spmv": (_c.c_int, [_vp, _vp, _vp, _i32, _c.POINTER(_c.c_float)]),
+    "hpccg_gpu_uniform_pm1": (_c.c_int, [_vp, _c.c_uint64, _i64, _i64, _vp]),
+    "hpccg_gpu_last_solve_ms": (_c.c_int, [_vp, _c.POINTER(_c.c_float)]),
+    "hpccg_gpu_time_cg_kernels": (_c.c_int, [_vp, _i32, _c.POINTER(_c.c_float)]),
+}
+for _name, (_res, _args) in _SIGS.items():
+    _fn = getattr(_lib, _name)
+    _fn.restype = _res
+    _fn.argtypes = _args
+
+
+def strerror(code: int) -> str:
+    return _lib.hpccg_strerror(code).decode()
+
+
+def _check(rc: int, what: str, allow=(HPCCG_OK,)) -> int:
+    if rc not in allow:
+        raise HpccgError(rc, what)
+    return rc
+
+
+def exported_symbols() -> list[str]:
+    """Names of the C-ABI entry points this binding resolved from the library."""
+    return sorted(_SIGS)
+
+
+def _dptr(t) -> int:
+    """Device pointer of a torch CUDA tensor (contiguous float64 expected)."""
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("expected a contiguous CUDA tensor")
+    return t.data_ptr()
+
+
+def _sync_torch():
+    import torch
+
+    torch.cuda.synchronize()
+
+
+# ---- host generator ------------------------------------------------------------
+
+def generate_matrix(nx: int, ny: int, nz: int):
+    """SparseMatrix.F90:68-185 on the host.  Returns (rowindex, colindex, values, x, b, xexact),
+    1-based int32 indices exactly as the reference stores them (colindex/values trimmed to nnz)."""
+    n = nx * ny * nz
+    rowindex = np.empty(n + 1, np.int32)
+    colindex = np.empty(27 * n, np.int32)
+    values = np.empty(27 * n, np.float64)
+    x = np.empty(n, np.float64)
+    b = np.empty(n, np.float64)
+    xexact = np.empty(n, np.float64)
+    nnz = _i64(0)
+    _check(_lib.hpccg_generate_matrix(nx, ny, nz, rowindex, colindex, values, x, b, xexact, _c.byref(nnz)),
+           "generate_matrix")
+    k = nnz.value
+    return rowindex, colindex[:k].copy(), values[:k].copy(), x, b, xexact
+
+
+class Matrix:
+    """A matrix resident on the GPU (the SparseMatrixT of the reference)."""
+
+    def __init__(self, handle: int):
+        self._h = _vp(handle)
+        nr, nnz, w = _i32(0), _i64(0), _i32(0)
+        _check(_lib.hpccg_gpu_info(self._h, _c.byref(nr), _c.byref(nnz), _c.byref(w)), "info")
+        self.nrow, self.nnz, self.ell_width = nr.value, nnz.value, w.value
+
+    # -- construction --
+    @classmethod
+    def from_csr(cls, rowindex, colindex, values) -> "Matrix":
+        rowindex = np.ascontiguousarray(rowindex, np.int32)
+        colindex = np.ascontiguousarray(colindex, np.int32)
+        values = np.ascontiguousarray(values, np.float64)
+        h = _vp()
+        _check(_lib.hpccg_gpu_create(len(rowindex) - 1, len(colindex), rowindex, colindex, values,
+                                     _c.byref(h)), "create")
+        return cls(h.value)
+
+    @classmethod
+    def generated(cls, nx: int, ny: int, nz: int, d_x=None, d_b=None, d_xexact=None) -> "Matrix":
+        h = _vp()
+        ptr = lambda t: None if t is None else _dptr(t)  # noqa: E731
+        if d_x is not None or d_b is not None or d_xexact is not None:
+            _sync_torch()
+        _check(_lib.hpccg_gpu_create_generated(nx, ny, nz, ptr(d_x), ptr(d_b), ptr(d_xexact), _c.byref(h)),
+               "create_generated")
+        return cls(h.value)
+
+    def close(self):
+        if self._h:
+            _lib.hpccg_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def download_csr(self):
+        rowindex = np.empty(self.nrow + 1, np.int32)
+        colindex = np.empty(self.nnz, np.int32)
+        values = np.empty(self.nnz, np.float64)
+        _check(_lib.hpccg_gpu_download_csr(self._h, rowindex, colindex, values), "download_csr")
+        return rowindex, colindex, values
+
+    # -- kernel selection --
+    def set_spmv(self, kind: int, param: int = 0):
+        _check(_lib.hpccg_gpu_set_spmv(self._h, kind, param), "set_spmv")
+
+    def get_spmv(self):
+        k, p = _i32(0), _i32(0)
+        _check(_lib.hpccg_gpu_get_spmv(self._h, _c.byref(k), _c.byref(p)), "get_spmv")
+        return k.value, p.value
+
+    # -- the CG entry point (numerics.F90:41-162) --
+    def cg(self, b, x, max_iter: int = 150, tolerance: float = 0.0, history: bool = True):
+        """Host arrays.  Returns (x, niters, normr, hist, status); x is updated in place."""
+        b = np.ascontiguousarray(b, np.float64)
+        if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous):
+            raise ValueError("x must be a contiguous float64 numpy array (updated in place)")
+        hist = np.zeros(max_iter + 1, np.float64)
+        niters, normr = _i32(0), _f64(0.0)
+        rc = _lib.hpccg_gpu_cg(self._h, b, x, max_iter, tolerance, _c.byref(niters), _c.byref(normr),
+                               hist.ctypes.data if history else None)
+        _check(rc, "cg", allow=(HPCCG_OK, HPCCG_ERR_BREAKDOWN))
+        return x, niters.value, normr.value, hist[: niters.value + 1], rc
+
+    def cg_device(self, d_b, d_x, max_iter: int = 150, tolerance: float = 0.0, history: bool = True):
+        """Device arrays (torch CUDA float64).  Returns (niters, normr, hist, status)."""
+        _sync_torch()
+        hist = np.zeros(max_iter + 1, np.float64)
+        niters, normr = _i32(0), _f64(0.0)
+        rc = _lib.hpccg_gpu_cg_device(self._h, _dptr(d_b), _dptr(d_x), max_iter, tolerance,
+                                      _c.byref(niters), _c.byref(normr), hist.ctypes.data if history else None)
+        _check(rc, "cg_device", allow=(HPCCG_OK, HPCCG_ERR_BREAKDOWN))
+        return niters.value, normr.value, hist[: niters.value + 1], rc
+
+    # -- op-level drop-ins on device tensors --
+    def spmv(self, d_x, d_y):
+        _sync_torch()
+        _check(_lib.hpccg_gpu_spmv(self._h, _dptr(d_x), _dptr(d_y)), "spmv")
+
+    def ddot(self, d_x, d_y) -> float:
+        _sync_torch()
+        r = _f64(0.0)
+        _check(_lib.hpccg_gpu_ddot(self._h, d_x.numel(), _dptr(d_x), _dptr(d_y), _c.byref(r)), "ddot")
+        return r.value
+
+    def ddot1(self, d_x) -> float:
+        _sync_torch()
+        r = _f64(0.0)
+        _check(_lib.hpccg_gpu_ddot1(self._h, d_x.numel(), _dptr(d_x), _c.byref(r)), "ddot1")
+        return r.value
+
+    def waxpby(self, alpha, d_x, beta, d_y, d_w):
+        _sync_torch()
+        _check(_lib.hpccg_gpu_waxpby(self._h, d_x.numel(), alpha, _dptr(d_x), beta, _dptr(d_y), _dptr(d_w)),
+               "waxpby")
+
+    def wwpby(self, beta, d_y, d_w):
+        _sync_torch()
+        _check(_lib.hpccg_gpu_wwpby(self._h, d_w.numel(), beta, _dptr(d_y), _dptr(d_w)), "wwpby")
+
+    def wxbw(self, d_x, beta, d_w):
+        _sync_torch()
+        _check(_lib.hpccg_gpu_wxbw(self._h, d_w.numel(), _dptr(d_x), beta, _dptr(d_w)), "wxbw")
+
+    def vcopy(self, d_x, d_y):
+        _sync_torch()
+        _check(_lib.hpccg_gpu_vcopy(self._h, d_x.numel(), _dptr(d_x), _dptr(d_y)), "vcopy")
+
+    def uniform_pm1(self, seed: int, d_out, offset: int = 0):
+        """Fill a device tensor with the project's counter-based U[-1,1) stream."""
+        _sync_torch()
+        _check(_lib.hpccg_gpu_uniform_pm1(self._h, seed, offset, d_out.numel(), _dptr(d_out)), "uniform_pm1")
+
+    def last_solve_ms(self) -> float:
+        ms = _c.c_float(0.0)
+        _check(_lib.hpccg_gpu_last_solve_ms(self._h, _c.byref(ms)), "last_solve_ms")
+        return ms.value
+
+    def time_cg_kernels(self, reps: int = 10):
+        """Average ms of (p/x update, SpMV+p.Ap, r update+r.r) launched back to back."""
+        ms = (_c.c_float * 3)()
+        _check(_lib.hpccg_gpu_time_cg_kernels(self._h, reps, ms), "time_cg_kernels")
+        return [ms[0], ms[1], ms[2]]
+
+    def time_spmv(self, d_x, d_y, reps: int = 10) -> float:
+        _sync_torch()
+        ms = _c.c_float(0.0)
+        _check(_lib.hpccg_gpu_time_spmv(self._h, _dptr(d_x), _dptr(d_y), reps, _c.byref(ms)), "time_spmv")
+        return ms.value

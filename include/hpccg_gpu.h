@@ -1,0 +1,149 @@
+/*
+ * hpccg_gpu.h -- C-ABI of the B200 (sm_100a) HPCCG conjugate-gradient library.
+ *
+ * Drop-in boundary for the reference's single-rank CG path
+ * (RRZE-HPC/HPCCG-F90, MPI variant; exchange_externals is a no-op on one rank,
+ * MPI/src/SparseMatrix.F90:643-645).  Plain C types only: the Fortran host
+ * binds these with ISO_C_BINDING interfaces, C/C++ hosts include this header,
+ * Python binds them with ctypes.
+ *
+ * Conventions
+ *  - Every call returns HPCCG_OK (0) or a positive HPCCG_ERR_* code; nothing
+ *    aborts the process (the reference calls `stop`).
+ *  - Matrices cross the boundary in the reference's layout: 1-based int32
+ *    rowindex(nrow+1) / colindex(nnz), real(dp) values(nnz)
+ *    (MPI/src/SparseMatrix.F90:44-64).
+ *  - `d_` arguments are device pointers on the context's GPU; other array
+ *    arguments are host pointers (pinned memory gives the fastest copies).
+ *  - A context is used from one host thread at a time; calls on one context
+ *    are serialised on its stream and return after the GPU work is done.
+ */
+#ifndef HPCCG_GPU_H
+#define HPCCG_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HPCCG_OK 0
+#define HPCCG_ERR_INVALID_ARG 1   /* null pointer, negative size, bad CSR */
+#define HPCCG_ERR_CUDA 2          /* a CUDA runtime call failed */
+#define HPCCG_ERR_OOM 3           /* device allocation failed */
+#define HPCCG_ERR_BREAKDOWN 4     /* p'Ap <= 0, or a NaN/Inf scalar, in CG */
+#define HPCCG_ERR_TIMEOUT 5       /* a bounded device-side wait gave up */
+#define HPCCG_ERR_NOT_CONVERGED 6 /* a solve with a target stopped short of it */
+#define HPCCG_ERR_UNSUPPORTED 7   /* option not available for this matrix */
+#define HPCCG_ERR_NO_DEVICE 8     /* no CUDA device visible */
+
+typedef struct hpccg_ctx hpccg_ctx;
+
+/* Human-readable name of an HPCCG_* code. */
+const char *hpccg_strerror(int code);
+
+/* ---- matrix construction ------------------------------------------------ */
+
+/* Host generator, bit-exact with MPI/src/SparseMatrix.F90:68-185
+ * generate_matrix on one rank.  rowindex: nrow+1, colindex/values: capacity
+ * 27*nrow (the reference allocates 27*nrow, :119-121), x/b/xexact: nrow,
+ * nrow = nx*ny*nz.  *nnz receives the number of stored nonzeros. */
+int hpccg_generate_matrix(int32_t nx, int32_t ny, int32_t nz, int32_t *rowindex,
+                          int32_t *colindex, double *values, double *x, double *b,
+                          double *xexact, int64_t *nnz);
+
+/* Uploads a CSR matrix (reference layout) to the current CUDA device and
+ * builds the device layouts the kernels use.  Replaces the matrix half of the
+ * `type(SparseMatrixT)` argument of cg (MPI/src/numerics.F90:41-49). */
+int hpccg_gpu_create(int32_t nrow, int64_t nnz, const int32_t *rowindex,
+                     const int32_t *colindex, const double *values, hpccg_ctx **ctx);
+
+/* Builds the generate_matrix(nx,ny,nz) matrix directly on the device (same
+ * rows/cols/values as the host generator) and, if the pointers are non-null,
+ * writes x (=0), b and xexact (=1) to DEVICE arrays of length nx*ny*nz. */
+int hpccg_gpu_create_generated(int32_t nx, int32_t ny, int32_t nz, double *d_x, double *d_b,
+                               double *d_xexact, hpccg_ctx **ctx);
+
+void hpccg_gpu_destroy(hpccg_ctx *ctx);
+
+/* Basic facts about the context: rows, stored nonzeros, ELL width. */
+int hpccg_gpu_info(const hpccg_ctx *ctx, int32_t *nrow, int64_t *nnz, int32_t *ell_width);
+
+/* Copies the device CSR back in the reference's 1-based layout (for checks). */
+int hpccg_gpu_download_csr(const hpccg_ctx *ctx, int32_t *rowindex, int32_t *colindex,
+                           double *values);
+
+/* SpMV kernel selection.  HPCCG_SPMV_AUTO picks the fastest bit-exact FP64
+ * kernel on first use; the others force one kernel. */
+#define HPCCG_SPMV_AUTO 0
+#define HPCCG_SPMV_ELL 1        /* thread per row, column-major ELL (param: resident blocks/SM hint 2,3,4,8) */
+#define HPCCG_SPMV_ELL2 2       /* two rows per thread, 16-byte loads (same param)  */
+#define HPCCG_SPMV_CSR_VECTOR 3 /* warp-per-row CSR (lanes per row = param)    */
+int hpccg_gpu_set_spmv(hpccg_ctx *ctx, int32_t kind, int32_t param);
+int hpccg_gpu_get_spmv(const hpccg_ctx *ctx, int32_t *kind, int32_t *param);
+
+/* ---- the CG entry point ------------------------------------------------- */
+
+/* MPI/src/numerics.F90:41-162 cg(A, b, x, max_iter, tolerance, niters, normr)
+ * on host arrays of length nrow.  x holds x0 on entry and the solution on
+ * exit.  niters and normr follow the reference exactly (normr is the last
+ * residual norm the loop computed, ||r_{niters-1}||; the stop test
+ * `normr < tolerance` runs at the top of each iteration).  resid_hist
+ * (nullable, length >= max_iter+1) receives [0] = Initial Residual and
+ * [k] = the normr of iteration k, k = 1..niters.  The whole loop runs on the
+ * device inside one CUDA graph with a device-side while condition. */
+int hpccg_gpu_cg(hpccg_ctx *ctx, const double *b, double *x, int32_t max_iter,
+                 double tolerance, int32_t *niters, double *normr, double *resid_hist);
+
+/* Same as hpccg_gpu_cg on device arrays (b, x on the context's device). */
+int hpccg_gpu_cg_device(hpccg_ctx *ctx, const double *d_b, double *d_x, int32_t max_iter,
+                        double tolerance, int32_t *niters, double *normr,
+                        double *resid_hist);
+
+/* ---- op-level drop-ins (device arrays), MPI/src/SparseMatrix.F90:213-232
+ *      and MPI/src/vector_operations.F90:40-169 ------------------------------ */
+
+int hpccg_gpu_spmv(hpccg_ctx *ctx, const double *d_x, double *d_y);      /* y = A x   */
+int hpccg_gpu_ddot(hpccg_ctx *ctx, int32_t n, const double *d_x, const double *d_y,
+                   double *result);                                          /* x.y       */
+int hpccg_gpu_ddot1(hpccg_ctx *ctx, int32_t n, const double *d_x, double *result); /* x.x */
+int hpccg_gpu_waxpby(hpccg_ctx *ctx, int32_t n, double alpha, const double *d_x, double beta,
+                     const double *d_y, double *d_w);                       /* w=ax+by   */
+int hpccg_gpu_wwpby(hpccg_ctx *ctx, int32_t n, double beta, const double *d_y,
+                    double *d_w);                                            /* w=w+by    */
+int hpccg_gpu_wxbw(hpccg_ctx *ctx, int32_t n, const double *d_x, double beta,
+                   double *d_w);                                             /* w=x+bw    */
+int hpccg_gpu_vcopy(hpccg_ctx *ctx, int32_t n, const double *d_x, double *d_y); /* y = x */
+
+/* ---- synthetic inputs -------------------------------------------------- */
+
+/* d_out[i] = uniform double in [-1,1) from the project's counter-based
+ * generator: z = splitmix64 finaliser of seed + (offset+i+1)*0x9E3779B97F4A7C15,
+ * value = 2*((z>>11)*2^-53) - 1.  No reference counterpart (the reference
+ * only uses x = 1); it makes the random right-hand sides reproducible on
+ * host and device. */
+int hpccg_gpu_uniform_pm1(hpccg_ctx *ctx, uint64_t seed, int64_t offset, int64_t n, double *d_out);
+
+/* ---- timing helpers (device time, CUDA events on the context stream) ----- */
+
+/* Device time in ms of the last hpccg_gpu_cg / hpccg_gpu_cg_device solve,
+ * from events recorded on the context stream around the graph launch (input
+ * and output copies excluded). */
+int hpccg_gpu_last_solve_ms(const hpccg_ctx *ctx, float *ms);
+
+/* Average device time in ms of each CG iteration kernel launched `reps` times
+ * back to back on the context stream: ms[0] = p/x update, ms[1] = SpMV fused
+ * with p.Ap, ms[2] = r update fused with r.r.  Leaves the CG work vectors
+ * with unspecified contents. */
+int hpccg_gpu_time_cg_kernels(hpccg_ctx *ctx, int32_t reps, float *ms);
+
+/* Average device time in ms of `reps` back-to-back SpMVs y = A x with the
+ * current kernel selection. */
+int hpccg_gpu_time_spmv(hpccg_ctx *ctx, const double *d_x, double *d_y, int32_t reps,
+                        float *ms_per_call);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HPCCG_GPU_H */

@@ -1,0 +1,77 @@
+/*
+ * hpccg_oracle.h -- CPU oracle for the HPCCG conjugate-gradient path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference
+ * Fortran 90 HPCCG (MPI/src, built sequentially: ENABLE_MPI=NO, ENABLE_OMP=NO)
+ * used as the checker for the CUDA product and as the timed CPU baseline.
+ * Nothing in the product links or calls it.
+ *
+ * Parity status: UNPINNED against reference outputs.  The reference ships no
+ * tests, fixtures or golden vectors, and it is Fortran 90 with no Fortran
+ * compiler available, so it cannot be run here.  The oracle is instead checked
+ * against analytic known answers that follow from the reference's definitions:
+ * nnz = (3nx-2)(3ny-2)(3nz-2), b = A*1 exactly, Initial Residual = ||b||,
+ * x -> xexact = 1, and the row/column layout implied by the loop nest.
+ *
+ * Floating-point semantics: compiled with -O2 -ffp-contract=off (no FMA, no
+ * reassociation), every loop runs in the reference's index order, so results
+ * equal what gfortran -O2/-O3 (no -ffast-math) would give for MPI/src.
+ * The OpenMP build (liboracle_omp.so) adds the reference's
+ * "!$OMP PARALLEL DO [REDUCTION(+:)]" work sharing and is used for timing only.
+ */
+#ifndef HPCCG_ORACLE_H
+#define HPCCG_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* MPI/src/SparseMatrix.F90:68-185 generate_matrix, one rank.
+ * rowindex: nrow+1 (1-based), colindex/values: 27*nrow (1-based cols),
+ * x, b, xexact: nrow.  Returns the number of stored nonzeros. */
+int64_t orc_generate_matrix(int32_t nx, int32_t ny, int32_t nz, int32_t *rowindex,
+                            int32_t *colindex, double *values, double *x, double *b,
+                            double *xexact);
+
+/* MPI/src/SparseMatrix.F90:213-232 spmv: y(i) = sum_k values(k)*x(colindex(k)). */
+void orc_spmv(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
+              const double *values, const double *x, double *y);
+
+/* MPI/src/vector_operations.F90:40-169 */
+double orc_ddot(int32_t n, const double *x, const double *y);
+double orc_ddot1(int32_t n, const double *x);
+void orc_waxpby(int32_t n, double alpha, const double *x, double beta, const double *y,
+                double *w);
+void orc_wwpby(int32_t n, double beta, const double *y, double *w);
+void orc_wxbw(int32_t n, const double *x, double beta, double *w);
+void orc_vcopy(int32_t n, const double *x, double *y);
+
+/* MPI/src/numerics.F90:41-162 cg.  x is updated in place.  hist (nullable,
+ * length max_iter+1) receives hist[0] = Initial Residual and hist[k] = the
+ * normr computed at iteration k (the value the reference prints), k=1..niters.
+ * Returns 0. */
+int orc_cg(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
+           const double *values, const double *b, double *x, int32_t max_iter,
+           double tolerance, int32_t *niters, double *normr, double *hist);
+
+/* MPI/src/numerics.F90:164-198 compute_residual: max_i |v1(i)-v2(i)|. */
+double orc_compute_residual(int32_t n, const double *v1, const double *v2);
+
+/* ||b - A x||_2 / ||b||_2 in sequential FP64 (the convergence judge). */
+double orc_true_relres(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
+                       const double *values, const double *b, const double *x);
+
+/* The project's counter-based generator (no reference counterpart): value i of
+ * stream `seed` is splitmix64's finaliser applied to seed + (i+1)*golden;
+ * uniform in [-1,1) is 2*((z>>11)*2^-53) - 1. */
+uint64_t orc_splitmix64_at(uint64_t seed, uint64_t i);
+void orc_uniform_pm1(uint64_t seed, int64_t n, double *out);
+/* Grid sizes for the batched workload: sizes[3*s+d] = lo + (z mod (hi-lo+1)),
+ * z = orc_splitmix64_at(seed, 3*s+d). */
+void orc_batch_sizes(uint64_t seed, int32_t nsys, int32_t lo, int32_t hi, int32_t *sizes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

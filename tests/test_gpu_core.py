@@ -1,0 +1,240 @@
+"""GPU parity of the FP64 path through the C-ABI against the CPU oracle.
+
+Bars: integer/index work (CSR, generators) bit-exact; SpMV on the ELL kernels
+bit-exact (same per-row order, no FMA); element-wise BLAS-1 bit-exact; dot
+products within 1e-13 relative (reassociated sum); CG residual history within
+1e-12 relative while ||r_k|| >= 1e-8 ||r_0|| and within 1e-12 ||r_0|| absolute
+afterwards; final x within 1e-10 of the oracle's and of xexact = 1.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture(scope="module")
+def hp():
+    import hpccg_b200
+    return hpccg_b200
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    assert t.cuda.is_available()
+    return t
+
+
+def assert_history_parity(h_gpu, h_ref, rtol=1e-12, band=1e-8):
+    n = min(len(h_gpu), len(h_ref))
+    r0 = h_ref[0]
+    for k in range(n):
+        if not np.isfinite(h_ref[k]):
+            break
+        bound = rtol * h_ref[k] if h_ref[k] >= band * r0 else rtol * r0
+        assert abs(h_gpu[k] - h_ref[k]) <= bound, (k, h_gpu[k], h_ref[k])
+
+
+SIZES = [(1, 1, 1), (2, 1, 1), (1, 2, 3), (2, 2, 2), (3, 5, 7), (4, 4, 4), (7, 1, 3), (16, 16, 16),
+         (9, 2, 11), (33, 17, 5), (64, 64, 64)]
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES)
+def test_upload_roundtrip_and_device_generator(hp, torch, nx, ny, nz):
+    A, x, b, xe = oracle.generate_matrix(nx, ny, nz)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    r, c, v = M.download_csr()
+    assert np.array_equal(r, A.rowindex) and np.array_equal(c, A.colindex) and np.array_equal(v, A.values)
+    n = nx * ny * nz
+    dx = torch.full((n,), 7.0, dtype=torch.float64, device="cuda")
+    db = torch.zeros(n, dtype=torch.float64, device="cuda")
+    dxe = torch.zeros(n, dtype=torch.float64, device="cuda")
+    G = hp.Matrix.generated(nx, ny, nz, dx, db, dxe)
+    assert G.nnz == A.nnz and G.nrow == n
+    r, c, v = G.download_csr()
+    assert np.array_equal(r, A.rowindex) and np.array_equal(c, A.colindex) and np.array_equal(v, A.values)
+    assert np.array_equal(db.cpu().numpy(), b)
+    assert np.array_equal(dx.cpu().numpy(), x) and np.array_equal(dxe.cpu().numpy(), xe)
+
+
+def test_invalid_csr_rejected(hp):
+    A, *_ = oracle.generate_matrix(3, 3, 3)
+    bad = A.colindex.copy()
+    bad[5] = 28  # column beyond nrow
+    with pytest.raises(hp.HpccgError) as e:
+        hp.Matrix.from_csr(A.rowindex, bad, A.values)
+    assert e.value.code == hp.HPCCG_ERR_INVALID_ARG
+    rows = A.rowindex.copy()
+    rows[3], rows[4] = rows[4], rows[3]  # non-monotone
+    with pytest.raises(hp.HpccgError):
+        hp.Matrix.from_csr(rows, A.colindex, A.values)
+
+
+SPMV_KINDS = [(1, 2), (1, 3), (1, 4), (1, 8), (2, 2), (2, 4), (2, 8)]
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(3, 5, 7), (16, 16, 16), (33, 17, 5), (64, 64, 64)])
+def test_spmv_bit_exact(hp, torch, nx, ny, nz):
+    A, *_ = oracle.generate_matrix(nx, ny, nz)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    rng = np.random.default_rng(11)
+    xv = rng.uniform(-1, 1, A.nrow)
+    want = oracle.spmv(A, xv)
+    dx = torch.from_numpy(xv).cuda()
+    dy = torch.empty_like(dx)
+    for kind, param in SPMV_KINDS:
+        M.set_spmv(kind, param)
+        dy.fill_(np.nan)
+        M.spmv(dx, dy)
+        assert np.array_equal(dy.cpu().numpy(), want), (kind, param)
+    for lpr in (4, 8, 16, 32):  # warp-per-row CSR reassociates the row sum
+        M.set_spmv(hp.SPMV_CSR_VECTOR, lpr)
+        M.spmv(dx, dy)
+        np.testing.assert_allclose(dy.cpu().numpy(), want, rtol=1e-13, atol=1e-13)
+
+
+def test_spmv_generic_csr_width(hp, torch):
+    """A CSR that is not the 27-point matrix (irregular rows, up to 40 per row)."""
+    rng = np.random.default_rng(3)
+    n = 5000
+    lens = rng.integers(0, 41, n)
+    rowindex = np.concatenate([[1], 1 + np.cumsum(lens)]).astype(np.int32)
+    cols = np.concatenate([np.sort(rng.choice(n, l, replace=False)) + 1 for l in lens]).astype(np.int32)
+    vals = rng.uniform(-2, 2, len(cols))
+    A = oracle.Matrix(n, 1, 1, rowindex, cols, vals, len(cols))
+    M = hp.Matrix.from_csr(rowindex, cols, vals)
+    xv = rng.uniform(-1, 1, n)
+    dx = torch.from_numpy(xv).cuda()
+    dy = torch.empty_like(dx)
+    M.spmv(dx, dy)  # width 40 > 32: CSR kernels only
+    np.testing.assert_allclose(dy.cpu().numpy(), oracle.spmv(A, xv), rtol=1e-13, atol=1e-13)
+
+
+def test_blas1(hp, torch):
+    A, *_ = oracle.generate_matrix(4, 4, 4)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    rng = np.random.default_rng(5)
+    for n in (1, 2, 7, 1000, 1 << 20, (1 << 20) + 3):
+        x = rng.uniform(-1, 1, n)
+        y = rng.uniform(-1, 1, n)
+        dx, dy = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+        assert M.ddot(dx, dy) == pytest.approx(oracle.ddot(x, y), rel=1e-13, abs=1e-13)
+        assert M.ddot1(dx) == pytest.approx(oracle.ddot1(x), rel=1e-13)
+        dw = torch.empty_like(dx)
+        M.waxpby(0.3, dx, -1.7, dy, dw)
+        assert np.array_equal(dw.cpu().numpy(), oracle.waxpby(0.3, x, -1.7, y))
+        w0 = rng.uniform(-1, 1, n)
+        dw = torch.from_numpy(w0.copy()).cuda()
+        M.wwpby(-0.25, dy, dw)
+        assert np.array_equal(dw.cpu().numpy(), oracle.wwpby(-0.25, y, w0))
+        dw = torch.from_numpy(w0.copy()).cuda()
+        M.wxbw(dx, 0.9, dw)
+        assert np.array_equal(dw.cpu().numpy(), oracle.wxbw(x, 0.9, w0))
+        M.vcopy(dx, dw)
+        assert np.array_equal(dw.cpu().numpy(), x)
+
+
+@pytest.mark.parametrize("key", ["16x16x16", "32x32x32", "3x5x7"])
+def test_cg_parity_150(hp, key):
+    nx, ny, nz = map(int, key.split("x"))
+    A, x, b, xe = oracle.generate_matrix(nx, ny, nz)
+    ref_x, ref_it, ref_normr, ref_hist = oracle.cg(A, b, x, 150, 0.0)
+    gold = np.load(os.path.join(GOLDEN, f"cg_{key}.npz"))
+    np.testing.assert_array_equal(ref_hist, gold["hist"])
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    gx = x.copy()
+    gx, it, normr, hist, status = M.cg(b, gx, 150, 0.0)
+    assert status == hp.HPCCG_OK and it == ref_it == 150
+    assert_history_parity(hist, ref_hist)
+    assert normr == pytest.approx(ref_normr, rel=1e-12, abs=1e-12 * ref_hist[0])
+    assert np.abs(gx - ref_x).max() <= 1e-10
+    assert np.abs(gx - xe).max() <= 1e-10
+
+
+@pytest.mark.parametrize("key", ["1x1x1", "2x2x2", "7x1x3"])
+def test_cg_exact_convergence_breakdown(hp, key):
+    """Tiny systems reach r = 0 exactly; the reference then divides 0/0 and
+    carries NaN to max_iter.  The C-ABI stops with HPCCG_ERR_BREAKDOWN and
+    returns the last finite iterate."""
+    nx, ny, nz = map(int, key.split("x"))
+    A, x, b, xe = oracle.generate_matrix(nx, ny, nz)
+    _, _, _, ref_hist = oracle.cg(A, b, x, 150, 0.0)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    gx = x.copy()
+    gx, it, normr, hist, status = M.cg(b, gx, 150, 0.0)
+    assert status in (hp.HPCCG_OK, hp.HPCCG_ERR_BREAKDOWN)
+    assert np.all(np.isfinite(gx)) and np.all(np.isfinite(hist))
+    assert_history_parity(hist, ref_hist)
+    assert np.abs(gx - 1.0).max() <= 1e-10
+
+
+def test_cg_zero_rhs(hp):
+    A, x, b, xe = oracle.generate_matrix(4, 4, 4)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    z = np.zeros_like(b)
+    gx = np.zeros_like(b)
+    gx, it, normr, hist, status = M.cg(z, gx, 150, 0.0)  # reference: 0/0 at k=1
+    assert status == hp.HPCCG_ERR_BREAKDOWN and it == 0 and np.all(gx == 0)
+    gx, it, normr, hist, status = M.cg(z, gx, 150, 1.0)  # normr = 0 < 1: converged at once
+    assert status == hp.HPCCG_OK and it == 0 and normr == 0.0
+
+
+def test_cg_tolerance_stop(hp):
+    A, x, b, xe = oracle.generate_matrix(32, 32, 32)
+    tol = 1e-8 * np.linalg.norm(b)
+    ref_x, ref_it, ref_normr, ref_hist = oracle.cg(A, b, x, 150, tol)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    gx, it, normr, hist, status = M.cg(b, x.copy(), 150, tol)
+    assert status == hp.HPCCG_OK
+    assert it == ref_it
+    assert normr == pytest.approx(ref_normr, rel=1e-12)
+    assert_history_parity(hist, ref_hist)
+    assert np.abs(gx - ref_x).max() <= 1e-10
+
+
+def test_cg_graph_eager_reproducible_and_kernel_independent(hp, monkeypatch):
+    A, x, b, xe = oracle.generate_matrix(20, 18, 16)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    runs = []
+    for kind, param in [(1, 4), (1, 4), (1, 2), (1, 8)]:
+        M.set_spmv(kind, param)
+        runs.append(M.cg(b, x.copy(), 150, 0.0))
+    monkeypatch.setenv("HPCCG_EAGER", "1")
+    M.set_spmv(1, 4)
+    runs.append(M.cg(b, x.copy(), 150, 0.0))
+    for r in runs[1:]:
+        assert np.array_equal(r[0], runs[0][0]) and np.array_equal(r[3], runs[0][3]) and r[1] == runs[0][1]
+
+
+def test_cg_device_arrays(hp, torch):
+    A, x, b, xe = oracle.generate_matrix(24, 24, 24)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    hx, it, normr, hist, status = M.cg(b, x.copy(), 60, 0.0)
+    db = torch.from_numpy(b).cuda()
+    dx = torch.zeros_like(db)
+    it2, normr2, hist2, status2 = M.cg_device(db, dx, 60, 0.0)
+    assert (it2, normr2, status2) == (it, normr, status)
+    assert np.array_equal(dx.cpu().numpy(), hx) and np.array_equal(hist2, hist)
+
+
+def test_cg_128_residual_history_and_solution(hp, torch):
+    """128^3 (2,097,152 rows, 55.7M nonzeros), 500 iterations on the GPU.  The
+    oracle's first 60 iterations pin the history; x -> 1 pins the end."""
+    n = 128
+    A, x, b, xe = oracle.generate_matrix(n, n, n)
+    assert A.nnz == 55742968
+    _, _, _, ref_hist = oracle.cg(A, b, x, 60, 0.0)
+    dx = torch.zeros(n ** 3, dtype=torch.float64, device="cuda")
+    db = torch.zeros_like(dx)
+    M = hp.Matrix.generated(n, n, n, dx, db, None)
+    assert np.array_equal(db.cpu().numpy(), b)
+    it, normr, hist, status = M.cg_device(db, dx, 500, 0.0)
+    assert status == hp.HPCCG_OK and it == 500
+    assert_history_parity(hist[:61], ref_hist)
+    assert np.abs(dx.cpu().numpy() - 1.0).max() <= 1e-10

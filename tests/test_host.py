@@ -1,0 +1,79 @@
+"""Host-side checks that need no GPU: the product's host generator, the C-ABI
+surface of libhpccg_b200.so, and the driver build."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import PKG, ROOT, gpu_available
+
+import hpccg_b200 as hp
+
+HEADER = os.path.join(ROOT, "include", "hpccg_gpu.h")
+
+
+def _declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(hpccg_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(hp.LIB_PATH)
+    declared = _declared_functions()
+    assert len(declared) >= 15
+    for name in declared:
+        assert hasattr(lib, name), name
+    nm = subprocess.run(["nm", "-D", "--defined-only", hp.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (hpccg_\w+)", nm))
+    assert set(declared) <= exported
+    assert set(hp.exported_symbols()) <= set(declared)
+
+
+def test_library_is_sm100a_only():
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", hp.LIB_PATH], capture_output=True,
+                         text=True).stdout
+    archs = set(re.findall(r"sm_(\d+a?)", out))
+    assert archs == {"100a"}, archs
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(1, 1, 1), (2, 1, 1), (1, 2, 3), (3, 5, 7), (4, 4, 4), (7, 1, 3),
+                                      (16, 16, 16), (9, 2, 11), (33, 17, 5)])
+def test_host_generator_bit_exact(nx, ny, nz):
+    A, x, b, xe = oracle.generate_matrix(nx, ny, nz)
+    rowindex, colindex, values, hx, hb, hxe = hp.generate_matrix(nx, ny, nz)
+    assert np.array_equal(rowindex, A.rowindex)
+    assert np.array_equal(colindex, A.colindex)
+    assert np.array_equal(values, A.values)
+    assert np.array_equal(hb, b) and np.array_equal(hx, x) and np.array_equal(hxe, xe)
+
+
+def test_host_generator_rejects_bad_sizes():
+    with pytest.raises(hp.HpccgError) as e:
+        hp.generate_matrix(0, 4, 4)
+    assert e.value.code == hp.HPCCG_ERR_INVALID_ARG
+
+
+def test_strerror_names():
+    assert hp.strerror(hp.HPCCG_OK) == "ok"
+    assert "breakdown" in hp.strerror(hp.HPCCG_ERR_BREAKDOWN)
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU error path")
+def test_create_without_gpu_fails_cleanly():
+    rowindex, colindex, values, *_ = hp.generate_matrix(3, 3, 3)
+    with pytest.raises(hp.HpccgError) as e:
+        hp.Matrix.from_csr(rowindex, colindex, values)
+    assert e.value.code == hp.HPCCG_ERR_NO_DEVICE
+
+
+def test_driver_built_and_prints_usage():
+    exe = os.path.join(PKG, "HPCCG-B200")
+    if not os.path.exists(exe):
+        subprocess.run(["make", "-s", "-C", PKG], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0 and "USAGE" in out.stdout
