@@ -151,5 +151,6 @@ inline Reduction reduction_of(const hpccg_ctx *c) { return Reduction{c->d_partia
 int launch_spmv(hpccg_ctx *c, const double *x, double *y, cudaStream_t s);
 int autotune_spmv(hpccg_ctx *c);
 int ensure_workspace(hpccg_ctx *c, int32_t hist_cap);
+void release_mixed(const hpccg_ctx *c);
 
 }  // namespace hpccg

@@ -252,6 +252,7 @@ extern "C" int hpccg_generate_matrix(int32_t nx, int32_t ny, int32_t nz, int32_t
 
 extern "C" void hpccg_gpu_destroy(hpccg_ctx *c) {
   if (!c) return;
+  release_mixed(c);
   if (c->cg_exec) cudaGraphExecDestroy(c->cg_exec);
   if (c->cg_graph) cudaGraphDestroy(c->cg_graph);
   void *bufs[] = {c->d_rowptr, c->d_col, c->d_val, c->d_ell_col, c->d_ell_val, c->d_r, c->d_p,

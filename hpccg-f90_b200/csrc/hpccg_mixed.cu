@@ -1,0 +1,681 @@
+// hpccg_mixed.cu -- FP64 iterative refinement around an FP32 / BF16-value inner CG.
+//
+// Outer loop (FP64, on the device):  r = b - A x (FP64 values, the bit-exact
+// reference SpMV), stop when ||r|| <= rel_tol ||b||; otherwise solve A d = r/||r||
+// approximately with the inner CG and update x += ||r|| d in FP64.
+// Inner CG (FP32 vectors; FP32 or BF16 copies of A's values; FP32 row sums;
+// FP64 dot-product accumulation) stops at ||r_in|| <= target ||r_in,0|| where
+// target = inner_rtol, or adaptively max(floor, 0.5 rel_tol ||b|| / ||r||).
+// The FP64 true residual is the judge: the solve only reports success when
+// the FP64 residual meets rel_tol.
+//
+// One CUDA graph: bnorm, residual64, while(outer){ start_inner,
+// while(inner){ P, A, B }, end_inner, residual64 }.
+#include <stdlib.h>
+
+#include <algorithm>
+#include <type_traits>
+
+#include "hpccg_rows.cuh"
+#include "hpccg_rows_lp.cuh"
+
+namespace hpccg {
+
+struct MixedState {
+  double bb, rr64, scale, rel_tol, relres, target, inner_rtol, inner_floor;
+  double rtrans, rr0, alpha, beta;
+  int outer, max_outer, inner_k, max_inner, inner_total, status, pending, inner_break;
+  int cont_outer, cont_inner, pad[2];
+};
+
+struct MixedArgs {
+  int n, npad;
+  const double *b;
+  double *x, *r64;
+  float *r, *p, *Ap, *d;
+  const int32_t *ell_col;
+  const void *val_lp;
+  MixedState *st;
+  Reduction red;
+  cudaGraphConditionalHandle cond_outer, cond_inner;
+  int use_cond;
+};
+
+__device__ __forceinline__ void set_outer(const MixedArgs &g, int v) {
+  g.st->cont_outer = v;
+  if (g.use_cond) cudaGraphSetConditional(g.cond_outer, (unsigned)v);
+}
+__device__ __forceinline__ void set_inner(const MixedArgs &g, int v) {
+  g.st->cont_inner = v;
+  if (g.use_cond) cudaGraphSetConditional(g.cond_inner, (unsigned)v);
+}
+
+__global__ void __launch_bounds__(kBlock) k_mp_bnorm(MixedArgs g) {
+  __shared__ double smem[32];
+  double part = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+    const double bi = g.b[i];
+    part = __dadd_rn(part, __dmul_rn(bi, bi));
+  }
+  const double tot = block_sum<kBlock>(part, smem);
+  if (arrive_last(g.red, tot)) {
+    const double bb = finish_sum<kBlock>(g.red, smem);
+    if (threadIdx.x == 0) {
+      g.st->bb = bb;
+      g.st->outer = 0;
+      g.st->inner_total = 0;
+      g.st->status = HPCCG_OK;
+    }
+  }
+}
+
+// r64 = b - A x64 (FP64, reference order) and the outer decision.
+template <class S>
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_residual64(SpmvArgs a, MixedArgs g) {
+  __shared__ double smem[32];
+  EpiResidual epi{g.b, g.r64};
+  const double part = S::rows(a, g.x, epi);
+  const double tot = block_sum<kBlock>(part, smem);
+  if (arrive_last(g.red, tot)) {
+    const double rr = finish_sum<kBlock>(g.red, smem);
+    if (threadIdx.x == 0) {
+      MixedState &st = *g.st;
+      st.rr64 = rr;
+      st.relres = st.bb > 0.0 ? sqrt(rr / st.bb) : 0.0;
+      int cont = (st.relres > st.rel_tol) && (st.outer < st.max_outer);
+      if (!isfinite(st.relres)) {
+        st.status = HPCCG_ERR_BREAKDOWN;
+        cont = 0;
+      }
+      if (cont) {
+        st.scale = sqrt(rr);
+        st.target = st.inner_rtol > 0.0 ? st.inner_rtol
+                                        : fmax(st.inner_floor, 0.5 * st.rel_tol / st.relres);
+        st.outer += 1;
+      }
+      set_outer(g, cont);
+    }
+  }
+}
+
+// r32 = r64 / ||r64||, d = 0, rr0 = ||r32||^2.
+__global__ void __launch_bounds__(kBlock) k_mp_start_inner(MixedArgs g) {
+  __shared__ double smem[32];
+  const double inv = 1.0 / g.st->scale;
+  double part = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+    const float ri = (float)(g.r64[i] * inv);
+    g.r[i] = ri;
+    g.d[i] = 0.f;
+    part += (double)ri * (double)ri;
+  }
+  const double tot = block_sum<kBlock>(part, smem);
+  if (arrive_last(g.red, tot)) {
+    const double rr = finish_sum<kBlock>(g.red, smem);
+    if (threadIdx.x == 0) {
+      MixedState &st = *g.st;
+      st.rtrans = rr;
+      st.rr0 = rr;
+      st.inner_k = 0;
+      st.pending = 0;
+      st.inner_break = 0;
+      set_inner(g, rr > 0.0 && st.max_inner > 0);
+    }
+  }
+}
+
+// p = r (first) or d += alpha p (deferred), p = r + beta p.
+__global__ void __launch_bounds__(kBlock) k_mp_update_p(MixedArgs g) {
+  const MixedState *st = g.st;
+  const int n4 = g.n >> 2;
+  const int stride = gridDim.x * blockDim.x;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  float4 *p4 = reinterpret_cast<float4 *>(g.p);
+  const float4 *r4 = reinterpret_cast<const float4 *>(g.r);
+  float4 *d4 = reinterpret_cast<float4 *>(g.d);
+  if (st->inner_k == 0) {
+    for (int i = tid; i < n4; i += stride) p4[i] = __ldcs(r4 + i);
+    for (int i = 4 * n4 + tid; i < g.n; i += stride) g.p[i] = g.r[i];
+    return;
+  }
+  const float alpha = (float)st->alpha, beta = (float)st->beta;
+  const int pend = st->pending;
+  for (int i = tid; i < n4; i += stride) {
+    float4 pi = p4[i];
+    const float4 ri = __ldcs(r4 + i);
+    if (pend) {
+      float4 di = __ldcs(d4 + i);
+      di.x = fmaf(alpha, pi.x, di.x);
+      di.y = fmaf(alpha, pi.y, di.y);
+      di.z = fmaf(alpha, pi.z, di.z);
+      di.w = fmaf(alpha, pi.w, di.w);
+      __stcs(d4 + i, di);
+    }
+    pi.x = fmaf(beta, pi.x, ri.x);
+    pi.y = fmaf(beta, pi.y, ri.y);
+    pi.z = fmaf(beta, pi.z, ri.z);
+    pi.w = fmaf(beta, pi.w, ri.w);
+    p4[i] = pi;
+  }
+  for (int i = 4 * n4 + tid; i < g.n; i += stride) {
+    const float pi = g.p[i];
+    if (pend) g.d[i] = fmaf(alpha, pi, g.d[i]);
+    g.p[i] = fmaf(beta, pi, g.r[i]);
+  }
+}
+
+struct EpiDot32 {
+  const float *p;
+  float *y;
+  __device__ __forceinline__ double operator()(int i, float s) const {
+    y[i] = s;
+    return (double)__ldg(p + i) * (double)s;
+  }
+};
+
+// Ap = A p with low-precision values, alpha = rtrans / p.Ap.
+template <class S, typename VT>
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_spmv_dot(MixedArgs g) {
+  __shared__ double smem[32];
+  EpiDot32 epi{g.p, g.Ap};
+  const double part = S::rows(g.n, g.npad, g.ell_col, reinterpret_cast<const VT *>(g.val_lp), g.p, epi);
+  const double tot = block_sum<kBlock>(part, smem);
+  if (arrive_last(g.red, tot)) {
+    const double pAp = finish_sum<kBlock>(g.red, smem);
+    if (threadIdx.x == 0) {
+      MixedState &st = *g.st;
+      st.pending = 0;
+      const double alpha = st.rtrans / pAp;
+      if (!(pAp > 0.0) || !isfinite(alpha)) {
+        st.inner_break = 1;
+        st.alpha = 0.0;
+      } else {
+        st.alpha = alpha;
+      }
+    }
+  }
+}
+
+// r -= alpha Ap, rr, inner stop test.
+__global__ void __launch_bounds__(kBlock) k_mp_update_r(MixedArgs g) {
+  __shared__ double smem[32];
+  if (g.st->inner_break) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_inner(g, 0);
+    return;
+  }
+  const float nalpha = -(float)g.st->alpha;
+  const int n4 = g.n >> 2;
+  const int stride = gridDim.x * blockDim.x;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  float4 *r4 = reinterpret_cast<float4 *>(g.r);
+  const float4 *a4 = reinterpret_cast<const float4 *>(g.Ap);
+  double part = 0.0;
+  for (int i = tid; i < n4; i += stride) {
+    float4 ri = r4[i];
+    const float4 ai = __ldcs(a4 + i);
+    ri.x = fmaf(nalpha, ai.x, ri.x);
+    ri.y = fmaf(nalpha, ai.y, ri.y);
+    ri.z = fmaf(nalpha, ai.z, ri.z);
+    ri.w = fmaf(nalpha, ai.w, ri.w);
+    r4[i] = ri;
+    part += (double)ri.x * ri.x + (double)ri.y * ri.y + (double)ri.z * ri.z + (double)ri.w * ri.w;
+  }
+  for (int i = 4 * n4 + tid; i < g.n; i += stride) {
+    const float ri = fmaf(nalpha, g.Ap[i], g.r[i]);
+    g.r[i] = ri;
+    part += (double)ri * ri;
+  }
+  const double tot = block_sum<kBlock>(part, smem);
+  if (arrive_last(g.red, tot)) {
+    const double rr = finish_sum<kBlock>(g.red, smem);
+    if (threadIdx.x == 0) {
+      MixedState &st = *g.st;
+      st.inner_k += 1;
+      st.inner_total += 1;
+      st.pending = 1;
+      st.beta = rr / st.rtrans;
+      st.rtrans = rr;
+      const int cont = isfinite(rr) && (rr > st.target * st.target * st.rr0) && (st.inner_k < st.max_inner);
+      set_inner(g, cont);
+    }
+  }
+}
+
+// d += alpha p (pending), x64 += ||r64|| d.
+__global__ void __launch_bounds__(kBlock) k_mp_end_inner(MixedArgs g) {
+  const MixedState *st = g.st;
+  const float alpha = st->pending ? (float)st->alpha : 0.f;
+  const double scale = st->scale;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+    const float di = fmaf(alpha, g.p[i], g.d[i]);
+    g.x[i] = fma(scale, (double)di, g.x[i]);
+  }
+}
+
+// Plain low-precision y = A x for tests and timing.
+struct EpiStore32 {
+  float *y;
+  __device__ __forceinline__ double operator()(int i, float s) const {
+    y[i] = s;
+    return 0.0;
+  }
+};
+template <class S, typename VT>
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_spmv_lp(int n, int npad, const int32_t *col,
+                                                                   const VT *val, const float *x, float *y) {
+  EpiStore32 epi{y};
+  S::rows(n, npad, col, val, x, epi);
+}
+
+__global__ void k_to_lp(const double *src, float *f32, __nv_bfloat16 *b16, size_t count) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+    const double v = src[i];
+    if (f32) f32[i] = (float)v;
+    if (b16) b16[i] = __double2bfloat16(v);
+  }
+}
+
+// Low-precision strategy dispatch: value type by precision, RPT and MINB by param.
+template <class F>
+inline int dispatch_lp(int precision, int rpt, F &&f) {
+  if (precision == 1) {
+    switch (rpt) {
+      case 1: return f(StratLp<float, 1, 4>{}, (float *)nullptr);
+      case 4: return f(StratLp<float, 4, 2>{}, (float *)nullptr);
+      default: return f(StratLp<float, 2, 2>{}, (float *)nullptr);
+    }
+  }
+  switch (rpt) {
+    case 1: return f(StratLp<__nv_bfloat16, 1, 4>{}, (__nv_bfloat16 *)nullptr);
+    case 2: return f(StratLp<__nv_bfloat16, 2, 2>{}, (__nv_bfloat16 *)nullptr);
+    default: return f(StratLp<__nv_bfloat16, 4, 2>{}, (__nv_bfloat16 *)nullptr);
+  }
+}
+
+}  // namespace hpccg
+
+using namespace hpccg;
+
+// Per-context mixed-precision resources, kept beside the context.
+struct MixedRes {
+  float *r = nullptr, *p = nullptr, *Ap = nullptr, *d = nullptr, *x32 = nullptr, *y32 = nullptr;
+  float *val32 = nullptr;
+  __nv_bfloat16 *val16 = nullptr;
+  int32_t *col27 = nullptr;  // ELL columns padded to width 27 when the FP64 ELL is narrower
+  MixedState *st = nullptr;
+  cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+  int exec_rpt[3] = {0, 0, 0};
+  int rpt[3] = {0, 2, 4};  // rows per thread per precision (index 1 = FP32, 2 = BF16)
+};
+
+#include <map>
+#include <mutex>
+static std::mutex g_mixed_mu;
+static std::map<const hpccg_ctx *, MixedRes *> g_mixed;
+
+namespace hpccg {
+void release_mixed(const hpccg_ctx *c) {
+  std::lock_guard<std::mutex> lk(g_mixed_mu);
+  auto it = g_mixed.find(c);
+  if (it == g_mixed.end()) return;
+  MixedRes *m = it->second;
+  for (auto &e : m->exec)
+    if (e) cudaGraphExecDestroy(e);
+  void *bufs[] = {m->r, m->p, m->Ap, m->d, m->x32, m->y32, m->val32, m->val16, m->col27, m->st};
+  for (void *b : bufs)
+    if (b) cudaFree(b);
+  delete m;
+  g_mixed.erase(it);
+}
+}  // namespace hpccg
+
+__global__ void k_pad_cols27(const int32_t *src, int W, int npad, int32_t *dst) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)npad; i += (size_t)gridDim.x * blockDim.x)
+    for (int k = 0; k < 27; ++k) dst[(size_t)k * npad + i] = k < W ? src[(size_t)k * npad + i] : (int32_t)i;
+}
+__global__ void k_pad_vals27(const double *src, int W, int npad, double *dst) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)npad; i += (size_t)gridDim.x * blockDim.x)
+    for (int k = 0; k < 27; ++k) dst[(size_t)k * npad + i] = k < W ? src[(size_t)k * npad + i] : 0.0;
+}
+
+static int mixed_res(hpccg_ctx *c, int precision, MixedRes **out) {
+  if (!c->d_ell_col || c->ell_width > 27) return HPCCG_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lk(g_mixed_mu);
+  MixedRes *&m = g_mixed[c];
+  if (!m) {
+    m = new MixedRes();
+    const size_t vec = sizeof(float) * (size_t)c->npad;
+    HPCCG_CUDA(cudaMalloc(&m->r, vec));
+    HPCCG_CUDA(cudaMalloc(&m->p, vec));
+    HPCCG_CUDA(cudaMalloc(&m->Ap, vec));
+    HPCCG_CUDA(cudaMalloc(&m->d, vec));
+    HPCCG_CUDA(cudaMemset(m->p, 0, vec));
+    HPCCG_CUDA(cudaMalloc(&m->st, sizeof(MixedState)));
+  }
+  const size_t slots = (size_t)27 * c->npad;
+  const double *src = c->d_ell_val;
+  double *tmp = nullptr;
+  if ((precision == 1 && !m->val32) || (precision == 2 && !m->val16) || (!m->col27 && c->ell_width != 27)) {
+    if (c->ell_width != 27) {
+      HPCCG_CUDA(cudaMalloc(&tmp, sizeof(double) * slots));
+      k_pad_vals27<<<c->num_sms * 8, kBlock, 0, c->stream>>>(c->d_ell_val, c->ell_width, c->npad, tmp);
+      src = tmp;
+      if (!m->col27) {
+        HPCCG_CUDA(cudaMalloc(&m->col27, sizeof(int32_t) * slots));
+        k_pad_cols27<<<c->num_sms * 8, kBlock, 0, c->stream>>>(c->d_ell_col, c->ell_width, c->npad, m->col27);
+      }
+    }
+    if (precision == 1 && !m->val32) {
+      HPCCG_CUDA(cudaMalloc(&m->val32, sizeof(float) * slots));
+      k_to_lp<<<c->num_sms * 8, kBlock, 0, c->stream>>>(src, m->val32, nullptr, slots);
+    }
+    if (precision == 2 && !m->val16) {
+      HPCCG_CUDA(cudaMalloc(&m->val16, sizeof(__nv_bfloat16) * slots));
+      k_to_lp<<<c->num_sms * 8, kBlock, 0, c->stream>>>(src, nullptr, m->val16, slots);
+    }
+    HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+    if (tmp) cudaFree(tmp);
+    HPCCG_CUDA(cudaGetLastError());
+  }
+  *out = m;
+  return HPCCG_OK;
+}
+
+static MixedArgs mixed_args(hpccg_ctx *c, MixedRes *m, int precision) {
+  MixedArgs g{};
+  g.n = c->nrow;
+  g.npad = c->npad;
+  g.b = c->d_b;
+  g.x = c->d_x;
+  g.r64 = c->d_r;
+  g.r = m->r;
+  g.p = m->p;
+  g.Ap = m->Ap;
+  g.d = m->d;
+  g.ell_col = m->col27 ? m->col27 : c->d_ell_col;
+  g.val_lp = precision == 1 ? (const void *)m->val32 : (const void *)m->val16;
+  g.st = m->st;
+  g.red = reduction_of(c);
+  return g;
+}
+
+static int launch_inner_body(hpccg_ctx *c, MixedRes *m, int precision, const MixedArgs &g, cudaStream_t s) {
+  k_mp_update_p<<<c->grid, kBlock, 0, s>>>(g);
+  int rc = dispatch_lp(precision, m->rpt[precision], [&](auto strat, auto *vt) {
+    using St = decltype(strat);
+    using VT = std::remove_pointer_t<decltype(vt)>;
+    k_mp_spmv_dot<St, VT><<<c->grid, kBlock, 0, s>>>(g);
+    return (int)cudaGetLastError();
+  });
+  if (rc) return rc;
+  k_mp_update_r<<<c->grid, kBlock, 0, s>>>(g);
+  return (int)cudaGetLastError();
+}
+
+static int launch_residual64(hpccg_ctx *c, const MixedArgs &g, cudaStream_t s) {
+  const SpmvArgs a = spmv_args(c);
+  return dispatch_strategy(a, [&](auto strat) {
+    using St = decltype(strat);
+    k_mp_residual64<St><<<c->grid, kBlock, 0, s>>>(a, g);
+    return (int)cudaGetLastError();
+  });
+}
+
+// Adds a while node at the capture point of `s` and captures `body` into it.
+template <class Body>
+static cudaError_t capture_while(cudaStream_t s, cudaGraphConditionalHandle h, Body &&body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &ndeps);
+  if (e != cudaSuccess) return e;
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  e = cudaGraphAddNode(&node, g, deps, ndeps, &cp);
+  if (e != cudaSuccess) return e;
+  cudaStream_t bs = nullptr;
+  e = cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return e;
+  cudaGraph_t bg = cp.conditional.phGraph_out[0];
+  e = cudaStreamBeginCaptureToGraph(bs, bg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    const cudaError_t e1 = body(bs, bg);
+    const cudaError_t e2 = cudaStreamEndCapture(bs, &bg);
+    e = e1 != cudaSuccess ? e1 : e2;
+  }
+  cudaStreamDestroy(bs);
+  if (e != cudaSuccess) return e;
+  return cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+static int build_mixed_graph(hpccg_ctx *c, MixedRes *m, int precision) {
+  if (m->exec[precision]) {
+    cudaGraphExecDestroy(m->exec[precision]);
+    m->exec[precision] = nullptr;
+  }
+  cudaStream_t s = c->stream;
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  cudaGraphConditionalHandle ho = 0;
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &ndeps);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&ho, g, 0, cudaGraphCondAssignDefault);
+  MixedArgs ga = mixed_args(c, m, precision);
+  ga.cond_outer = ho;
+  ga.use_cond = 1;
+  if (e == cudaSuccess) {
+    k_mp_bnorm<<<c->grid, kBlock, 0, s>>>(ga);
+    e = (cudaError_t)launch_residual64(c, ga, s);
+  }
+  if (e == cudaSuccess)
+    e = capture_while(s, ho, [&](cudaStream_t os, cudaGraph_t og) -> cudaError_t {
+      cudaGraphConditionalHandle hi = 0;
+      cudaError_t ee = cudaGraphConditionalHandleCreate(&hi, og, 0, 0);
+      if (ee != cudaSuccess) return ee;
+      MixedArgs gi = ga;
+      gi.cond_inner = hi;
+      k_mp_start_inner<<<c->grid, kBlock, 0, os>>>(gi);
+      ee = cudaGetLastError();
+      if (ee == cudaSuccess)
+        ee = capture_while(os, hi, [&](cudaStream_t is, cudaGraph_t) -> cudaError_t {
+          return (cudaError_t)launch_inner_body(c, m, precision, gi, is);
+        });
+      if (ee == cudaSuccess) {
+        k_mp_end_inner<<<c->grid, kBlock, 0, os>>>(gi);
+        ee = cudaGetLastError();
+      }
+      if (ee == cudaSuccess) ee = (cudaError_t)launch_residual64(c, gi, os);
+      return ee;
+    });
+  cudaGraph_t out = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(s, &out);
+  if (e == cudaSuccess) e = ee;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&m->exec[precision], out, 0);
+  if (out) cudaGraphDestroy(out);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_cuda_error(e, "build mixed graph", __FILE__, __LINE__);
+  }
+  m->exec_rpt[precision] = m->rpt[precision];
+  return HPCCG_OK;
+}
+
+static int run_mixed_eager(hpccg_ctx *c, MixedRes *m, int precision) {
+  MixedArgs g = mixed_args(c, m, precision);
+  g.use_cond = 0;
+  k_mp_bnorm<<<c->grid, kBlock, 0, c->stream>>>(g);
+  int rc = launch_residual64(c, g, c->stream);
+  if (rc) return set_cuda_error((cudaError_t)rc, "residual64", __FILE__, __LINE__);
+  for (;;) {
+    int cont = 0;
+    HPCCG_CUDA(cudaMemcpyAsync(&cont, &m->st->cont_outer, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+    if (!cont) break;
+    k_mp_start_inner<<<c->grid, kBlock, 0, c->stream>>>(g);
+    for (;;) {
+      int ci = 0;
+      HPCCG_CUDA(cudaMemcpyAsync(&ci, &m->st->cont_inner, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+      if (!ci) break;
+      rc = launch_inner_body(c, m, precision, g, c->stream);
+      if (rc) return set_cuda_error((cudaError_t)rc, "inner", __FILE__, __LINE__);
+    }
+    k_mp_end_inner<<<c->grid, kBlock, 0, c->stream>>>(g);
+    rc = launch_residual64(c, g, c->stream);
+    if (rc) return set_cuda_error((cudaError_t)rc, "residual64", __FILE__, __LINE__);
+  }
+  return HPCCG_OK;
+}
+
+extern "C" int hpccg_gpu_set_mixed_rows_per_thread(hpccg_ctx *c, int32_t precision, int32_t rpt) {
+  if (!c || (precision != HPCCG_PREC_FP32 && precision != HPCCG_PREC_BF16)) return HPCCG_ERR_INVALID_ARG;
+  if (rpt != 1 && rpt != 2 && rpt != 4) return HPCCG_ERR_INVALID_ARG;
+  MixedRes *m = nullptr;
+  int rc = mixed_res(c, precision, &m);
+  if (rc) return rc;
+  m->rpt[precision] = rpt;
+  return HPCCG_OK;
+}
+
+static int solve_mixed_common(hpccg_ctx *c, int precision, double rel_tol, int32_t max_outer,
+                              int32_t max_inner, double inner_rtol, hpccg_mixed_info *info) {
+  MixedRes *m = nullptr;
+  int rc = mixed_res(c, precision, &m);
+  if (rc) return rc;
+  if ((rc = autotune_spmv(c))) return rc;
+  MixedState h0 = {};
+  h0.rel_tol = rel_tol;
+  h0.max_outer = max_outer;
+  h0.max_inner = max_inner;
+  h0.inner_rtol = inner_rtol;
+  h0.inner_floor = 1e-5;
+  HPCCG_CUDA(cudaMemcpyAsync(m->st, &h0, sizeof(MixedState), cudaMemcpyHostToDevice, c->stream));
+  HPCCG_CUDA(cudaEventRecord(c->solve0, c->stream));
+  const bool eager = getenv("HPCCG_EAGER") && atoi(getenv("HPCCG_EAGER")) != 0;
+  if (eager) {
+    if ((rc = run_mixed_eager(c, m, precision))) return rc;
+  } else {
+    if (!m->exec[precision] || m->exec_rpt[precision] != m->rpt[precision])
+      if ((rc = build_mixed_graph(c, m, precision))) return rc;
+    HPCCG_CUDA(cudaGraphLaunch(m->exec[precision], c->stream));
+  }
+  HPCCG_CUDA(cudaEventRecord(c->solve1, c->stream));
+  MixedState hs;
+  HPCCG_CUDA(cudaMemcpyAsync(&hs, m->st, sizeof(MixedState), cudaMemcpyDeviceToHost, c->stream));
+  HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+  HPCCG_CUDA(cudaEventElapsedTime(&c->last_solve_ms, c->solve0, c->solve1));
+  if (info) {
+    info->outer_iters = hs.outer;
+    info->inner_iters = hs.inner_total;
+    info->relres = hs.relres;
+    info->status = hs.status;
+  }
+  if (hs.status) return hs.status;
+  return hs.relres <= rel_tol ? HPCCG_OK : HPCCG_ERR_NOT_CONVERGED;
+}
+
+static bool prec_ok(int p) { return p == HPCCG_PREC_FP32 || p == HPCCG_PREC_BF16; }
+
+extern "C" int hpccg_gpu_solve_mixed_device(hpccg_ctx *c, const double *d_b, double *d_x, int32_t precision,
+                                            double rel_tol, int32_t max_outer, int32_t max_inner,
+                                            double inner_rtol, hpccg_mixed_info *info) {
+  if (!c || !d_b || !d_x || !prec_ok(precision) || !(rel_tol >= 0.0) || max_outer < 0 || max_inner < 0 ||
+      !(inner_rtol >= 0.0) || inner_rtol >= 1.0)
+    return HPCCG_ERR_INVALID_ARG;
+  const size_t bytes = sizeof(double) * (size_t)c->nrow;
+  HPCCG_CUDA(cudaMemcpyAsync(c->d_b, d_b, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  HPCCG_CUDA(cudaMemcpyAsync(c->d_x, d_x, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  const int rc = solve_mixed_common(c, precision, rel_tol, max_outer, max_inner, inner_rtol, info);
+  if (rc != HPCCG_OK && rc != HPCCG_ERR_NOT_CONVERGED && rc != HPCCG_ERR_BREAKDOWN) return rc;
+  HPCCG_CUDA(cudaMemcpyAsync(d_x, c->d_x, bytes, cudaMemcpyDeviceToDevice, c->stream));
+  HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
+extern "C" int hpccg_gpu_solve_mixed(hpccg_ctx *c, const double *b, double *x, int32_t precision,
+                                     double rel_tol, int32_t max_outer, int32_t max_inner, double inner_rtol,
+                                     hpccg_mixed_info *info) {
+  if (!c || !b || !x || !prec_ok(precision) || !(rel_tol >= 0.0) || max_outer < 0 || max_inner < 0 ||
+      !(inner_rtol >= 0.0) || inner_rtol >= 1.0)
+    return HPCCG_ERR_INVALID_ARG;
+  const size_t bytes = sizeof(double) * (size_t)c->nrow;
+  HPCCG_CUDA(cudaMemcpyAsync(c->d_b, b, bytes, cudaMemcpyHostToDevice, c->stream));
+  HPCCG_CUDA(cudaMemcpyAsync(c->d_x, x, bytes, cudaMemcpyHostToDevice, c->stream));
+  const int rc = solve_mixed_common(c, precision, rel_tol, max_outer, max_inner, inner_rtol, info);
+  if (rc != HPCCG_OK && rc != HPCCG_ERR_NOT_CONVERGED && rc != HPCCG_ERR_BREAKDOWN) return rc;
+  HPCCG_CUDA(cudaMemcpyAsync(x, c->d_x, bytes, cudaMemcpyDeviceToHost, c->stream));
+  HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
+extern "C" int hpccg_gpu_spmv_lowp(hpccg_ctx *c, int32_t precision, const float *d_x, float *d_y) {
+  if (!c || !prec_ok(precision) || !d_x || !d_y || d_x == d_y) return HPCCG_ERR_INVALID_ARG;
+  MixedRes *m = nullptr;
+  int rc = mixed_res(c, precision, &m);
+  if (rc) return rc;
+  const int32_t *col = m->col27 ? m->col27 : c->d_ell_col;
+  const void *val = precision == 1 ? (const void *)m->val32 : (const void *)m->val16;
+  rc = dispatch_lp(precision, m->rpt[precision], [&](auto strat, auto *vt) {
+    using St = decltype(strat);
+    using VT = std::remove_pointer_t<decltype(vt)>;
+    k_spmv_lp<St, VT><<<c->grid, kBlock, 0, c->stream>>>(c->nrow, c->npad, col, (const VT *)val, d_x, d_y);
+    return (int)cudaGetLastError();
+  });
+  if (rc) return set_cuda_error((cudaError_t)rc, "spmv_lowp", __FILE__, __LINE__);
+  HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+  return HPCCG_OK;
+}
+
+extern "C" int hpccg_gpu_time_mixed_kernels(hpccg_ctx *c, int32_t precision, int32_t reps, float *ms) {
+  if (!c || !prec_ok(precision) || reps < 1 || !ms) return HPCCG_ERR_INVALID_ARG;
+  MixedRes *m = nullptr;
+  int rc = mixed_res(c, precision, &m);
+  if (rc) return rc;
+  const size_t vec = sizeof(float) * (size_t)c->npad;
+  HPCCG_CUDA(cudaMemsetAsync(m->p, 0, vec, c->stream));
+  HPCCG_CUDA(cudaMemsetAsync(m->r, 0, vec, c->stream));
+  HPCCG_CUDA(cudaMemsetAsync(m->d, 0, vec, c->stream));
+  MixedState h0 = {};
+  h0.inner_k = 1;
+  h0.rtrans = 1.0;
+  h0.alpha = 0.5;
+  h0.beta = 0.5;
+  h0.pending = 1;
+  h0.max_inner = 1 << 30;
+  h0.rr0 = 1.0;
+  HPCCG_CUDA(cudaMemcpyAsync(m->st, &h0, sizeof(MixedState), cudaMemcpyHostToDevice, c->stream));
+  MixedArgs g = mixed_args(c, m, precision);
+  g.use_cond = 0;
+  for (int which = 0; which < 3; ++which) {
+    for (int rep = -1; rep < reps; ++rep) {
+      if (rep == 0) HPCCG_CUDA(cudaEventRecord(c->ev0, c->stream));
+      HPCCG_CUDA(cudaMemsetAsync(&m->st->inner_break, 0, sizeof(int), c->stream));
+      if (which == 0) {
+        k_mp_update_p<<<c->grid, kBlock, 0, c->stream>>>(g);
+      } else if (which == 1) {
+        dispatch_lp(precision, m->rpt[precision], [&](auto strat, auto *vt) {
+          using St = decltype(strat);
+          using VT = std::remove_pointer_t<decltype(vt)>;
+          k_mp_spmv_dot<St, VT><<<c->grid, kBlock, 0, c->stream>>>(g);
+          return 0;
+        });
+      } else {
+        k_mp_update_r<<<c->grid, kBlock, 0, c->stream>>>(g);
+      }
+      HPCCG_CUDA(cudaGetLastError());
+    }
+    HPCCG_CUDA(cudaEventRecord(c->ev1, c->stream));
+    HPCCG_CUDA(cudaEventSynchronize(c->ev1));
+    float t = 0.f;
+    HPCCG_CUDA(cudaEventElapsedTime(&t, c->ev0, c->ev1));
+    ms[which] = t / (float)reps;
+  }
+  return HPCCG_OK;
+}

@@ -30,6 +30,13 @@ HPCCG_ERR_UNSUPPORTED = 7
 HPCCG_ERR_NO_DEVICE = 8
 
 SPMV_AUTO, SPMV_ELL, SPMV_ELL2, SPMV_CSR_VECTOR = 0, 1, 2, 3
+PREC_FP64, PREC_FP32, PREC_BF16 = 0, 1, 2
+
+
+class MixedInfo(ctypes.Structure):
+    """hpccg_mixed_info: refinement cycles, inner iterations, FP64 relres, status."""
+    _fields_ = [("outer_iters", ctypes.c_int32), ("inner_iters", ctypes.c_int32), ("relres", ctypes.c_double),
+                ("status", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class HpccgError(RuntimeError):
@@ -74,6 +81,11 @@ _SIGS = {
     "hpccg_gpu_uniform_pm1": (_c.c_int, [_vp, _c.c_uint64, _i64, _i64, _vp]),
     "hpccg_gpu_last_solve_ms": (_c.c_int, [_vp, _c.POINTER(_c.c_float)]),
     "hpccg_gpu_time_cg_kernels": (_c.c_int, [_vp, _i32, _c.POINTER(_c.c_float)]),
+    "hpccg_gpu_solve_mixed": (_c.c_int, [_vp, _f64p, _f64p, _i32, _f64, _i32, _i32, _f64, _vp]),
+    "hpccg_gpu_solve_mixed_device": (_c.c_int, [_vp, _vp, _vp, _i32, _f64, _i32, _i32, _f64, _vp]),
+    "hpccg_gpu_spmv_lowp": (_c.c_int, [_vp, _i32, _vp, _vp]),
+    "hpccg_gpu_set_mixed_rows_per_thread": (_c.c_int, [_vp, _i32, _i32]),
+    "hpccg_gpu_time_mixed_kernels": (_c.c_int, [_vp, _i32, _i32, _c.POINTER(_c.c_float)]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _fn = getattr(_lib, _name)
@@ -245,6 +257,40 @@ class Matrix:
     def vcopy(self, d_x, d_y):
         _sync_torch()
         _check(_lib.hpccg_gpu_vcopy(self._h, d_x.numel(), _dptr(d_x), _dptr(d_y)), "vcopy")
+
+    # -- mixed precision (FP64 iterative refinement, low-precision inner CG) --
+    def solve_mixed(self, b, x, precision: int, rel_tol: float = 1e-8, max_outer: int = 20,
+                    max_inner: int = 1000, inner_rtol: float = 0.0):
+        """Host arrays.  Returns (x, MixedInfo, status); x is updated in place."""
+        b = np.ascontiguousarray(b, np.float64)
+        if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous):
+            raise ValueError("x must be a contiguous float64 numpy array (updated in place)")
+        info = MixedInfo()
+        rc = _lib.hpccg_gpu_solve_mixed(self._h, b, x, precision, rel_tol, max_outer, max_inner, inner_rtol,
+                                        ctypes.byref(info))
+        _check(rc, "solve_mixed", allow=(HPCCG_OK, HPCCG_ERR_NOT_CONVERGED, HPCCG_ERR_BREAKDOWN))
+        return x, info, rc
+
+    def solve_mixed_device(self, d_b, d_x, precision: int, rel_tol: float = 1e-8, max_outer: int = 20,
+                           max_inner: int = 1000, inner_rtol: float = 0.0):
+        _sync_torch()
+        info = MixedInfo()
+        rc = _lib.hpccg_gpu_solve_mixed_device(self._h, _dptr(d_b), _dptr(d_x), precision, rel_tol, max_outer,
+                                               max_inner, inner_rtol, ctypes.byref(info))
+        _check(rc, "solve_mixed_device", allow=(HPCCG_OK, HPCCG_ERR_NOT_CONVERGED, HPCCG_ERR_BREAKDOWN))
+        return info, rc
+
+    def spmv_lowp(self, precision: int, d_x, d_y):
+        _sync_torch()
+        _check(_lib.hpccg_gpu_spmv_lowp(self._h, precision, _dptr(d_x), _dptr(d_y)), "spmv_lowp")
+
+    def set_mixed_rows_per_thread(self, precision: int, rpt: int):
+        _check(_lib.hpccg_gpu_set_mixed_rows_per_thread(self._h, precision, rpt), "set_mixed_rows_per_thread")
+
+    def time_mixed_kernels(self, precision: int, reps: int = 10):
+        ms = (_c.c_float * 3)()
+        _check(_lib.hpccg_gpu_time_mixed_kernels(self._h, precision, reps, ms), "time_mixed_kernels")
+        return [ms[0], ms[1], ms[2]]
 
     def uniform_pm1(self, seed: int, d_out, offset: int = 0):
         """Fill a device tensor with the project's counter-based U[-1,1) stream."""

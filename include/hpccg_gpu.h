@@ -101,6 +101,50 @@ int hpccg_gpu_cg_device(hpccg_ctx *ctx, const double *d_b, double *d_x, int32_t 
                         double tolerance, int32_t *niters, double *normr,
                         double *resid_hist);
 
+/* ---- mixed precision: FP64 iterative refinement around a low-precision CG ----
+ *
+ * No single reference routine: this replaces the whole `cg` call
+ * (MPI/src/numerics.F90:41-162) when the caller wants time to a relative
+ * residual instead of the reference's fixed iteration count.  The outer loop
+ * is FP64 on the device: r = b - A x with the FP64 values (bit-exact
+ * reference SpMV), stop when ||r||_2 <= rel_tol ||b||_2 (the FP64 true
+ * residual is the only convergence judge), else solve A d = r/||r|| with an
+ * inner CG in FP32 vectors and FP32 (HPCCG_PREC_FP32) or BF16
+ * (HPCCG_PREC_BF16) copies of A's values, row sums accumulated in FP32, and
+ * update x += ||r|| d in FP64.  The inner CG stops at ||r_in|| <= inner_rtol
+ * ||r_in,0||, or, with inner_rtol = 0, at the adaptive target
+ * max(1e-5, 0.5 rel_tol ||b|| / ||r||).  Needs an ELL width <= 27.
+ * Returns HPCCG_OK when the FP64 target is met, HPCCG_ERR_NOT_CONVERGED when
+ * max_outer cycles did not reach it (x holds the last iterate). */
+#define HPCCG_PREC_FP64 0
+#define HPCCG_PREC_FP32 1
+#define HPCCG_PREC_BF16 2
+
+typedef struct hpccg_mixed_info {
+  int32_t outer_iters; /* FP64 refinement cycles run                 */
+  int32_t inner_iters; /* low-precision CG iterations, all cycles    */
+  double relres;       /* final FP64 ||b - A x|| / ||b||             */
+  int32_t status;      /* device status word (HPCCG_OK or BREAKDOWN) */
+  int32_t reserved;
+} hpccg_mixed_info;
+
+int hpccg_gpu_solve_mixed(hpccg_ctx *ctx, const double *b, double *x, int32_t precision,
+                          double rel_tol, int32_t max_outer, int32_t max_inner, double inner_rtol,
+                          hpccg_mixed_info *info);
+int hpccg_gpu_solve_mixed_device(hpccg_ctx *ctx, const double *d_b, double *d_x, int32_t precision,
+                                 double rel_tol, int32_t max_outer, int32_t max_inner,
+                                 double inner_rtol, hpccg_mixed_info *info);
+
+/* y = A x with the low-precision values (FP32 vectors), for checks/timing. */
+int hpccg_gpu_spmv_lowp(hpccg_ctx *ctx, int32_t precision, const float *d_x, float *d_y);
+
+/* Rows per thread (1, 2 or 4) of the low-precision SpMV for one precision. */
+int hpccg_gpu_set_mixed_rows_per_thread(hpccg_ctx *ctx, int32_t precision, int32_t rpt);
+
+/* Average ms of the inner-CG kernels (p update, low-precision SpMV + p.Ap,
+ * r update + r.r), each launched `reps` times back to back. */
+int hpccg_gpu_time_mixed_kernels(hpccg_ctx *ctx, int32_t precision, int32_t reps, float *ms);
+
 /* ---- op-level drop-ins (device arrays), MPI/src/SparseMatrix.F90:213-232
  *      and MPI/src/vector_operations.F90:40-169 ------------------------------ */
 

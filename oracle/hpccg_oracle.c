@@ -75,9 +75,33 @@ void orc_spmv(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
     }
 }
 
+/* Dot-product summation used by orc_ddot/orc_ddot1 (and so by orc_cg):
+ * 0 = the reference's sequential loop (default), 1 = Neumaier-compensated
+ * sequential sum, a near-exact value used only to attribute differences
+ * between the GPU's reassociated sums and the reference's own rounding. */
+static int g_dot_mode = 0;
+void orc_set_dot_mode(int mode) { g_dot_mode = mode; }
+
+static double dot_compensated(int32_t n, const double *x, const double *y)
+{
+    double s = 0.0, c = 0.0;
+    for (int32_t i = 0; i < n; ++i) {
+        const double t = x[i] * y[i];
+        const double u = s + t;
+        if (fabs(s) >= fabs(t))
+            c += (s - u) + t;
+        else
+            c += (t - u) + s;
+        s = u;
+    }
+    return s + c;
+}
+
 /* MPI/src/vector_operations.F90:40-71 ddot (single rank: no allreduce). */
 double orc_ddot(int32_t n, const double *x, const double *y)
 {
+    if (g_dot_mode == 1)
+        return dot_compensated(n, x, y);
     double local_result = 0.0;
 #ifdef _OPENMP
 #pragma omp parallel for schedule(static) reduction(+ : local_result)
@@ -90,6 +114,8 @@ double orc_ddot(int32_t n, const double *x, const double *y)
 /* MPI/src/vector_operations.F90:73-103 ddot1. */
 double orc_ddot1(int32_t n, const double *x)
 {
+    if (g_dot_mode == 1)
+        return dot_compensated(n, x, x);
     double local_result = 0.0;
 #ifdef _OPENMP
 #pragma omp parallel for schedule(static) reduction(+ : local_result)

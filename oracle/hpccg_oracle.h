@@ -38,6 +38,10 @@ int64_t orc_generate_matrix(int32_t nx, int32_t ny, int32_t nz, int32_t *rowinde
 void orc_spmv(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
               const double *values, const double *x, double *y);
 
+/* Summation of orc_ddot/orc_ddot1: 0 = reference sequential order (default),
+ * 1 = Neumaier-compensated (a near-exact value, to attribute differences). */
+void orc_set_dot_mode(int mode);
+
 /* MPI/src/vector_operations.F90:40-169 */
 double orc_ddot(int32_t n, const double *x, const double *y);
 double orc_ddot1(int32_t n, const double *x);

@@ -60,6 +60,8 @@ def _lib(omp: bool = False) -> ctypes.CDLL:
     lib.orc_splitmix64_at.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
     lib.orc_uniform_pm1.restype = None
     lib.orc_uniform_pm1.argtypes = [ctypes.c_uint64, ctypes.c_int64, _f64p]
+    lib.orc_set_dot_mode.restype = None
+    lib.orc_set_dot_mode.argtypes = [ctypes.c_int]
     lib.orc_batch_sizes.restype = None
     lib.orc_batch_sizes.argtypes = [ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p]
     _libs[name] = lib
@@ -137,6 +139,20 @@ def cg(A: Matrix, b, x0, max_iter: int, tolerance: float, omp: bool = False):
     _lib(omp).orc_cg(A.nrow, A.rowindex, A.colindex, A.values, np.ascontiguousarray(b, np.float64),
                      x, max_iter, tolerance, ctypes.byref(niters), ctypes.byref(normr), hist)
     return x, niters.value, normr.value, hist[: niters.value + 1].copy()
+
+
+class compensated_dots:
+    """Context manager: the oracle's dot products use compensated summation inside."""
+
+    def __init__(self, omp: bool = False):
+        self.omp = omp
+
+    def __enter__(self):
+        _lib(self.omp).orc_set_dot_mode(1)
+        return self
+
+    def __exit__(self, *exc):
+        _lib(self.omp).orc_set_dot_mode(0)
 
 
 def compute_residual(v1, v2) -> float:

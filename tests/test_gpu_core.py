@@ -225,12 +225,21 @@ def test_cg_device_arrays(hp, torch):
 
 
 def test_cg_128_residual_history_and_solution(hp, torch):
-    """128^3 (2,097,152 rows, 55.7M nonzeros), 500 iterations on the GPU.  The
-    oracle's first 60 iterations pin the history; x -> 1 pins the end."""
+    """128^3 (2,097,152 rows, 55.7M nonzeros), 500 iterations on the GPU.
+
+    At this size the reference's own sequential dot products carry a rounding
+    error of order N*u = 2.3e-10 relative: with x = 1 most entries of r are
+    equal, so recursive summation errs systematically (measured 1.1e-11 at
+    k = 2).  The GPU history is therefore checked (a) against the sequential
+    oracle within N*u and (b) against the oracle with compensated dot products
+    (the same iteration computed with near-exact sums) within the 1e-12 band.
+    x -> 1 after 500 iterations pins the end."""
     n = 128
     A, x, b, xe = oracle.generate_matrix(n, n, n)
     assert A.nnz == 55742968
-    _, _, _, ref_hist = oracle.cg(A, b, x, 60, 0.0)
+    _, _, _, seq_hist = oracle.cg(A, b, x, 60, 0.0)
+    with oracle.compensated_dots():
+        _, _, _, ref_hist = oracle.cg(A, b, x, 60, 0.0)
     dx = torch.zeros(n ** 3, dtype=torch.float64, device="cuda")
     db = torch.zeros_like(dx)
     M = hp.Matrix.generated(n, n, n, dx, db, None)
@@ -238,4 +247,5 @@ def test_cg_128_residual_history_and_solution(hp, torch):
     it, normr, hist, status = M.cg_device(db, dx, 500, 0.0)
     assert status == hp.HPCCG_OK and it == 500
     assert_history_parity(hist[:61], ref_hist)
+    assert_history_parity(hist[:61], seq_hist, rtol=n ** 3 * 2.0 ** -53)
     assert np.abs(dx.cpu().numpy() - 1.0).max() <= 1e-10
