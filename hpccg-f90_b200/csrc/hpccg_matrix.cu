@@ -211,6 +211,7 @@ extern "C" const char *hpccg_strerror(int code) {
     case HPCCG_ERR_NOT_CONVERGED: return "not converged";
     case HPCCG_ERR_UNSUPPORTED: return "unsupported option";
     case HPCCG_ERR_NO_DEVICE: return "no CUDA device";
+    case HPCCG_ERR_TOO_LARGE: return "input larger than the fixed capacity of this entry point";
     default: return "unknown error";
   }
 }

@@ -28,6 +28,7 @@ HPCCG_ERR_TIMEOUT = 5
 HPCCG_ERR_NOT_CONVERGED = 6
 HPCCG_ERR_UNSUPPORTED = 7
 HPCCG_ERR_NO_DEVICE = 8
+HPCCG_ERR_TOO_LARGE = 9
 
 SPMV_AUTO, SPMV_ELL, SPMV_ELL2, SPMV_CSR_VECTOR = 0, 1, 2, 3
 PREC_FP64, PREC_FP32, PREC_BF16 = 0, 1, 2
@@ -81,6 +82,7 @@ _SIGS = {
     "hpccg_gpu_uniform_pm1": (_c.c_int, [_vp, _c.c_uint64, _i64, _i64, _vp]),
     "hpccg_gpu_last_solve_ms": (_c.c_int, [_vp, _c.POINTER(_c.c_float)]),
     "hpccg_gpu_time_cg_kernels": (_c.c_int, [_vp, _i32, _c.POINTER(_c.c_float)]),
+    "hpccg_gpu_ddot_noalloc": (_c.c_int, [_i32, _vp, _vp, _c.POINTER(_f64), _vp]),
     "hpccg_gpu_solve_mixed": (_c.c_int, [_vp, _f64p, _f64p, _i32, _f64, _i32, _i32, _f64, _vp]),
     "hpccg_gpu_solve_mixed_device": (_c.c_int, [_vp, _vp, _vp, _i32, _f64, _i32, _i32, _f64, _vp]),
     "hpccg_gpu_spmv_lowp": (_c.c_int, [_vp, _i32, _vp, _vp]),
@@ -119,6 +121,16 @@ def _sync_torch():
     import torch
 
     torch.cuda.synchronize()
+
+
+def ddot_noalloc(d_x, d_y, stream=None) -> float:
+    """x.y through hpccg_gpu_ddot_noalloc: no context and no device allocation
+    (partial sums in a fixed array inside the library; n <= 134,217,728)."""
+    _sync_torch()
+    r = _f64(0.0)
+    _check(_lib.hpccg_gpu_ddot_noalloc(d_x.numel(), _dptr(d_x), _dptr(d_y), _c.byref(r), stream),
+           "ddot_noalloc")
+    return r.value
 
 
 # ---- host generator ------------------------------------------------------------

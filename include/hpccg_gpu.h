@@ -37,6 +37,7 @@ extern "C" {
 #define HPCCG_ERR_NOT_CONVERGED 6 /* a solve with a target stopped short of it */
 #define HPCCG_ERR_UNSUPPORTED 7   /* option not available for this matrix */
 #define HPCCG_ERR_NO_DEVICE 8     /* no CUDA device visible */
+#define HPCCG_ERR_TOO_LARGE 9     /* input larger than a fixed capacity */
 
 typedef struct hpccg_ctx hpccg_ctx;
 
@@ -168,6 +169,27 @@ int hpccg_gpu_vcopy(hpccg_ctx *ctx, int32_t n, const double *d_x, double *d_y); 
  * only uses x = 1); it makes the random right-hand sides reproducible on
  * host and device. */
 int hpccg_gpu_uniform_pm1(hpccg_ctx *ctx, uint64_t seed, int64_t offset, int64_t n, double *d_out);
+
+/* ---- allocation-free entry point ---------------------------------------- */
+
+/* Dot product x.y of two device arrays that allocates no device memory.  This
+ * entry point has no counterpart in the reference.  It exists for callers that
+ * cannot let a library call cudaMalloc: hosts whose own memory manager owns
+ * all device memory (a pre-sized pool or a caching allocator the whole
+ * process must use), and code that may not allocate after its set-up phase
+ * (cudaMalloc can synchronise the device and can fail on a fragmented heap).
+ * It needs no hpccg_ctx.  The partial sums live in a fixed 512 KiB array
+ * compiled into the library, which every GPU that loads the library keeps
+ * until the process exits; so n is limited to 134,217,728 elements and larger
+ * n returns HPCCG_ERR_TOO_LARGE.  The work runs on `stream` (a cudaStream_t;
+ * NULL = the legacy default stream) on the current device, and the call
+ * returns after *result (host memory) is written.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU (from several host threads or
+ * streams at once) race and must be serialised by the caller. */
+int hpccg_gpu_ddot_noalloc(int32_t n, const double *d_x, const double *d_y, double *result,
+                           void *stream);
 
 /* ---- timing helpers (device time, CUDA events on the context stream) ----- */
 
