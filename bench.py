@@ -11,11 +11,14 @@ stopped when ||r|| < 1e-8 ||b||; the FP64 true residual is checked afterwards.
 Inputs (5.4 GB of matrix) are far larger than the 126 MB L2, so no flush is
 needed between steps.
 
-`value` is the device time of one solve (CUDA events on the library stream,
-max over ranks); `e2e` is the same solve through the host-array C-ABI call
-hpccg_gpu_cg with b and x0 copied from pinned host memory and x copied back
-inside the timed region.  `roofline` covers the dominant kernel (SpMV fused
-with p.Ap).  `cpu_baseline` times the CPU oracle (a C restatement of the
+Solvers timed: plain FP64 CG (the reference's algorithm), and FP64 iterative
+refinement around an FP32 or BF16-value inner CG.  `value` is the device time
+of one solve of the fastest solver whose FP64 true residual meets 1e-8 (CUDA
+events on the library stream, max over ranks); config.methods lists every
+solver.  `e2e` is the same solve through the host-array C-ABI call
+(hpccg_gpu_cg / hpccg_gpu_solve_mixed) with b and x0 copied from pinned host
+memory and x copied back inside the timed region.  `roofline` covers the
+dominant kernel of that solver (its SpMV fused with p.Ap).  `cpu_baseline` times the CPU oracle (a C restatement of the
 reference, OpenMP over all host cores) on a bounded sample of the same solve.
 
 N > 1 GPUs run independent replicas (the path does not shard at one rank:
@@ -42,7 +45,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "hpccg-f90_b200"))
 
-METRIC = "s to rel-res 1e-8 @256^3 (FP64 true residual)"
+METRIC = "s to rel-res 1e-8 @256^3 (FP64 true residual), best of plain FP64 CG / mixed-precision IR"
 SEED_XSTAR = 1234
 REL_TOL = 1e-8
 
@@ -213,6 +216,13 @@ def run_reference(args):
 # GPU side
 # ---------------------------------------------------------------------------------------
 
+def _fp64_relres(M, d_x, d_b, bnorm, scratch):
+    """FP64 true residual ||b - A x|| / ||b|| with the library's own kernels."""
+    M.spmv(d_x, scratch)
+    M.waxpby(1.0, d_b, -1.0, scratch, scratch)
+    return float(np.sqrt(M.ddot1(scratch))) / bnorm
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -235,89 +245,124 @@ def run_ours(args):
     M.spmv(xstar, d_b)  # b = A x* (bit-identical to the reference's spmv order)
     bnorm = float(np.sqrt(M.ddot1(d_b)))
     tol = REL_TOL * bnorm
+    scratch = torch.empty_like(d_b)
     max_iter = 1000
+    for prec in (hp.PREC_FP32, hp.PREC_BF16):
+        M.set_mixed_rows_per_thread(prec, 4)
 
-    def solve():
-        d_x.zero_()
-        it, normr, _, status = M.cg_device(d_b, d_x, max_iter, tol, history=False)
-        assert status == hp.HPCCG_OK, status
-        return it, M.last_solve_ms()
+    # Each solver maps to (device solve returning (info dict, kernel launches), host-array solve).
+    def fp64_cg():
+        it, _, _, st = M.cg_device(d_b, d_x, max_iter, tol, history=False)
+        assert st == hp.HPCCG_OK, st
+        return {"iterations": it}, 2 + 3 * it
 
-    for _ in range(args.warmup):
-        it, _ = solve()
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    times = []
-    with ClockSampler(torch.cuda.current_device()) as clk:
-        for _ in range(args.steps):
-            it, ms = solve()
-            times.append(ms)
-    torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
-    solve_ms = max_over_ranks(float(np.median(times)), dev)
-    # FP64 true residual of the last solve and error against x*
-    r = torch.empty_like(d_b)
-    M.spmv(d_x, r)
-    M.waxpby(1.0, d_b, -1.0, r, r)
-    relres = float(np.sqrt(M.ddot1(r))) / bnorm
-    err_xstar = float((d_x - xstar).abs().max().item())
+    def mixed(prec):
+        def run():
+            info, st = M.solve_mixed_device(d_b, d_x, prec, REL_TOL)
+            assert st == hp.HPCCG_OK, st
+            launches = 1 + (info.outer_iters + 1) + 2 * info.outer_iters + 3 * info.inner_iters
+            return {"outer": info.outer_iters, "inner": info.inner_iters, "device_relres": info.relres}, launches
+        return run
 
-    # end to end through the host-array C-ABI call, pinned host buffers
+    methods = [("fp64_cg", "plain FP64 CG (reference operation order), one CUDA graph", fp64_cg),
+               ("fp32_ir", "FP64 iterative refinement, FP32 inner CG", mixed(hp.PREC_FP32)),
+               ("bf16_ir", "FP64 iterative refinement, inner CG on BF16 values / FP32 vectors", mixed(hp.PREC_BF16))]
+    results = {}
+    clk_summary = None
+    for name, desc, fn in methods:
+        for _ in range(args.warmup):
+            d_x.zero_()
+            fn()
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        times, launches = [], 0
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            for _ in range(args.steps):
+                d_x.zero_()
+                info, nl = fn()
+                times.append(M.last_solve_ms())
+                launches += nl
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        ms = max_over_ranks(float(np.median(times)), dev)
+        relres = _fp64_relres(M, d_x, d_b, bnorm, scratch)
+        err = float((d_x - xstar).abs().max().item())
+        results[name] = {"ms": ms, "method": desc, "true_relres": relres, "max_abs_err_vs_xstar": err,
+                         "gpu_launches": launches, "clocks": clk.summary(), **info}
+    ok = {k: v for k, v in results.items() if v["true_relres"] <= REL_TOL}
+    head = min(ok, key=lambda k: ok[k]["ms"])
+    plain_ms = results["fp64_cg"]["ms"]
+
+    # end to end through the host-array C-ABI call of the headline solver, pinned host buffers
     h_b = torch.empty(N, dtype=torch.float64, pin_memory=True)
     h_b.copy_(d_b)
     h_x = torch.zeros(N, dtype=torch.float64, pin_memory=True)
-    xb = h_x.numpy()
-    bb = h_b.numpy()
+    xb, bb = h_x.numpy(), h_b.numpy()
     e2e = []
     for s in range(args.warmup + args.steps):
         xb[:] = 0.0
         t0 = time.perf_counter()
-        _, it_e, _, _, st = M.cg(bb, xb, max_iter, tol, history=False)
+        if head == "fp64_cg":
+            M.cg(bb, xb, max_iter, tol, history=False)
+        else:
+            M.solve_mixed(bb, xb, hp.PREC_FP32 if head == "fp32_ir" else hp.PREC_BF16, REL_TOL)
         dt = time.perf_counter() - t0
         if s >= args.warmup:
             e2e.append(dt)
     e2e_s = max_over_ranks(float(np.median(e2e)), dev)
 
-    # roofline of the dominant kernel (SpMV fused with p.Ap), timed on its own stream
-    kms = M.time_cg_kernels(reps=20)
-    nnz = M.nnz
-    alg_bytes = 12 * nnz + 20 * N + 4
+    # rooflines (CUDA events on the library stream around back-to-back launches)
     hbm, _, peak_kind = _peaks()
-    achieved = alg_bytes / (kms[1] * 1e-3) / 1e9
-    iter_bytes = alg_bytes + 40 * N + 24 * N  # + p/x update + r update passes
-    iter_ms = sum(kms)
+    nnz = M.nnz
+    kms64 = M.time_cg_kernels(reps=20)
+    alg64 = 12 * nnz + 20 * N + 4
+    roof64 = {"bound": "hbm", "kernel": "k_cg_spmv_dot (FP64 SpMV + p.Ap)", "kernel_ms": kms64[1],
+              "alg_bytes_per_launch": alg64, "achieved": alg64 / (kms64[1] * 1e-3) / 1e9, "peak": hbm,
+              "unit": "GB/s", "peak_source": peak_kind, "traffic": _traffic_from_profile()}
+    roof64["frac"] = roof64["achieved"] / hbm
+    roofs = {"fp64_cg": roof64}
+    for name, prec, vb in (("fp32_ir", hp.PREC_FP32, 4), ("bf16_ir", hp.PREC_BF16, 2)):
+        km = M.time_mixed_kernels(prec, 20)
+        alg = (4 + vb) * nnz + 12 * N + 4
+        roofs[name] = {"bound": "hbm", "kernel": f"k_mp_spmv_dot ({name[:4].upper()} values, FP32 vectors, + p.Ap)",
+                       "kernel_ms": km[1], "alg_bytes_per_launch": alg, "achieved": alg / (km[1] * 1e-3) / 1e9,
+                       "peak": hbm, "unit": "GB/s", "peak_source": peak_kind, "traffic": None,
+                       "inner_iteration_ms": sum(km)}
+        roofs[name]["frac"] = roofs[name]["achieved"] / hbm
 
     if rank != 0:
-        dist.destroy_process_group() if ws > 1 else None
+        if ws > 1:
+            dist.destroy_process_group()
         return 0
 
     cpu = None
     if not args.no_cpu_baseline:
-        c = cpu_reference_time(n, args.ref_sample_iters, 1, 0, iters_needed=it)
+        it64 = results["fp64_cg"]["iterations"]
+        c = cpu_reference_time(n, args.ref_sample_iters, 1, 0, iters_needed=it64)
         cpu = {"value": c["value"], "unit": "s", "cores": c["cores"], "kind": "port",
                "sample": f"{args.ref_sample_iters} CG iterations of the C restatement of MPI/src at {n}^3 "
-                         f"(OpenMP, {c['cores']} threads) x {it} iterations (the GPU FP64 count)"}
+                         f"(OpenMP, {c['cores']} threads) x {it64} iterations (the GPU FP64 count)"}
+    hr = results[head]
     line = {
-        "metric": METRIC, "value": solve_ms / 1e3, "unit": "s", "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": solve_ms, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "metric": METRIC, "value": hr["ms"] / 1e3, "unit": "s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": hr["ms"], "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if head == "fp64_cg" else "f32/bf16 inner, f64 outer",
+        "data": "synthetic",
         "config": {"workload": f"{n}^3 27-point HPCCG matrix ({N} rows, {nnz} nonzeros), x* U[-1,1) seed 1234, "
-                               f"b = A x*, x0 = 0, FP64 CG (reference operation order) to ||r|| < 1e-8 ||b||",
-                   "method": "plain FP64 CG, one CUDA graph with a device-side while loop",
-                   "iterations": it, "true_relres": relres, "max_abs_err_vs_xstar": err_xstar,
+                               f"b = A x*, x0 = 0, solved to FP64 ||b - A x|| <= 1e-8 ||b||",
+                   "method": head, "speedup_vs_plain_gpu_cg": plain_ms / hr["ms"],
+                   "methods": results,
                    "l2": "inputs (5.4 GB matrix) exceed the 126 MB L2; no flush",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
                    "spmv_kernel": list(M.get_spmv())},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": _traffic_from_profile(), "kernel": "k_cg_spmv_dot (SpMV + p.Ap)",
-                     "alg_bytes_per_launch": alg_bytes, "kernel_ms": kms[1], "peak_source": peak_kind,
-                     "iteration_ms": iter_ms, "iteration_gbs": iter_bytes / (iter_ms * 1e-3) / 1e9},
+        "roofline": roofs[head], "roofline_all": roofs,
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 16 * N, "d2h_bytes_per_step": 8 * N},
-        "gpu_launches": args.steps * (2 + 3 * it),
-        "clocks": clk.summary(),
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 16 * N, "d2h_bytes_per_step": 8 * N,
+                "call": "hpccg_gpu_cg" if head == "fp64_cg" else "hpccg_gpu_solve_mixed"},
+        "gpu_launches": hr["gpu_launches"],
+        "clocks": hr["clocks"],
     }
     print(json.dumps(line), flush=True)
     if ws > 1:
