@@ -1,0 +1,986 @@
+// hpccg_batch.cu -- many independent HPCCG systems solved together.
+//
+// The systems are stacked block-diagonally in one column-major ELL (27 slots,
+// global column indices); each system's rows start on a 512-row chunk
+// boundary.  A schedule cuts every system into tiles of whole chunks; one
+// persistent kernel per CG phase walks the tiles of all systems that are still
+// active.  Every dot product is reduced per 512-row chunk in a fixed order
+// (thread pair sums, fixed block butterfly), and per system over its chunks in
+// index order, so the result does not depend on the schedule: the autotuner
+// may pick any tile size / grid and every iterate stays bit-identical.
+//
+// Solvers (all on the device, one CUDA graph with while nodes):
+//   FP64: CG per system (same steps as MPI/src/numerics.F90:108-147, stopping
+//         per system at ||r|| <= rel_tol ||b||), then an FP64 true residual.
+//   FP32 / BF16: per-system FP64 iterative refinement around an inner CG in
+//         FP32 vectors and FP32 / BF16 values (as hpccg_mixed.cu), with the
+//         FP64 true residual as the judge of every system.
+#include <stdlib.h>
+
+#include <algorithm>
+#include <type_traits>
+#include <vector>
+
+#include "hpccg_internal.cuh"
+#include "hpccg_rows_lp.cuh"
+
+namespace hpccg {
+
+constexpr int kChunk = 512;  // rows per reduction chunk (2 per thread of a 256-thread block)
+
+struct BatchSys {
+  double bb, tol2, rtrans, pAp, alpha, beta, relres, scale, target, rr0;
+  int k, active, status, outer, inner_k, inner_active, iters, converged;
+};
+
+struct BatchArgs {
+  int nsys, ntiles;
+  const int4 *tiles;        // (system, first row, end row, first chunk)
+  const int *sys_chunk0;    // nsys+1 chunk offsets
+  int npad;
+  const int32_t *col;
+  const double *val;
+  const void *val_lp;
+  double *x, *b, *r, *p, *Ap;
+  float *r32, *p32, *Ap32, *d32;
+  double *part;             // one partial per chunk
+  unsigned *counter;
+  BatchSys *sys;
+  double rel_tol, inner_rtol;
+  int max_iter, max_outer, max_inner;
+  cudaGraphConditionalHandle c_outer, c_inner;
+  int use_cond;
+};
+
+// ---- per-row operations ------------------------------------------------------
+__device__ __forceinline__ double row_fp64(const BatchArgs &g, int i, const double *x) {
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 27; ++k) {
+    const size_t o = (size_t)k * g.npad + i;
+    s = __dadd_rn(s, __dmul_rn(__ldcs(g.val + o), __ldg(x + __ldcs(g.col + o))));
+  }
+  return s;
+}
+
+template <typename VT>
+__device__ __forceinline__ float row_lp(const BatchArgs &g, int i, const float *x) {
+  float s = 0.f;
+  const VT *val = reinterpret_cast<const VT *>(g.val_lp);
+#pragma unroll
+  for (int k = 0; k < 27; ++k) {
+    const size_t o = (size_t)k * g.npad + i;
+    float v[1];
+    LpLoad<VT, 1>::vals(val, o, v);
+    s = fmaf(v[0], __ldg(x + __ldcs(g.col + o)), s);
+  }
+  return s;
+}
+
+// ---- the phases ----------------------------------------------------------------
+// Each phase: active(s) selects the systems it touches, row(i, s) does the row's
+// work and returns its dot-product term, finalize(s, total) runs once per
+// active system in the last block, cond() names the loop condition it sets.
+struct PhBnorm {  // bb = b.b
+  static __device__ bool active(const BatchArgs &g, int s) { return true; }
+  static __device__ double row(const BatchArgs &g, int i, int s) { return __dmul_rn(g.b[i], g.b[i]); }
+  static __device__ void finalize(const BatchArgs &g, int s, double t) {
+    BatchSys &y = g.sys[s];
+    y.bb = t;
+    y.tol2 = g.rel_tol * g.rel_tol * t;
+    y.outer = 0;
+    y.iters = 0;
+    y.status = HPCCG_OK;
+    y.converged = 0;
+    y.active = 1;
+  }
+  static constexpr int kCond = -1;
+};
+
+struct PhInit64 {  // r = b - A x, p = r, rtrans = r.r
+  static __device__ bool active(const BatchArgs &g, int s) { return true; }
+  static __device__ double row(const BatchArgs &g, int i, int s) {
+    const double ri = __dsub_rn(g.b[i], row_fp64(g, i, g.x));
+    g.r[i] = ri;
+    return __dmul_rn(ri, ri);
+  }
+  static __device__ void finalize(const BatchArgs &g, int s, double t) {
+    BatchSys &y = g.sys[s];
+    y.rtrans = t;
+    y.k = 0;
+    y.active = (t > y.tol2) && (g.max_iter > 0);
+    y.converged = !(t > y.tol2);
+    y.relres = y.bb > 0.0 ? sqrt(t / y.bb) : 0.0;
+  }
+  static constexpr int kCond = 1;  // outer (the CG loop)
+};
+
+struct PhSpmvDot64 {  // Ap = A p, alpha = rtrans / p.Ap
+  static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].active; }
+  static __device__ double row(const BatchArgs &g, int i, int s) {
+    const double ai = row_fp64(g, i, g.p);
+    g.Ap[i] = ai;
+    return __dmul_rn(g.p[i], ai);
+  }
+  static __device__ void finalize(const BatchArgs &g, int s, double t) {
+    BatchSys &y = g.sys[s];
+    y.pAp = t;
+    const double a = y.rtrans / t;
+    if (!isfinite(a)) {
+      y.status = HPCCG_ERR_BREAKDOWN;
+      y.active = 0;
+    } else {
+      y.alpha = a;
+    }
+  }
+  static constexpr int kCond = -1;
+};
+
+struct PhUpdate64 {  // x += alpha p, r -= alpha Ap, beta, per-system stop test
+  static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].active; }
+  static __device__ double row(const BatchArgs &g, int i, int s) {
+    const double a = g.sys[s].alpha;
+    g.x[i] = __dadd_rn(g.x[i], __dmul_rn(a, g.p[i]));
+    const double ri = __dadd_rn(g.r[i], __dmul_rn(-a, g.Ap[i]));
+    g.r[i] = ri;
+    return __dmul_rn(ri, ri);
+  }
+  static __device__ void finalize(const BatchArgs &g, int s, double t) {
+    BatchSys &y = g.sys[s];
+    y.k += 1;
+    y.iters = y.k;
+    y.beta = t / y.rtrans;
+    y.rtrans = t;
+    if (!(t > y.tol2)) {
+      y.active = 0;
+      y.converged = 1;
+    } else if (y.k >= g.max_iter || !isfinite(t)) {
+      y.active = 0;
+    }
+  }
+  static constexpr int kCond = 1;
+};
+
+struct PhResidual64 {  // final r = b - A x, relres (all systems)
+  static __device__ bool active(const BatchArgs &g, int s) { return true; }
+  static __device__ double row(const BatchArgs &g, int i, int s) {
+    const double ri = __dsub_rn(g.b[i], row_fp64(g, i, g.x));
+    return __dmul_rn(ri, ri);
+  }
+  static __device__ void finalize(const BatchArgs &g, int s, double t) {
+    BatchSys &y = g.sys[s];
+    y.relres = y.bb > 0.0 ? sqrt(t / y.bb) : 0.0;
+    y.converged = y.relres <= g.rel_tol;
+  }
+  static constexpr int kCond = -1;
+};
+
+// -- iterative refinement phases --
+struct PhOuter64 {  // r64 = b - A x, relres, outer decision (systems still refining)
+  static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].active; }
+  static __device__ double row(const BatchArgs &g, int i, int s) {
+    const double ri = __dsub_rn(g.b[i], row_fp64(g, i, g.x));
+    g.r[i] = ri;
+    return __dmul_rn(ri, ri);
+  }
+  static __device__ void finalize(const BatchArgs &g, int s, double t) {
+    BatchSys &y = g.sys[s];
+    y.relres = y.bb > 0.0 ? sqrt(t / y.bb) : 0.0;
+    if (!isfinite(y.relres)) {
+      y.status = HPCCG_ERR_BREAKDOWN;
+      y.active = 0;
+      return;
+    }
+    y.converged = y.relres <= g.rel_tol;
+    y.active = !y.converged && y.outer < g.max_outer;
+    if (y.active) {
+      y.scale = sqrt(t);
+      y.target = g.inner_rtol > 0.0 ? g.inner_rtol : fmax(1e-5, 0.5 * g.rel_tol / y.relres);
+      y.outer += 1;
+    }
+  }
+  static constexpr int kCond = 1;
+};
+
+struct PhStartInner {  // r32 = r64 / ||r64||, d = 0, rr0
+  static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].active; }
+  static __device__ double row(const BatchArgs &g, int i, int s) {
+    const float ri = (float)(g.r[i] / g.sys[s].scale);
+    g.r32[i] = ri;
+    g.d32[i] = 0.f;
+    return (double)ri * ri;
+  }
+  static __device__ void finalize(const BatchArgs &g, int s, double t) {
+    BatchSys &y = g.sys[s];
+    y.rtrans = t;
+    y.rr0 = t;
+    y.inner_k = 0;
+    y.inner_active = t > 0.0 && g.max_inner > 0;
+  }
+  static constexpr int kCond = 2;  // inner
+};
+
+template <typename VT>
+struct PhSpmvDotLp {
+  static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].inner_active; }
+  static __device__ double row(const BatchArgs &g, int i, int s) {
+    const float ai = row_lp<VT>(g, i, g.p32);
+    g.Ap32[i] = ai;
+    return (double)g.p32[i] * ai;
+  }
+  static __device__ void finalize(const BatchArgs &g, int s, double t) {
+    BatchSys &y = g.sys[s];
+    const double a = y.rtrans / t;
+    if (!(t > 0.0) || !isfinite(a)) {
+      y.inner_active = 0;
+      y.alpha = 0.0;
+    } else {
+      y.alpha = a;
+    }
+  }
+  static constexpr int kCond = -1;
+};
+
+struct PhUpdateLp {  // d += alpha p, r -= alpha Ap, inner stop test
+  static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].inner_active; }
+  static __device__ double row(const BatchArgs &g, int i, int s) {
+    const float a = (float)g.sys[s].alpha;
+    g.d32[i] = fmaf(a, g.p32[i], g.d32[i]);
+    const float ri = fmaf(-a, g.Ap32[i], g.r32[i]);
+    g.r32[i] = ri;
+    return (double)ri * ri;
+  }
+  static __device__ void finalize(const BatchArgs &g, int s, double t) {
+    BatchSys &y = g.sys[s];
+    y.inner_k += 1;
+    y.iters += 1;
+    y.beta = t / y.rtrans;
+    y.rtrans = t;
+    y.inner_active = isfinite(t) && t > y.target * y.target * y.rr0 && y.inner_k < g.max_inner;
+  }
+  static constexpr int kCond = 2;
+};
+
+// ---- the persistent phase kernel --------------------------------------------------
+__device__ __forceinline__ void set_cond(const BatchArgs &g, int which, int v) {
+  if (!g.use_cond || which < 0) return;
+  cudaGraphSetConditional(which == 1 ? g.c_outer : g.c_inner, (unsigned)v);
+}
+
+template <class Ph>
+__global__ void __launch_bounds__(256, 4) k_batch_phase(BatchArgs g) {
+  __shared__ double smem[32];
+  __shared__ bool s_last;
+  for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
+    const int4 tile = g.tiles[t];
+    const int s = tile.x;
+    if (!Ph::active(g, s)) continue;  // uniform over the block
+    const int nch = (tile.z - tile.y + kChunk - 1) / kChunk;
+    for (int c = 0; c < nch; ++c) {
+      const int r0 = tile.y + c * kChunk;
+      const int i0 = r0 + threadIdx.x, i1 = i0 + 256;
+      double v0 = 0.0, v1 = 0.0;
+      if (i0 < tile.z) v0 = Ph::row(g, i0, s);
+      if (i1 < tile.z) v1 = Ph::row(g, i1, s);
+      const double cs = block_sum<256>(__dadd_rn(v0, v1), smem);
+      if (threadIdx.x == 0) g.part[tile.w + c] = cs;
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(g.counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // one warp per system: lanes stride the system's chunks, fixed butterfly
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int s = warp; s < g.nsys; s += 8) {
+    if (!Ph::active(g, s)) continue;
+    double v = 0.0;
+    for (int c = g.sys_chunk0[s] + lane; c < g.sys_chunk0[s + 1]; c += 32)
+      v = __dadd_rn(v, ((volatile double *)g.part)[c]);
+    v = warp_sum(v);
+    if (lane == 0) Ph::finalize(g, s, v);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *g.counter = 0u;
+    if (Ph::kCond >= 0) {
+      int any = 0;
+      for (int s = 0; s < g.nsys; ++s) {
+        const volatile BatchSys &y = g.sys[s];
+        any |= Ph::kCond == 2 ? y.inner_active : y.active;
+      }
+      set_cond(g, Ph::kCond, any);
+    }
+  }
+}
+
+// Element-wise phases without a reduction, persistent over the same tiles.
+__global__ void __launch_bounds__(256) k_batch_p64(BatchArgs g) {
+  for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
+    const int4 tile = g.tiles[t];
+    const BatchSys &y = g.sys[tile.x];
+    if (!y.active) continue;
+    const bool first = y.k == 0;
+    const double beta = y.beta;
+    for (int i = tile.y + threadIdx.x; i < tile.z; i += 256)
+      g.p[i] = first ? g.r[i] : __dadd_rn(g.r[i], __dmul_rn(beta, g.p[i]));
+  }
+}
+
+__global__ void __launch_bounds__(256) k_batch_p32(BatchArgs g) {
+  for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
+    const int4 tile = g.tiles[t];
+    const BatchSys &y = g.sys[tile.x];
+    if (!y.inner_active) continue;
+    const bool first = y.inner_k == 0;
+    const float beta = (float)y.beta;
+    for (int i = tile.y + threadIdx.x; i < tile.z; i += 256)
+      g.p32[i] = first ? g.r32[i] : fmaf(beta, g.p32[i], g.r32[i]);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_batch_end_inner(BatchArgs g) {
+  for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
+    const int4 tile = g.tiles[t];
+    const BatchSys &y = g.sys[tile.x];
+    if (!y.active) continue;
+    const double scale = y.scale;
+    for (int i = tile.y + threadIdx.x; i < tile.z; i += 256) g.x[i] = fma(scale, (double)g.d32[i], g.x[i]);
+  }
+}
+
+// Plain FP64 y = A x over all systems (tests, b = A x*).
+__global__ void k_batch_spmv(BatchArgs g, const double *x, double *y) {
+  for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
+    const int4 tile = g.tiles[t];
+    for (int i = tile.y + threadIdx.x; i < tile.z; i += 256) y[i] = row_fp64(g, i, x);
+  }
+}
+
+// generate_matrix(nx,ny,nz) rows written into the stacked ELL at row offset `off`.
+__global__ void k_batch_generate(int nx, int ny, int nz, int off, int npad, int32_t *col, double *val) {
+  const int n = nx * ny * nz;
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    const int ix = row % nx + 1, iy = (row / nx) % ny + 1, iz = row / (nx * ny) + 1;
+    int k = 0;
+    for (int sz = (iz > 1 ? -1 : 0); sz <= (iz < nz ? 1 : 0); ++sz)
+      for (int sy = (iy > 1 ? -1 : 0); sy <= (iy < ny ? 1 : 0); ++sy)
+        for (int sx = (ix > 1 ? -1 : 0); sx <= (ix < nx ? 1 : 0); ++sx) {
+          const size_t o = (size_t)k * npad + off + row;
+          col[o] = off + row + sz * nx * ny + sy * nx + sx;
+          val[o] = (sz == 0 && sy == 0 && sx == 0) ? 27.0 : -1.0;
+          ++k;
+        }
+    for (; k < 27; ++k) {
+      const size_t o = (size_t)k * npad + off + row;
+      col[o] = off + row;
+      val[o] = 0.0;
+    }
+  }
+}
+
+// 1-based CSR rows of one system into the stacked ELL at row offset `off`.
+__global__ void k_batch_from_csr(int n, const int32_t *rowindex, const int32_t *colindex, const double *values,
+                                 int off, int npad, int32_t *col, double *val, int *bad) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
+    const int a = rowindex[row] - 1, e = rowindex[row + 1] - 1;
+    if (e < a || e - a > 27) {
+      atomicOr(bad, 1);
+      continue;
+    }
+    for (int k = 0; k < 27; ++k) {
+      const size_t o = (size_t)k * npad + off + row;
+      if (k < e - a) {
+        const int c = colindex[a + k];
+        if (c < 1 || c > n) atomicOr(bad, 2);
+        col[o] = off + (c >= 1 && c <= n ? c - 1 : row);
+        val[o] = values[a + k];
+      } else {
+        col[o] = off + row;
+        val[o] = 0.0;
+      }
+    }
+  }
+}
+
+__global__ void k_batch_pad(int npad, int32_t *col, double *val, const int *is_row) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += gridDim.x * blockDim.x)
+    if (!is_row[i])
+      for (int k = 0; k < 27; ++k) {
+        col[(size_t)k * npad + i] = i;
+        val[(size_t)k * npad + i] = 0.0;
+      }
+}
+
+}  // namespace hpccg
+
+using namespace hpccg;
+
+struct hpccg_batch {
+  int device = 0, num_sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int nsys = 0;
+  int npad = 0;
+  std::vector<int> n, off, chunk0;  // per system rows, row offset, first chunk (host copies)
+  int nchunks = 0;
+  int32_t *col = nullptr;
+  double *val = nullptr;
+  float *val32 = nullptr;
+  __nv_bfloat16 *val16 = nullptr;
+  double *x = nullptr, *b = nullptr, *r = nullptr, *p = nullptr, *Ap = nullptr;
+  float *r32 = nullptr, *p32 = nullptr, *Ap32 = nullptr, *d32 = nullptr;
+  double *part = nullptr;
+  unsigned *counter = nullptr;
+  BatchSys *sys = nullptr;
+  int *d_sys_chunk0 = nullptr;
+  int4 *d_tiles = nullptr;
+  int ntiles = 0;
+  int tile_chunks = 0, blocks_per_sm = 0;  // schedule; 0 = not tuned yet
+  bool tuned = false;
+  cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
+  int exec_tile[3] = {0, 0, 0}, exec_bps[3] = {0, 0, 0}, exec_maxit[3] = {-1, -1, -1};
+  double exec_tol[3] = {-1.0, -1.0, -1.0};
+  float last_ms = 0.f;
+};
+
+static void batch_free(hpccg_batch *B) {
+  for (auto &e : B->exec)
+    if (e) cudaGraphExecDestroy(e);
+  void *bufs[] = {B->col, B->val, B->val32, B->val16, B->x, B->b, B->r, B->p, B->Ap, B->r32, B->p32,
+                  B->Ap32, B->d32, B->part, B->counter, B->sys, B->d_sys_chunk0, B->d_tiles};
+  for (void *q : bufs)
+    if (q) cudaFree(q);
+  if (B->ev0) cudaEventDestroy(B->ev0);
+  if (B->ev1) cudaEventDestroy(B->ev1);
+  if (B->stream) cudaStreamDestroy(B->stream);
+  delete B;
+}
+
+static int build_tiles(hpccg_batch *B, int tile_chunks) {
+  std::vector<int4> tiles;
+  for (int s = 0; s < B->nsys; ++s) {
+    const int rows_per_tile = tile_chunks * kChunk;
+    for (int r0 = 0; r0 < B->n[s]; r0 += rows_per_tile) {
+      const int r1 = std::min(B->n[s], r0 + rows_per_tile);
+      tiles.push_back(make_int4(s, B->off[s] + r0, B->off[s] + r1, B->chunk0[s] + r0 / kChunk));
+    }
+  }
+  if (B->d_tiles) cudaFree(B->d_tiles);
+  B->d_tiles = nullptr;
+  HPCCG_CUDA(cudaMalloc(&B->d_tiles, sizeof(int4) * tiles.size()));
+  HPCCG_CUDA(cudaMemcpyAsync(B->d_tiles, tiles.data(), sizeof(int4) * tiles.size(), cudaMemcpyHostToDevice, B->stream));
+  HPCCG_CUDA(cudaStreamSynchronize(B->stream));
+  B->ntiles = (int)tiles.size();
+  B->tile_chunks = tile_chunks;
+  return HPCCG_OK;
+}
+
+// Lays out the systems (rows on 512-row boundaries) and allocates everything.
+static int batch_alloc(hpccg_batch *B, int nsys, const int64_t *rows) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return HPCCG_ERR_NO_DEVICE;
+  HPCCG_CUDA(cudaGetDevice(&B->device));
+  HPCCG_CUDA(cudaDeviceGetAttribute(&B->num_sms, cudaDevAttrMultiProcessorCount, B->device));
+  HPCCG_CUDA(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+  HPCCG_CUDA(cudaEventCreate(&B->ev0));
+  HPCCG_CUDA(cudaEventCreate(&B->ev1));
+  B->nsys = nsys;
+  int64_t off = 0, chunks = 0;
+  for (int s = 0; s < nsys; ++s) {
+    B->n.push_back((int)rows[s]);
+    B->off.push_back((int)off);
+    B->chunk0.push_back((int)chunks);
+    const int64_t c = (rows[s] + kChunk - 1) / kChunk;
+    chunks += c;
+    off += c * kChunk;
+  }
+  B->chunk0.push_back((int)chunks);
+  if (off * 27 > INT32_MAX) return HPCCG_ERR_INVALID_ARG;
+  B->npad = (int)off;
+  B->nchunks = (int)chunks;
+  const size_t slots = (size_t)27 * B->npad;
+  HPCCG_CUDA(cudaMalloc(&B->col, sizeof(int32_t) * slots));
+  HPCCG_CUDA(cudaMalloc(&B->val, sizeof(double) * slots));
+  const size_t v64 = sizeof(double) * B->npad, v32 = sizeof(float) * B->npad;
+  double **d64[] = {&B->x, &B->b, &B->r, &B->p, &B->Ap};
+  for (double **q : d64) {
+    HPCCG_CUDA(cudaMalloc(q, v64));
+    HPCCG_CUDA(cudaMemsetAsync(*q, 0, v64, B->stream));
+  }
+  float **d32[] = {&B->r32, &B->p32, &B->Ap32, &B->d32};
+  for (float **q : d32) {
+    HPCCG_CUDA(cudaMalloc(q, v32));
+    HPCCG_CUDA(cudaMemsetAsync(*q, 0, v32, B->stream));
+  }
+  HPCCG_CUDA(cudaMalloc(&B->part, sizeof(double) * std::max(1, B->nchunks)));
+  HPCCG_CUDA(cudaMalloc(&B->counter, sizeof(unsigned) * 4));
+  HPCCG_CUDA(cudaMemsetAsync(B->counter, 0, sizeof(unsigned) * 4, B->stream));
+  HPCCG_CUDA(cudaMalloc(&B->sys, sizeof(BatchSys) * nsys));
+  HPCCG_CUDA(cudaMemsetAsync(B->sys, 0, sizeof(BatchSys) * nsys, B->stream));
+  HPCCG_CUDA(cudaMalloc(&B->d_sys_chunk0, sizeof(int) * (nsys + 1)));
+  HPCCG_CUDA(cudaMemcpyAsync(B->d_sys_chunk0, B->chunk0.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice,
+                             B->stream));
+  HPCCG_CUDA(cudaStreamSynchronize(B->stream));
+  B->blocks_per_sm = 4;
+  return build_tiles(B, 4);
+}
+
+// Marks padding rows (between systems) so they multiply as exact zeros.
+static int batch_pad_rows(hpccg_batch *B) {
+  std::vector<int> is_row(B->npad, 0);
+  for (int s = 0; s < B->nsys; ++s)
+    for (int i = 0; i < B->n[s]; ++i) is_row[B->off[s] + i] = 1;
+  int *d = nullptr;
+  HPCCG_CUDA(cudaMalloc(&d, sizeof(int) * B->npad));
+  cudaMemcpyAsync(d, is_row.data(), sizeof(int) * B->npad, cudaMemcpyHostToDevice, B->stream);
+  k_batch_pad<<<B->num_sms * 8, 256, 0, B->stream>>>(B->npad, B->col, B->val, d);
+  const cudaError_t e = cudaStreamSynchronize(B->stream);
+  cudaFree(d);
+  HPCCG_CUDA(e);
+  return HPCCG_OK;
+}
+
+extern "C" int hpccg_batch_create_generated(int32_t nsys, const int32_t *sizes, hpccg_batch **out) {
+  if (!out || nsys < 1 || !sizes) return HPCCG_ERR_INVALID_ARG;
+  std::vector<int64_t> rows(nsys);
+  for (int s = 0; s < nsys; ++s) {
+    if (sizes[3 * s] < 1 || sizes[3 * s + 1] < 1 || sizes[3 * s + 2] < 1) return HPCCG_ERR_INVALID_ARG;
+    rows[s] = (int64_t)sizes[3 * s] * sizes[3 * s + 1] * sizes[3 * s + 2];
+    if (rows[s] * 27 > INT32_MAX) return HPCCG_ERR_INVALID_ARG;
+  }
+  *out = nullptr;
+  hpccg_batch *B = new hpccg_batch();
+  int rc = batch_alloc(B, nsys, rows.data());
+  if (rc) {
+    batch_free(B);
+    return rc;
+  }
+  for (int s = 0; s < nsys; ++s)
+    k_batch_generate<<<B->num_sms * 8, 256, 0, B->stream>>>(sizes[3 * s], sizes[3 * s + 1], sizes[3 * s + 2],
+                                                             B->off[s], B->npad, B->col, B->val);
+  if ((rc = batch_pad_rows(B))) {
+    batch_free(B);
+    return rc;
+  }
+  *out = B;
+  return HPCCG_OK;
+}
+
+extern "C" int hpccg_batch_create(int32_t nsys, const int32_t *nrows, const int32_t *const *rowindex,
+                                  const int32_t *const *colindex, const double *const *values,
+                                  hpccg_batch **out) {
+  if (!out || nsys < 1 || !nrows || !rowindex || !colindex || !values) return HPCCG_ERR_INVALID_ARG;
+  std::vector<int64_t> rows(nsys);
+  for (int s = 0; s < nsys; ++s) {
+    if (nrows[s] < 1 || !rowindex[s]) return HPCCG_ERR_INVALID_ARG;
+    rows[s] = nrows[s];
+  }
+  *out = nullptr;
+  hpccg_batch *B = new hpccg_batch();
+  int rc = batch_alloc(B, nsys, rows.data());
+  int *d_bad = nullptr;
+  int bad = 0;
+  if (!rc && cudaMalloc(&d_bad, sizeof(int)) != cudaSuccess) rc = HPCCG_ERR_OOM;
+  if (!rc) cudaMemsetAsync(d_bad, 0, sizeof(int), B->stream);
+  for (int s = 0; s < nsys && !rc; ++s) {
+    const int n = nrows[s];
+    const int64_t nnz = (int64_t)rowindex[s][n] - 1;
+    if (nnz < 0 || nnz > 27 * (int64_t)n || (nnz > 0 && (!colindex[s] || !values[s]))) {
+      rc = HPCCG_ERR_INVALID_ARG;
+      break;
+    }
+    int32_t *dr = nullptr, *dc = nullptr;
+    double *dv = nullptr;
+    if (cudaMalloc(&dr, sizeof(int32_t) * (n + 1)) != cudaSuccess ||
+        cudaMalloc(&dc, sizeof(int32_t) * std::max<int64_t>(nnz, 1)) != cudaSuccess ||
+        cudaMalloc(&dv, sizeof(double) * std::max<int64_t>(nnz, 1)) != cudaSuccess) {
+      rc = HPCCG_ERR_OOM;
+    } else {
+      // copies and kernel on the batch stream, so the kernel sees finished copies
+      cudaMemcpyAsync(dr, rowindex[s], sizeof(int32_t) * (n + 1), cudaMemcpyHostToDevice, B->stream);
+      if (nnz > 0) {
+        cudaMemcpyAsync(dc, colindex[s], sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, B->stream);
+        cudaMemcpyAsync(dv, values[s], sizeof(double) * nnz, cudaMemcpyHostToDevice, B->stream);
+      }
+      k_batch_from_csr<<<B->num_sms * 8, 256, 0, B->stream>>>(n, dr, dc, dv, B->off[s], B->npad, B->col,
+                                                               B->val, d_bad);
+      if (cudaStreamSynchronize(B->stream) != cudaSuccess) rc = set_cuda_error(cudaGetLastError(), "batch csr", __FILE__, __LINE__);
+    }
+    if (dr) cudaFree(dr);
+    if (dc) cudaFree(dc);
+    if (dv) cudaFree(dv);
+  }
+  if (!rc) {
+    cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, B->stream);
+    cudaStreamSynchronize(B->stream);
+    if (bad) rc = HPCCG_ERR_INVALID_ARG;
+  }
+  if (d_bad) cudaFree(d_bad);
+  if (!rc) rc = batch_pad_rows(B);
+  if (rc) {
+    batch_free(B);
+    return rc;
+  }
+  *out = B;
+  return HPCCG_OK;
+}
+
+extern "C" void hpccg_batch_destroy(hpccg_batch *B) {
+  if (B) batch_free(B);
+}
+
+extern "C" int hpccg_batch_info(const hpccg_batch *B, int32_t *nsys, int64_t *stacked_rows,
+                                int64_t *row_offsets) {
+  if (!B) return HPCCG_ERR_INVALID_ARG;
+  if (nsys) *nsys = B->nsys;
+  if (stacked_rows) *stacked_rows = B->npad;
+  if (row_offsets)
+    for (int s = 0; s < B->nsys; ++s) {
+      row_offsets[2 * s] = B->off[s];
+      row_offsets[2 * s + 1] = B->n[s];
+    }
+  return HPCCG_OK;
+}
+
+static BatchArgs batch_args(hpccg_batch *B, int precision) {
+  BatchArgs g{};
+  g.nsys = B->nsys;
+  g.ntiles = B->ntiles;
+  g.tiles = B->d_tiles;
+  g.sys_chunk0 = B->d_sys_chunk0;
+  g.npad = B->npad;
+  g.col = B->col;
+  g.val = B->val;
+  g.val_lp = precision == HPCCG_PREC_BF16 ? (const void *)B->val16 : (const void *)B->val32;
+  g.x = B->x;
+  g.b = B->b;
+  g.r = B->r;
+  g.p = B->p;
+  g.Ap = B->Ap;
+  g.r32 = B->r32;
+  g.p32 = B->p32;
+  g.Ap32 = B->Ap32;
+  g.d32 = B->d32;
+  g.part = B->part;
+  g.counter = B->counter;
+  g.sys = B->sys;
+  return g;
+}
+
+static int grid_of(const hpccg_batch *B) { return B->num_sms * B->blocks_per_sm; }
+
+template <class Ph>
+static cudaError_t phase(hpccg_batch *B, const BatchArgs &g, cudaStream_t s) {
+  k_batch_phase<Ph><<<grid_of(B), 256, 0, s>>>(g);
+  return cudaGetLastError();
+}
+
+static cudaError_t launch_cg64_body(hpccg_batch *B, const BatchArgs &g, cudaStream_t s) {
+  k_batch_p64<<<grid_of(B), 256, 0, s>>>(g);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = phase<PhSpmvDot64>(B, g, s);
+  if (e == cudaSuccess) e = phase<PhUpdate64>(B, g, s);
+  return e;
+}
+
+template <typename VT>
+static cudaError_t launch_inner_body(hpccg_batch *B, const BatchArgs &g, cudaStream_t s) {
+  k_batch_p32<<<grid_of(B), 256, 0, s>>>(g);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = phase<PhSpmvDotLp<VT>>(B, g, s);
+  if (e == cudaSuccess) e = phase<PhUpdateLp>(B, g, s);
+  return e;
+}
+
+template <typename VT>
+static cudaError_t launch_outer_body(hpccg_batch *B, const BatchArgs &g, cudaStream_t s,
+                                     cudaGraph_t og, bool graph) {
+  cudaError_t e = phase<PhStartInner>(B, g, s);
+  if (e != cudaSuccess) return e;
+  if (graph) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd);
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t node = nullptr;
+    if (e == cudaSuccess) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = g.c_inner;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      e = cudaGraphAddNode(&node, cg, deps, nd, &cp);
+    }
+    cudaStream_t is = nullptr;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&is, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(is, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        const cudaError_t e1 = launch_inner_body<VT>(B, g, is);
+        const cudaError_t e2 = cudaStreamEndCapture(is, &body);
+        e = e1 != cudaSuccess ? e1 : e2;
+      }
+      cudaStreamDestroy(is);
+    }
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+  } else {
+    for (;;) {
+      int any = 0;
+      std::vector<BatchSys> hs(B->nsys);
+      e = cudaMemcpyAsync(hs.data(), B->sys, sizeof(BatchSys) * B->nsys, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return e;
+      for (auto &y : hs) any |= y.inner_active;
+      if (!any) break;
+      if ((e = launch_inner_body<VT>(B, g, s)) != cudaSuccess) return e;
+    }
+  }
+  if (e != cudaSuccess) return e;
+  k_batch_end_inner<<<grid_of(B), 256, 0, s>>>(g);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = phase<PhOuter64>(B, g, s);
+  return e;
+}
+
+constexpr int kBatchMaxOuter = 30;  // refinement cycles per system (mixed precision)
+
+// Captures the solver for one precision as a graph (or runs it eagerly).  The
+// solve parameters travel in the kernel arguments, so a graph is rebuilt when
+// they or the schedule change.
+static int run_batch(hpccg_batch *B, int precision, bool eager, double rel_tol, int max_iter) {
+  cudaStream_t s = B->stream;
+  BatchArgs g = batch_args(B, precision);
+  g.rel_tol = rel_tol;
+  g.max_iter = max_iter;
+  g.max_inner = max_iter;
+  g.max_outer = kBatchMaxOuter;
+  g.inner_rtol = 0.0;
+  if (eager) {
+    g.use_cond = 0;
+    auto any_active = [&](int &any) -> cudaError_t {
+      std::vector<BatchSys> hs(B->nsys);
+      cudaError_t e = cudaMemcpyAsync(hs.data(), B->sys, sizeof(BatchSys) * B->nsys, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      any = 0;
+      for (auto &y : hs) any |= y.active;
+      return e;
+    };
+    HPCCG_CUDA(phase<PhBnorm>(B, g, s));
+    if (precision == HPCCG_PREC_FP64) {
+      HPCCG_CUDA(phase<PhInit64>(B, g, s));
+      for (;;) {
+        int any = 0;
+        HPCCG_CUDA(any_active(any));
+        if (!any) break;
+        HPCCG_CUDA(launch_cg64_body(B, g, s));
+      }
+      HPCCG_CUDA(phase<PhResidual64>(B, g, s));
+    } else {
+      HPCCG_CUDA(phase<PhOuter64>(B, g, s));
+      for (;;) {
+        int any = 0;
+        HPCCG_CUDA(any_active(any));
+        if (!any) break;
+        cudaError_t e = precision == HPCCG_PREC_BF16 ? launch_outer_body<__nv_bfloat16>(B, g, s, nullptr, false)
+                                                     : launch_outer_body<float>(B, g, s, nullptr, false);
+        HPCCG_CUDA(e);
+      }
+    }
+    return HPCCG_OK;
+  }
+  if (!B->exec[precision] || B->exec_tile[precision] != B->tile_chunks || B->exec_bps[precision] != B->blocks_per_sm ||
+      B->exec_tol[precision] != rel_tol || B->exec_maxit[precision] != max_iter) {
+    if (B->exec[precision]) cudaGraphExecDestroy(B->exec[precision]);
+    B->exec[precision] = nullptr;
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    cudaGraphConditionalHandle ho = 0, hi = 0;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&ho, cg, 0, cudaGraphCondAssignDefault);
+    g.c_outer = ho;
+    g.use_cond = 1;
+    if (e == cudaSuccess) e = phase<PhBnorm>(B, g, s);
+    if (e == cudaSuccess) e = precision == HPCCG_PREC_FP64 ? phase<PhInit64>(B, g, s) : phase<PhOuter64>(B, g, s);
+    cudaGraphNode_t node = nullptr;
+    cudaGraphNodeParams cp = {};
+    if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd);
+    if (e == cudaSuccess) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = ho;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      e = cudaGraphAddNode(&node, cg, deps, nd, &cp);
+    }
+    cudaStream_t bs = nullptr;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      if (precision != HPCCG_PREC_FP64) e = cudaGraphConditionalHandleCreate(&hi, body, 0, 0);
+      g.c_inner = hi;
+      if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        cudaError_t e1;
+        if (precision == HPCCG_PREC_FP64) e1 = launch_cg64_body(B, g, bs);
+        else if (precision == HPCCG_PREC_BF16) e1 = launch_outer_body<__nv_bfloat16>(B, g, bs, body, true);
+        else e1 = launch_outer_body<float>(B, g, bs, body, true);
+        const cudaError_t e2 = cudaStreamEndCapture(bs, &body);
+        e = e1 != cudaSuccess ? e1 : e2;
+      }
+      cudaStreamDestroy(bs);
+    }
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess && precision == HPCCG_PREC_FP64) e = phase<PhResidual64>(B, g, s);
+    cudaGraph_t outg = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(s, &outg);
+    if (e == cudaSuccess) e = ee;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&B->exec[precision], outg, 0);
+    if (outg) cudaGraphDestroy(outg);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return set_cuda_error(e, "build batch graph", __FILE__, __LINE__);
+    }
+    B->exec_tile[precision] = B->tile_chunks;
+    B->exec_bps[precision] = B->blocks_per_sm;
+    B->exec_tol[precision] = rel_tol;
+    B->exec_maxit[precision] = max_iter;
+  }
+  HPCCG_CUDA(cudaGraphLaunch(B->exec[precision], s));
+  return HPCCG_OK;
+}
+
+__global__ void k_batch_to_lp(const double *src, float *f32, __nv_bfloat16 *b16, size_t count) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+    if (f32) f32[i] = (float)src[i];
+    if (b16) b16[i] = __double2bfloat16(src[i]);
+  }
+}
+
+static int ensure_lp(hpccg_batch *B, int precision) {
+  const size_t slots = (size_t)27 * B->npad;
+  if (precision == HPCCG_PREC_FP32 && !B->val32) {
+    HPCCG_CUDA(cudaMalloc(&B->val32, sizeof(float) * slots));
+    k_batch_to_lp<<<B->num_sms * 8, 256, 0, B->stream>>>(B->val, B->val32, nullptr, slots);
+  }
+  if (precision == HPCCG_PREC_BF16 && !B->val16) {
+    HPCCG_CUDA(cudaMalloc(&B->val16, sizeof(__nv_bfloat16) * slots));
+    k_batch_to_lp<<<B->num_sms * 8, 256, 0, B->stream>>>(B->val, nullptr, B->val16, slots);
+  }
+  HPCCG_CUDA(cudaStreamSynchronize(B->stream));
+  return HPCCG_OK;
+}
+
+// Times one FP64 SpMV+dot phase per candidate schedule and keeps the fastest.
+// Candidates differ only in tile size and grid, so the solves they produce are
+// bit-identical.
+static int autotune(hpccg_batch *B) {
+  if (B->tuned) return HPCCG_OK;
+  B->tuned = true;
+  const int tiles[] = {1, 2, 4, 8};
+  const int bps[] = {2, 4, 8};
+  float best = 1e30f;
+  int bt = 4, bb = 4;
+  std::vector<BatchSys> hs(B->nsys);
+  for (auto &y : hs) {
+    y = BatchSys{};
+    y.active = 1;
+    y.rtrans = 1.0;
+  }
+  for (int t : tiles)
+    for (int b : bps) {
+      int rc = build_tiles(B, t);
+      if (rc) return rc;
+      B->blocks_per_sm = b;
+      BatchArgs g = batch_args(B, HPCCG_PREC_FP64);
+      float ms = 0.f;
+      for (int rep = 0; rep < 4; ++rep) {
+        HPCCG_CUDA(cudaMemcpyAsync(B->sys, hs.data(), sizeof(BatchSys) * B->nsys, cudaMemcpyHostToDevice, B->stream));
+        if (rep == 1) HPCCG_CUDA(cudaEventRecord(B->ev0, B->stream));
+        HPCCG_CUDA(phase<PhSpmvDot64>(B, g, B->stream));
+      }
+      HPCCG_CUDA(cudaEventRecord(B->ev1, B->stream));
+      HPCCG_CUDA(cudaEventSynchronize(B->ev1));
+      HPCCG_CUDA(cudaEventElapsedTime(&ms, B->ev0, B->ev1));
+      if (ms < best) {
+        best = ms;
+        bt = t;
+        bb = b;
+      }
+    }
+  B->blocks_per_sm = bb;
+  return build_tiles(B, bt);
+}
+
+extern "C" int hpccg_batch_set_schedule(hpccg_batch *B, int32_t tile_chunks, int32_t blocks_per_sm) {
+  if (!B || tile_chunks < 0 || blocks_per_sm < 0 || tile_chunks > 64 || blocks_per_sm > 16) return HPCCG_ERR_INVALID_ARG;
+  if (tile_chunks == 0 || blocks_per_sm == 0) {
+    B->tuned = false;
+    return HPCCG_OK;
+  }
+  B->tuned = true;
+  B->blocks_per_sm = blocks_per_sm;
+  return build_tiles(B, tile_chunks);
+}
+
+extern "C" int hpccg_batch_get_schedule(const hpccg_batch *B, int32_t *tile_chunks, int32_t *blocks_per_sm) {
+  if (!B) return HPCCG_ERR_INVALID_ARG;
+  if (tile_chunks) *tile_chunks = B->tile_chunks;
+  if (blocks_per_sm) *blocks_per_sm = B->blocks_per_sm;
+  return HPCCG_OK;
+}
+
+extern "C" int hpccg_batch_spmv(hpccg_batch *B, const double *d_x, double *d_y) {
+  if (!B || !d_x || !d_y || d_x == d_y) return HPCCG_ERR_INVALID_ARG;
+  BatchArgs g = batch_args(B, HPCCG_PREC_FP64);
+  k_batch_spmv<<<grid_of(B), 256, 0, B->stream>>>(g, d_x, d_y);
+  HPCCG_CUDA(cudaGetLastError());
+  HPCCG_CUDA(cudaStreamSynchronize(B->stream));
+  return HPCCG_OK;
+}
+
+extern "C" int hpccg_batch_solve(hpccg_batch *B, const double *d_b, double *d_x, int32_t precision,
+                                 double rel_tol, int32_t max_iter, int32_t *iters, double *relres,
+                                 int32_t *outer) {
+  if (!B || !d_b || !d_x || !(rel_tol >= 0.0) || max_iter < 0) return HPCCG_ERR_INVALID_ARG;
+  if (precision != HPCCG_PREC_FP64 && precision != HPCCG_PREC_FP32 && precision != HPCCG_PREC_BF16)
+    return HPCCG_ERR_INVALID_ARG;
+  int rc = autotune(B);
+  if (rc) return rc;
+  if (precision != HPCCG_PREC_FP64 && (rc = ensure_lp(B, precision))) return rc;
+  const size_t bytes = sizeof(double) * B->npad;
+  HPCCG_CUDA(cudaMemcpyAsync(B->b, d_b, bytes, cudaMemcpyDeviceToDevice, B->stream));
+  HPCCG_CUDA(cudaMemcpyAsync(B->x, d_x, bytes, cudaMemcpyDeviceToDevice, B->stream));
+  HPCCG_CUDA(cudaEventRecord(B->ev0, B->stream));
+  const bool eager = getenv("HPCCG_EAGER") && atoi(getenv("HPCCG_EAGER")) != 0;
+  rc = run_batch(B, precision, eager, rel_tol, max_iter);
+  if (rc) return rc;
+  HPCCG_CUDA(cudaEventRecord(B->ev1, B->stream));
+  HPCCG_CUDA(cudaMemcpyAsync(d_x, B->x, bytes, cudaMemcpyDeviceToDevice, B->stream));
+  std::vector<BatchSys> hs(B->nsys);
+  HPCCG_CUDA(cudaMemcpyAsync(hs.data(), B->sys, sizeof(BatchSys) * B->nsys, cudaMemcpyDeviceToHost, B->stream));
+  HPCCG_CUDA(cudaStreamSynchronize(B->stream));
+  HPCCG_CUDA(cudaEventElapsedTime(&B->last_ms, B->ev0, B->ev1));
+  int status = HPCCG_OK;
+  for (int s = 0; s < B->nsys; ++s) {
+    if (iters) iters[s] = hs[s].iters;
+    if (relres) relres[s] = hs[s].relres;
+    if (outer) outer[s] = hs[s].outer;
+    if (hs[s].status) status = hs[s].status;
+    else if (!hs[s].converged && status == HPCCG_OK) status = HPCCG_ERR_NOT_CONVERGED;
+  }
+  return status;
+}
+
+extern "C" int hpccg_batch_last_solve_ms(const hpccg_batch *B, float *ms) {
+  if (!B || !ms) return HPCCG_ERR_INVALID_ARG;
+  *ms = B->last_ms;
+  return HPCCG_OK;
+}

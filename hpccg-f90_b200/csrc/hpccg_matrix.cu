@@ -150,7 +150,7 @@ static int init_ctx_common(hpccg_ctx *c) {
   c->grid = std::min(kMaxPartials, c->num_sms * 8);
   HPCCG_CUDA(cudaMalloc(&c->d_partials, sizeof(double) * kMaxPartials));
   HPCCG_CUDA(cudaMalloc(&c->d_counter, sizeof(unsigned) * 16));
-  HPCCG_CUDA(cudaMemset(c->d_counter, 0, sizeof(unsigned) * 16));
+  HPCCG_CUDA(cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned) * 16, c->stream));
   HPCCG_CUDA(cudaMalloc(&c->d_state, sizeof(CgState)));
   return HPCCG_OK;
 }
@@ -169,7 +169,7 @@ static int alloc_matrix(hpccg_ctx *c, int32_t n, int64_t nnz, int W) {
   HPCCG_CUDA(cudaMalloc(&c->d_Ap, vec));
   HPCCG_CUDA(cudaMalloc(&c->d_x, vec));
   HPCCG_CUDA(cudaMalloc(&c->d_b, vec));
-  HPCCG_CUDA(cudaMemset(c->d_p, 0, vec));
+  HPCCG_CUDA(cudaMemsetAsync(c->d_p, 0, vec, c->stream));
   return HPCCG_OK;
 }
 

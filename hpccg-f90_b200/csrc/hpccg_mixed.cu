@@ -349,7 +349,7 @@ static int mixed_res(hpccg_ctx *c, int precision, MixedRes **out) {
     HPCCG_CUDA(cudaMalloc(&m->p, vec));
     HPCCG_CUDA(cudaMalloc(&m->Ap, vec));
     HPCCG_CUDA(cudaMalloc(&m->d, vec));
-    HPCCG_CUDA(cudaMemset(m->p, 0, vec));
+    HPCCG_CUDA(cudaMemsetAsync(m->p, 0, vec, c->stream));
     HPCCG_CUDA(cudaMalloc(&m->st, sizeof(MixedState)));
   }
   const size_t slots = (size_t)27 * c->npad;

@@ -83,6 +83,15 @@ _SIGS = {
     "hpccg_gpu_last_solve_ms": (_c.c_int, [_vp, _c.POINTER(_c.c_float)]),
     "hpccg_gpu_time_cg_kernels": (_c.c_int, [_vp, _i32, _c.POINTER(_c.c_float)]),
     "hpccg_gpu_ddot_noalloc": (_c.c_int, [_i32, _vp, _vp, _c.POINTER(_f64), _vp]),
+    "hpccg_batch_create_generated": (_c.c_int, [_i32, _i32p, _c.POINTER(_vp)]),
+    "hpccg_batch_create": (_c.c_int, [_i32, _i32p, _vp, _vp, _vp, _c.POINTER(_vp)]),
+    "hpccg_batch_destroy": (None, [_vp]),
+    "hpccg_batch_info": (_c.c_int, [_vp, _c.POINTER(_i32), _c.POINTER(_i64), _vp]),
+    "hpccg_batch_set_schedule": (_c.c_int, [_vp, _i32, _i32]),
+    "hpccg_batch_get_schedule": (_c.c_int, [_vp, _c.POINTER(_i32), _c.POINTER(_i32)]),
+    "hpccg_batch_spmv": (_c.c_int, [_vp, _vp, _vp]),
+    "hpccg_batch_solve": (_c.c_int, [_vp, _vp, _vp, _i32, _f64, _i32, _vp, _vp, _vp]),
+    "hpccg_batch_last_solve_ms": (_c.c_int, [_vp, _c.POINTER(_c.c_float)]),
     "hpccg_gpu_solve_mixed": (_c.c_int, [_vp, _f64p, _f64p, _i32, _f64, _i32, _i32, _f64, _vp]),
     "hpccg_gpu_solve_mixed_device": (_c.c_int, [_vp, _vp, _vp, _i32, _f64, _i32, _i32, _f64, _vp]),
     "hpccg_gpu_spmv_lowp": (_c.c_int, [_vp, _i32, _vp, _vp]),
@@ -324,4 +333,89 @@ class Matrix:
         _sync_torch()
         ms = _c.c_float(0.0)
         _check(_lib.hpccg_gpu_time_spmv(self._h, _dptr(d_x), _dptr(d_y), reps, _c.byref(ms)), "time_spmv")
+        return ms.value
+
+
+class Batch:
+    """Many independent systems solved together (hpccg_batch_* in the C-ABI).
+
+    Vectors are "stacked": system s occupies rows offsets[s] .. offsets[s]+nrows[s]
+    of one device vector of length stacked_rows (gaps between systems are zero)."""
+
+    def __init__(self, handle):
+        self._h = _vp(handle)
+        ns, rows = _i32(0), _i64(0)
+        _check(_lib.hpccg_batch_info(self._h, _c.byref(ns), _c.byref(rows), None), "batch_info")
+        self.nsys, self.stacked_rows = ns.value, rows.value
+        offs = np.zeros(2 * self.nsys, np.int64)
+        _check(_lib.hpccg_batch_info(self._h, None, None, offs.ctypes.data), "batch_info")
+        self.offsets, self.nrows = offs[0::2].copy(), offs[1::2].copy()
+
+    @classmethod
+    def generated(cls, sizes) -> "Batch":
+        sizes = np.ascontiguousarray(np.asarray(sizes, np.int32).reshape(-1))
+        h = _vp()
+        _check(_lib.hpccg_batch_create_generated(len(sizes) // 3, sizes, _c.byref(h)), "batch_create_generated")
+        return cls(h.value)
+
+    @classmethod
+    def from_csr(cls, systems) -> "Batch":
+        """systems: list of (rowindex, colindex, values) in the reference's 1-based layout."""
+        rows = [np.ascontiguousarray(r, np.int32) for r, _, _ in systems]
+        cols = [np.ascontiguousarray(c, np.int32) for _, c, _ in systems]
+        vals = [np.ascontiguousarray(v, np.float64) for _, _, v in systems]
+        n = len(systems)
+        nrows = np.array([len(r) - 1 for r in rows], np.int32)
+        P = _vp * n
+        h = _vp()
+        _check(_lib.hpccg_batch_create(n, nrows, P(*[r.ctypes.data for r in rows]), P(*[c.ctypes.data for c in cols]),
+                                       P(*[v.ctypes.data for v in vals]), _c.byref(h)), "batch_create")
+        return cls(h.value)
+
+    def close(self):
+        if self._h:
+            _lib.hpccg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stack(self, vectors):
+        out = np.zeros(self.stacked_rows, np.float64)
+        for s, v in enumerate(vectors):
+            out[self.offsets[s]:self.offsets[s] + self.nrows[s]] = v
+        return out
+
+    def unstack(self, stacked):
+        return [np.asarray(stacked[self.offsets[s]:self.offsets[s] + self.nrows[s]]) for s in range(self.nsys)]
+
+    def set_schedule(self, tile_chunks: int, blocks_per_sm: int):
+        _check(_lib.hpccg_batch_set_schedule(self._h, tile_chunks, blocks_per_sm), "batch_set_schedule")
+
+    def get_schedule(self):
+        t, b = _i32(0), _i32(0)
+        _check(_lib.hpccg_batch_get_schedule(self._h, _c.byref(t), _c.byref(b)), "batch_get_schedule")
+        return t.value, b.value
+
+    def spmv(self, d_x, d_y):
+        _sync_torch()
+        _check(_lib.hpccg_batch_spmv(self._h, _dptr(d_x), _dptr(d_y)), "batch_spmv")
+
+    def solve(self, d_b, d_x, precision: int = PREC_FP64, rel_tol: float = 1e-8, max_iter: int = 1000):
+        """Stacked device vectors.  Returns (iters, relres, outer, status) per system."""
+        _sync_torch()
+        iters = np.zeros(self.nsys, np.int32)
+        relres = np.zeros(self.nsys, np.float64)
+        outer = np.zeros(self.nsys, np.int32)
+        rc = _lib.hpccg_batch_solve(self._h, _dptr(d_b), _dptr(d_x), precision, rel_tol, max_iter,
+                                    iters.ctypes.data, relres.ctypes.data, outer.ctypes.data)
+        _check(rc, "batch_solve", allow=(HPCCG_OK, HPCCG_ERR_NOT_CONVERGED, HPCCG_ERR_BREAKDOWN))
+        return iters, relres, outer, rc
+
+    def last_solve_ms(self) -> float:
+        ms = _c.c_float(0.0)
+        _check(_lib.hpccg_batch_last_solve_ms(self._h, _c.byref(ms)), "batch_last_solve_ms")
         return ms.value

@@ -146,6 +146,48 @@ int hpccg_gpu_set_mixed_rows_per_thread(hpccg_ctx *ctx, int32_t precision, int32
  * r update + r.r), each launched `reps` times back to back. */
 int hpccg_gpu_time_mixed_kernels(hpccg_ctx *ctx, int32_t precision, int32_t reps, float *ms);
 
+/* ---- batched solves of many independent systems ------------------------
+ *
+ * No single reference routine: the reference solves one system per run.  A
+ * batch stacks independent systems block-diagonally (each system's rows start
+ * on a 512-row boundary of one "stacked" vector).  One persistent kernel per
+ * CG phase walks tiles of every system that is still active; the loop runs
+ * on the device in one CUDA graph.  Each system stops on its own at
+ * ||b_s - A_s x_s|| <= rel_tol ||b_s||.  Dot products are reduced per
+ * 512-row chunk in a fixed order, so results do not depend on the tile
+ * schedule the autotuner picks. */
+typedef struct hpccg_batch hpccg_batch;
+
+/* generate_matrix systems: sizes[3s..3s+2] = nx, ny, nz of system s. */
+int hpccg_batch_create_generated(int32_t nsys, const int32_t *sizes, hpccg_batch **batch);
+/* Systems given as reference-layout CSRs (1-based; at most 27 entries a row). */
+int hpccg_batch_create(int32_t nsys, const int32_t *nrows, const int32_t *const *rowindex,
+                       const int32_t *const *colindex, const double *const *values,
+                       hpccg_batch **batch);
+void hpccg_batch_destroy(hpccg_batch *batch);
+/* stacked_rows: length of the stacked vectors; row_offsets (nullable, 2*nsys):
+ * [2s] = first stacked row of system s, [2s+1] = its row count. */
+int hpccg_batch_info(const hpccg_batch *batch, int32_t *nsys, int64_t *stacked_rows,
+                     int64_t *row_offsets);
+/* Tile size in 512-row chunks and resident blocks per SM of the phase
+ * kernels; (0, 0) re-enables the autotuner (run on the next solve). */
+int hpccg_batch_set_schedule(hpccg_batch *batch, int32_t tile_chunks, int32_t blocks_per_sm);
+int hpccg_batch_get_schedule(const hpccg_batch *batch, int32_t *tile_chunks, int32_t *blocks_per_sm);
+/* y = A x over all systems (stacked device vectors). */
+int hpccg_batch_spmv(hpccg_batch *batch, const double *d_x, double *d_y);
+/* Solves every system.  d_b / d_x are stacked device vectors (x: x0 in,
+ * solution out).  precision HPCCG_PREC_FP64: CG per system (max_iter caps the
+ * iterations); HPCCG_PREC_FP32 / HPCCG_PREC_BF16: per-system FP64 iterative
+ * refinement around an inner CG (max_iter caps each inner solve, at most 30
+ * cycles).  Host outputs (nullable, nsys each): iterations (inner iterations
+ * for the refinement solvers), final FP64 relative residual, refinement
+ * cycles.  Returns HPCCG_ERR_NOT_CONVERGED if any system missed rel_tol. */
+int hpccg_batch_solve(hpccg_batch *batch, const double *d_b, double *d_x, int32_t precision,
+                      double rel_tol, int32_t max_iter, int32_t *iters, double *relres,
+                      int32_t *outer);
+/* Device ms of the last hpccg_batch_solve (events around the graph launch). */
+int hpccg_batch_last_solve_ms(const hpccg_batch *batch, float *ms);
+
 /* ---- op-level drop-ins (device arrays), MPI/src/SparseMatrix.F90:213-232
  *      and MPI/src/vector_operations.F90:40-169 ------------------------------ */
 

@@ -1,0 +1,143 @@
+"""Batched solves of independent systems (stacked, one persistent kernel per phase).
+
+Bars: per system, the FP64 true residual recomputed by the CPU oracle meets
+rel_tol; the FP64 batch takes the same iteration count as the oracle's CG to
+the same residual (+-1 for a borderline stop); the iterates do not depend on
+the tile schedule (bit-identical); CSR input equals generated input.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+FP64, FP32, BF16 = 0, 1, 2
+SIZES = [(3, 5, 7), (16, 16, 16), (1, 1, 1), (20, 9, 13), (12, 12, 12), (2, 2, 2), (31, 17, 5)]
+
+
+@pytest.fixture(scope="module")
+def hp():
+    import hpccg_b200
+    return hpccg_b200
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    return t
+
+
+def _systems(sizes, seed=7):
+    out = []
+    for s, (nx, ny, nz) in enumerate(sizes):
+        A, x, b1, xe = oracle.generate_matrix(nx, ny, nz)
+        xs = oracle.uniform_pm1(seed + s, A.nrow)
+        out.append((A, oracle.spmv(A, xs), xs))
+    return out
+
+
+def _oracle_iters(A, b, rel_tol):
+    """Iterations plain CG needs for ||r_j|| <= rel_tol ||b|| (the reference's hist[j+1] = ||r_j||)."""
+    _, it, _, hist = oracle.cg(A, b, np.zeros_like(b), 500, 0.0)
+    tol = rel_tol * np.linalg.norm(b)
+    r = hist[1:]  # r[j] = ||r_j||
+    hit = np.nonzero(~(r > tol))[0]
+    return int(hit[0]) if len(hit) else None
+
+
+@pytest.mark.parametrize("prec", [FP64, FP32, BF16])
+def test_batch_solve_per_system(hp, torch, prec):
+    sysl = _systems(SIZES)
+    B = hp.Batch.generated(SIZES)
+    assert B.nsys == len(SIZES) and list(B.nrows) == [a * b * c for a, b, c in SIZES]
+    assert all(o % 512 == 0 for o in B.offsets)
+    db = torch.from_numpy(B.stack([b for _, b, _ in sysl])).cuda()
+    dx = torch.zeros_like(db)
+    iters, relres, outer, st = B.solve(db, dx, prec, 1e-8, 1000)
+    assert st == hp.HPCCG_OK
+    xs = B.unstack(dx.cpu().numpy())
+    for s, (A, b, xstar) in enumerate(sysl):
+        rel = oracle.true_relres(A, b, xs[s])
+        assert rel <= 1e-8, (s, rel)
+        assert relres[s] == pytest.approx(rel, rel=1e-6, abs=1e-15)
+        assert np.abs(xs[s] - xstar).max() <= 1e-6
+        if prec == FP64:
+            want = _oracle_iters(A, b, 1e-8)
+            assert want is not None and abs(int(iters[s]) - want) <= 1, (s, iters[s], want)
+        else:
+            assert outer[s] >= 1
+
+
+def test_batch_schedule_independent(hp, torch):
+    sysl = _systems(SIZES)
+    B = hp.Batch.generated(SIZES)
+    db = torch.from_numpy(B.stack([b for _, b, _ in sysl])).cuda()
+    ref = None
+    for sched in [(1, 2), (4, 4), (8, 8), (2, 3)]:
+        B.set_schedule(*sched)
+        assert B.get_schedule() == sched
+        for prec in (FP64, BF16):
+            dx = torch.zeros_like(db)
+            iters, relres, outer, st = B.solve(db, dx, prec, 1e-8, 1000)
+            got = (dx.cpu().numpy(), iters.copy())
+            if ref is None:
+                ref = {}
+            if prec in ref:
+                assert np.array_equal(got[0], ref[prec][0]) and np.array_equal(got[1], ref[prec][1]), sched
+            else:
+                ref[prec] = got
+    B.set_schedule(0, 0)  # back to the autotuner
+    dx = torch.zeros_like(db)
+    B.solve(db, dx, FP64, 1e-8, 1000)
+    assert np.array_equal(dx.cpu().numpy(), ref[FP64][0])
+
+
+def test_batch_from_csr_equals_generated(hp, torch):
+    sizes = SIZES[:4]
+    sysl = _systems(sizes)
+    G = hp.Batch.generated(sizes)
+    C = hp.Batch.from_csr([(A.rowindex, A.colindex, A.values) for A, _, _ in sysl])
+    assert list(C.offsets) == list(G.offsets)
+    db = torch.from_numpy(G.stack([b for _, b, _ in sysl])).cuda()
+    out = []
+    for B in (G, C):
+        dx = torch.zeros_like(db)
+        B.solve(db, dx, FP64, 1e-8, 1000)
+        out.append(dx.cpu().numpy())
+    assert np.array_equal(out[0], out[1])
+
+
+def test_batch_spmv_bit_exact(hp, torch):
+    sysl = _systems(SIZES)
+    B = hp.Batch.generated(SIZES)
+    dx = torch.from_numpy(B.stack([xs for _, _, xs in sysl])).cuda()
+    dy = torch.empty_like(dx)
+    B.spmv(dx, dy)
+    ys = B.unstack(dy.cpu().numpy())
+    for s, (A, b, xs) in enumerate(sysl):
+        assert np.array_equal(ys[s], b)
+
+
+def test_batch_iteration_cap_reports_not_converged(hp, torch):
+    sysl = _systems(SIZES[:2])
+    B = hp.Batch.generated(SIZES[:2])
+    db = torch.from_numpy(B.stack([b for _, b, _ in sysl])).cuda()
+    dx = torch.zeros_like(db)
+    iters, relres, outer, st = B.solve(db, dx, FP64, 1e-8, 3)
+    assert st == hp.HPCCG_ERR_NOT_CONVERGED
+    assert iters.max() <= 3 and relres.max() > 1e-8
+
+
+def test_batch_eager_equals_graph(hp, torch, monkeypatch):
+    sysl = _systems(SIZES[:3])
+    B = hp.Batch.generated(SIZES[:3])
+    db = torch.from_numpy(B.stack([b for _, b, _ in sysl])).cuda()
+    res = []
+    for eager in ("0", "1"):
+        monkeypatch.setenv("HPCCG_EAGER", eager)
+        for prec in (FP64, FP32):
+            dx = torch.zeros_like(db)
+            B.solve(db, dx, prec, 1e-8, 1000)
+            res.append(dx.cpu().numpy())
+    assert np.array_equal(res[0], res[2]) and np.array_equal(res[1], res[3])
