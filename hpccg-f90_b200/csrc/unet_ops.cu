@@ -1,0 +1,291 @@
+// unet_ops.cu -- CUDA-core kernels of the U-Net: the 1-channel input conv and
+// small-volume convs, weight packing for the tcgen05 convs, pooling,
+// upsampling, ReLU masks, weight/bias gradients, the output projection, the
+// loss and the Adam update.  All are memory-bound or tiny.
+#include "unet_ops.cuh"
+
+namespace hpccg {
+
+// ---- weight packing ------------------------------------------------------------------
+// Forward B operand of input group `in`: packed[in][tap][kc][co][j] =
+// W[tap][in*16 + kc*8 + j][co] (W is FP32 [27][cin][16]).
+__global__ void k_pack_fwd(const float *W, int cin, int nin, __nv_bfloat16 *packed) {
+  const int total = nin * 27 * 256;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const int j = e & 7, co = (e >> 3) & 15, kc = (e >> 7) & 1, tap = (e >> 8) % 27, in = (e >> 8) / 27;
+    packed[e] = __float2bfloat16(W[((size_t)tap * cin + in * 16 + kc * 8 + j) * 16 + co]);
+  }
+}
+// Backward-data operand for the gradient w.r.t. input group g: a conv over dY
+// (16 channels) with taps flipped and in/out transposed:
+// packed[tap][kc][ci][j] = W[26 - tap][g*16 + ci][kc*8 + j].
+__global__ void k_pack_bwd(const float *W, int cin, int g, __nv_bfloat16 *packed) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 27 * 256; e += gridDim.x * blockDim.x) {
+    const int j = e & 7, ci = (e >> 3) & 15, kc = (e >> 7) & 1, tap = e >> 8;
+    packed[e] = __float2bfloat16(W[((size_t)(26 - tap) * cin + g * 16 + ci) * 16 + kc * 8 + j]);
+  }
+}
+// The same flipped/transposed weights in FP32 [27][16][16] for the CUDA-core conv.
+__global__ void k_flip_fp32(const float *W, int cin, int g, float *Wf) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 27 * 256; e += gridDim.x * blockDim.x) {
+    const int ci = e & 15, co = (e >> 4) & 15, tap = e >> 8;  // Wf[tap][co as input][ci as output]
+    Wf[e] = W[((size_t)(26 - tap) * cin + g * 16 + ci) * 16 + co];
+  }
+}
+
+// ---- direct conv on CUDA cores --------------------------------------------------------
+// out[v][co] = sum_tap sum_ci in[v + off(tap)][ci] * W[tap][ci][co] (+ bias, ReLU).
+// Inputs: in0/in1 BF16 channels-last 16-channel tensors (in1 nullable), or
+// in_f32 one-channel FP32 (cin = 1).  One thread per output voxel.
+__global__ void k_conv3_cc(CcConvArgs a) {
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int64_t nvox = (int64_t)nx * ny * nz * a.nb;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvox; v += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)((v / ((int64_t)nx * ny)) % nz);
+    const int64_t b = v / ((int64_t)nx * ny * nz);
+    float acc[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) acc[c] = 0.f;
+    for (int tap = 0; tap < 27; ++tap) {
+      const int xx = x + tap % 3 - 1, yy = y + (tap / 3) % 3 - 1, zz = z + tap / 9 - 1;
+      if (xx < 0 || xx >= nx || yy < 0 || yy >= ny || zz < 0 || zz >= nz) continue;
+      const int64_t u = ((b * nz + zz) * ny + yy) * nx + xx;
+      if (a.in_f32) {
+        const float s = a.in_f32[u];
+        const float *w = a.W + (size_t)tap * 16;
+#pragma unroll
+        for (int c = 0; c < 16; ++c) acc[c] = fmaf(s, w[c], acc[c]);
+        continue;
+      }
+      for (int g = 0; g < a.nin; ++g) {
+        const __nv_bfloat16 *src = (g ? a.in1 : a.in0) + u * 16;
+        for (int ci = 0; ci < 16; ++ci) {
+          const float s = __bfloat162float(src[ci]);
+          const float *w = a.W + ((size_t)tap * a.cin + g * 16 + ci) * 16;
+#pragma unroll
+          for (int c = 0; c < 16; ++c) acc[c] = fmaf(s, w[c], acc[c]);
+        }
+      }
+    }
+    if (a.epi == kEpiRawF32) {
+      float *o = static_cast<float *>(a.out) + v * 16;
+#pragma unroll
+      for (int c = 0; c < 16; ++c) o[c] = acc[c];
+    } else if (a.epi == kEpiProject) {
+      float r = a.proj[16];
+#pragma unroll
+      for (int c = 0; c < 16; ++c) r = fmaf(a.proj[c], fmaxf(acc[c] + a.bias[c], 0.f), r);
+      static_cast<float *>(a.out)[v] = r;
+    } else {
+      __nv_bfloat16 *o = static_cast<__nv_bfloat16 *>(a.out) + v * 16;
+#pragma unroll
+      for (int c = 0; c < 16; ++c) {
+        float t = acc[c] + (a.bias ? a.bias[c] : 0.f);
+        if (a.epi == kEpiBiasRelu) t = fmaxf(t, 0.f);
+        o[c] = __float2bfloat16(t);
+      }
+    }
+  }
+}
+
+// ---- resampling --------------------------------------------------------------------------
+// 2x2x2 average pooling of a 16-channel BF16 tensor (fine dims nx,ny,nz even).
+__global__ void k_pool(const __nv_bfloat16 *in, __nv_bfloat16 *out, int nx, int ny, int nz, int nb) {
+  const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
+  const int64_t n = (int64_t)cx * cy * cz * nb * 16;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(e & 15);
+    int64_t v = e >> 4;
+    const int x = (int)(v % cx), y = (int)((v / cx) % cy), z = (int)((v / ((int64_t)cx * cy)) % cz);
+    const int64_t b = v / ((int64_t)cx * cy * cz);
+    float s = 0.f;
+    for (int k = 0; k < 8; ++k) {
+      const int64_t u = ((b * nz + 2 * z + (k >> 2)) * ny + 2 * y + ((k >> 1) & 1)) * nx + 2 * x + (k & 1);
+      s += __bfloat162float(in[u * 16 + c]);
+    }
+    out[e] = __float2bfloat16(0.125f * s);
+  }
+}
+// Nearest-neighbour 2x upsampling: fine (nx,ny,nz) from coarse (nx/2,...).
+__global__ void k_upsample(const __nv_bfloat16 *in, __nv_bfloat16 *out, int nx, int ny, int nz, int nb) {
+  const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
+  const int64_t n = (int64_t)nx * ny * nz * nb * 2;  // 16-byte (8-channel) units
+  const uint4 *src = reinterpret_cast<const uint4 *>(in);
+  uint4 *dst = reinterpret_cast<uint4 *>(out);
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int h = (int)(e & 1);
+    const int64_t v = e >> 1;
+    const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)((v / ((int64_t)nx * ny)) % nz);
+    const int64_t b = v / ((int64_t)nx * ny * nz);
+    const int64_t u = ((b * cz + z / 2) * cy + y / 2) * cx + x / 2;
+    dst[e] = src[u * 2 + h];
+  }
+}
+// Backward of pooling: d_fine += d_coarse / 8 (FP32 16-channel tensors).
+__global__ void k_pool_bwd(const float *dc, float *df, int nx, int ny, int nz, int nb) {
+  const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
+  const int64_t n = (int64_t)nx * ny * nz * nb * 16;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(e & 15);
+    const int64_t v = e >> 4;
+    const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)((v / ((int64_t)nx * ny)) % nz);
+    const int64_t b = v / ((int64_t)nx * ny * nz);
+    const int64_t u = ((b * cz + z / 2) * cy + y / 2) * cx + x / 2;
+    df[e] += 0.125f * dc[u * 16 + c];
+  }
+}
+// Backward of nearest upsampling: d_coarse = sum of the 8 fine children.
+__global__ void k_up_bwd(const float *df, float *dc, int nx, int ny, int nz, int nb) {
+  const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
+  const int64_t n = (int64_t)cx * cy * cz * nb * 16;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(e & 15);
+    const int64_t v = e >> 4;
+    const int x = (int)(v % cx), y = (int)((v / cx) % cy), z = (int)((v / ((int64_t)cx * cy)) % cz);
+    const int64_t b = v / ((int64_t)cx * cy * cz);
+    float s = 0.f;
+    for (int k = 0; k < 8; ++k) {
+      const int64_t u = ((b * nz + 2 * z + (k >> 2)) * ny + 2 * y + ((k >> 1) & 1)) * nx + 2 * x + (k & 1);
+      s += df[u * 16 + c];
+    }
+    dc[e] = s;
+  }
+}
+// dpre = d * (act > 0), to BF16 (the next backward conv's input) and optionally FP32.
+__global__ void k_relu_mask(const float *d, const __nv_bfloat16 *act, __nv_bfloat16 *out, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    out[e] = __float2bfloat16(__bfloat162float(act[e]) > 0.f ? d[e] : 0.f);
+}
+__global__ void k_add_f32(const float *src, float *dst, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+    dst[e] += src[e];
+}
+
+// ---- gradients --------------------------------------------------------------------------------
+// Per block partial of dW[tap][ci][co] = sum_v X[v+off(tap)][ci] dY[v][co] and
+// dbias[co] = sum_v dY[v][co] over the voxels v = blockIdx.x, +gridDim.x, ...
+// Task t < 27*cin is (tap, ci); task 27*cin is the bias.  partial layout:
+// [block][27*cin + 1][16].  A fixed grid and a fixed block-order reduction
+// (k_reduce_partials) keep the gradients deterministic.
+__global__ void __launch_bounds__(256) k_dW(DwArgs a) {
+  const int ntask = 27 * a.cin + 1;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int64_t nvox = (int64_t)nx * ny * nz * a.nb;
+  __shared__ float sdy[64][16];
+  for (int task0 = 0; task0 < ntask; task0 += blockDim.x) {
+    const int task = task0 + threadIdx.x;
+    float acc[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) acc[c] = 0.f;
+    const int tap = task < 27 * a.cin ? task / a.cin : 0, ci = task < 27 * a.cin ? task % a.cin : 0;
+    const int ox = tap % 3 - 1, oy = (tap / 3) % 3 - 1, oz = tap / 9 - 1;
+    for (int64_t v0 = (int64_t)blockIdx.x * 64; v0 < nvox; v0 += (int64_t)gridDim.x * 64) {
+      __syncthreads();
+      for (int e = threadIdx.x; e < 64 * 16; e += blockDim.x) {
+        const int64_t v = v0 + e / 16;
+        sdy[e / 16][e % 16] = v < nvox ? __bfloat162float(a.dy[v * 16 + e % 16]) : 0.f;
+      }
+      __syncthreads();
+      if (task >= ntask) continue;
+      for (int j = 0; j < 64 && v0 + j < nvox; ++j) {
+        const int64_t v = v0 + j;
+        float s = 1.f;
+        if (task < 27 * a.cin) {
+          const int x = (int)(v % nx) + ox, y = (int)((v / nx) % ny) + oy, z = (int)((v / ((int64_t)nx * ny)) % nz) + oz;
+          if (x < 0 || x >= nx || y < 0 || y >= ny || z < 0 || z >= nz) continue;
+          const int64_t b = v / ((int64_t)nx * ny * nz);
+          const int64_t u = ((b * nz + z) * ny + y) * nx + x;
+          if (a.x_f32) s = a.x_f32[u];
+          else s = __bfloat162float(ci < 16 ? a.x0[u * 16 + ci] : a.x1[u * 16 + ci - 16]);
+        }
+#pragma unroll
+        for (int c = 0; c < 16; ++c) acc[c] = fmaf(s, sdy[j][c], acc[c]);
+      }
+    }
+    if (task < ntask) {
+      float *o = a.partial + ((size_t)blockIdx.x * ntask + task) * 16;
+#pragma unroll
+      for (int c = 0; c < 16; ++c) o[c] = acc[c];
+    }
+  }
+}
+// grad[k] (+)= sum over blocks of partial[block][k], k < n, in block order.
+__global__ void k_reduce_partials(const float *partial, int nblocks, int n, float *grad, int accumulate) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int b = 0; b < nblocks; ++b) s += partial[(size_t)b * n + k];
+    grad[k] = accumulate ? grad[k] + s : s;
+  }
+}
+
+// Output projection (training path): out[v] = proj . act[v] + proj_b.
+__global__ void k_proj_fwd(const __nv_bfloat16 *act, const float *proj, float *out, int64_t nvox) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvox; v += (int64_t)gridDim.x * blockDim.x) {
+    float r = proj[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) r = fmaf(proj[c], __bfloat162float(act[v * 16 + c]), r);
+    out[v] = r;
+  }
+}
+// d act = proj * dOut (masked by act > 0, to BF16); per-block partials of
+// dproj[c] = sum act[v][c] dOut[v] and dproj_b = sum dOut[v] ([block][17]).
+__global__ void __launch_bounds__(256) k_proj_bwd(const __nv_bfloat16 *act, const float *proj, const float *dout,
+                                                  __nv_bfloat16 *dact, float *partial, int64_t nvox) {
+  __shared__ float red[17][256];
+  float acc[17];
+#pragma unroll
+  for (int c = 0; c < 17; ++c) acc[c] = 0.f;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvox; v += (int64_t)gridDim.x * blockDim.x) {
+    const float d = dout[v];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const float av = __bfloat162float(act[v * 16 + c]);
+      acc[c] = fmaf(av, d, acc[c]);
+      dact[v * 16 + c] = __float2bfloat16(av > 0.f ? proj[c] * d : 0.f);
+    }
+    acc[16] += d;
+  }
+#pragma unroll
+  for (int c = 0; c < 17; ++c) red[c][threadIdx.x] = acc[c];
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int c = 0; c < 17; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 17) partial[(size_t)blockIdx.x * 17 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// Mean squared error over n values and dL/dout; per-block loss partials.
+__global__ void __launch_bounds__(256) k_mse(const float *out, const float *tgt, float *dout, float *partial,
+                                             int64_t n) {
+  __shared__ float red[256];
+  float s = 0.f;
+  const float scale = 2.f / (float)n;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const float e = out[v] - tgt[v];
+    s += e * e;
+    dout[v] = scale * e;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+__global__ void k_adam(float *p, const float *g, float *m, float *v, int n, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const float gk = g[k];
+    const float mk = b1 * m[k] + (1.f - b1) * gk;
+    const float vk = b2 * v[k] + (1.f - b2) * gk * gk;
+    m[k] = mk;
+    v[k] = vk;
+    p[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
+  }
+}
+
+}  // namespace hpccg

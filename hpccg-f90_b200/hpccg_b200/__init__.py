@@ -92,6 +92,16 @@ _SIGS = {
     "hpccg_batch_spmv": (_c.c_int, [_vp, _vp, _vp]),
     "hpccg_batch_solve": (_c.c_int, [_vp, _vp, _vp, _i32, _f64, _i32, _vp, _vp, _vp]),
     "hpccg_batch_last_solve_ms": (_c.c_int, [_vp, _c.POINTER(_c.c_float)]),
+    "hpccg_unet_create": (_c.c_int, [_c.c_uint64, _c.POINTER(_vp)]),
+    "hpccg_unet_destroy": (None, [_vp]),
+    "hpccg_unet_num_params": (_c.c_int, [_vp, _c.POINTER(_i64)]),
+    "hpccg_unet_get_params": (_c.c_int, [_vp, _vp]),
+    "hpccg_unet_set_params": (_c.c_int, [_vp, _vp]),
+    "hpccg_unet_forward": (_c.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, _vp]),
+    "hpccg_unet_loss_grad": (_c.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, _vp, _c.POINTER(_c.c_float), _vp]),
+    "hpccg_unet_adam_step": (_c.c_int, [_vp, _c.c_float, _c.c_float, _c.c_float, _c.c_float]),
+    "hpccg_unet_time_forward": (_c.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, _vp, _c.POINTER(_c.c_float)]),
+    "hpccg_unet_conv3_layer": (_c.c_int, [_i32, _i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _vp]),
     "hpccg_gpu_solve_mixed": (_c.c_int, [_vp, _f64p, _f64p, _i32, _f64, _i32, _i32, _f64, _vp]),
     "hpccg_gpu_solve_mixed_device": (_c.c_int, [_vp, _vp, _vp, _i32, _f64, _i32, _i32, _f64, _vp]),
     "hpccg_gpu_spmv_lowp": (_c.c_int, [_vp, _i32, _vp, _vp]),
@@ -418,4 +428,72 @@ class Batch:
     def last_solve_ms(self) -> float:
         ms = _c.c_float(0.0)
         _check(_lib.hpccg_batch_last_solve_ms(self._h, _c.byref(ms)), "batch_last_solve_ms")
+        return ms.value
+
+
+def conv3_layer(d_in0, d_in1, d_w, d_bias, d_proj, epi: int, path: int, d_out, nx, ny, nz, nb=1):
+    """One 3x3x3 conv with 16 outputs (test entry): torch device tensors, BF16 inputs."""
+    _sync_torch()
+    nin = 1 if d_in1 is None else 2
+    p = lambda t: None if t is None else _dptr(t)  # noqa: E731
+    _check(_lib.hpccg_unet_conv3_layer(nx, ny, nz, nb, nin, p(d_in0), p(d_in1), p(d_w), p(d_bias), p(d_proj), epi,
+                                       path, p(d_out)), "conv3_layer")
+
+
+class Unet:
+    """The learned preconditioner network (hpccg_unet_* in the C-ABI)."""
+
+    def __init__(self, seed: int = 1):
+        h = _vp()
+        _check(_lib.hpccg_unet_create(seed, _c.byref(h)), "unet_create")
+        self._h = h
+        n = _i64(0)
+        _check(_lib.hpccg_unet_num_params(self._h, _c.byref(n)), "unet_num_params")
+        self.nparams = n.value
+
+    def close(self):
+        if self._h:
+            _lib.hpccg_unet_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def get_params(self):
+        out = np.empty(self.nparams, np.float32)
+        _check(_lib.hpccg_unet_get_params(self._h, out.ctypes.data), "unet_get_params")
+        return out
+
+    def set_params(self, params):
+        params = np.ascontiguousarray(params, np.float32)
+        assert params.size == self.nparams
+        _check(_lib.hpccg_unet_set_params(self._h, params.ctypes.data), "unet_set_params")
+
+    def forward(self, d_in, d_out, nx, ny, nz, nb=1):
+        _sync_torch()
+        _check(_lib.hpccg_unet_forward(self._h, nx, ny, nz, nb, _dptr(d_in), _dptr(d_out)), "unet_forward")
+
+    def loss_grad(self, d_in, d_target, nx, ny, nz, nb=1, want_grad=False):
+        _sync_torch()
+        loss = _c.c_float(0.0)
+        g = np.empty(self.nparams, np.float32) if want_grad else None
+        _check(_lib.hpccg_unet_loss_grad(self._h, nx, ny, nz, nb, _dptr(d_in), _dptr(d_target), _c.byref(loss),
+                                         g.ctypes.data if want_grad else None), "unet_loss_grad")
+        return (loss.value, g) if want_grad else loss.value
+
+    def adam_step(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
+        _check(_lib.hpccg_unet_adam_step(self._h, lr, beta1, beta2, eps), "unet_adam_step")
+
+    def time_forward(self, d_in, d_out, nx, ny, nz, reps=10) -> float:
+        _sync_torch()
+        ms = _c.c_float(0.0)
+        _check(_lib.hpccg_unet_time_forward(self._h, nx, ny, nz, reps, _dptr(d_in), _dptr(d_out), _c.byref(ms)),
+               "unet_time_forward")
         return ms.value

@@ -188,6 +188,44 @@ int hpccg_batch_solve(hpccg_batch *batch, const double *d_b, double *d_x, int32_
 /* Device ms of the last hpccg_batch_solve (events around the graph launch). */
 int hpccg_batch_last_solve_ms(const hpccg_batch *batch, float *ms);
 
+/* ---- learned preconditioner: a 3D U-Net -----------------------------------
+ *
+ * No reference counterpart (the reference's CG is unpreconditioned).  A
+ * 4-level U-Net with 16 channels at every level (104,337 parameters), BF16
+ * activations on tcgen05 tensor cores with FP32 accumulation, FP32 master
+ * weights; input and output are one FP32 channel on an nx*ny*nz grid (each a
+ * multiple of 8), batches stacked along a slowest batch dimension. */
+typedef struct hpccg_unet hpccg_unet;
+
+/* He-uniform weights from the project's generator (seed), zero biases. */
+int hpccg_unet_create(uint64_t seed, hpccg_unet **unet);
+void hpccg_unet_destroy(hpccg_unet *unet);
+int hpccg_unet_num_params(const hpccg_unet *unet, int64_t *nparams);
+/* Flat FP32 parameter vector (host), layer by layer: W[27][cin][16], bias[16];
+ * then the 16->1 projection (16 weights, 1 bias). */
+int hpccg_unet_get_params(const hpccg_unet *unet, float *host_params);
+int hpccg_unet_set_params(hpccg_unet *unet, const float *host_params);
+/* out = net(in) for nb stacked grids (device FP32 arrays of nb*nx*ny*nz). */
+int hpccg_unet_forward(hpccg_unet *unet, int32_t nx, int32_t ny, int32_t nz, int32_t nb, const float *d_in,
+                       float *d_out);
+/* Mean squared error against d_target and its gradient w.r.t. every
+ * parameter (kept on the device; copied to grad_host when non-null). */
+int hpccg_unet_loss_grad(hpccg_unet *unet, int32_t nx, int32_t ny, int32_t nz, int32_t nb, const float *d_in,
+                         const float *d_target, float *loss, float *grad_host);
+/* One Adam update with the gradient of the last hpccg_unet_loss_grad. */
+int hpccg_unet_adam_step(hpccg_unet *unet, float lr, float beta1, float beta2, float eps);
+/* Average ms of `reps` forward passes on one grid. */
+int hpccg_unet_time_forward(hpccg_unet *unet, int32_t nx, int32_t ny, int32_t nz, int32_t reps,
+                            const float *d_in, float *d_out, float *ms);
+/* One 3x3x3 conv layer with 16 outputs, for tests: BF16 channels-last inputs
+ * (nin = 1 or 2 groups of 16 channels), weights FP32 [27][16*nin][16],
+ * epi 0 = bias+ReLU (BF16 out), 1 = bias (BF16), 2 = bias+ReLU then the 16->1
+ * projection d_proj (FP32 out), 3 = raw FP32 16-channel out; path 0 =
+ * tcgen05, 1 = CUDA cores. */
+int hpccg_unet_conv3_layer(int32_t nx, int32_t ny, int32_t nz, int32_t nb, int32_t nin, const void *d_in0,
+                           const void *d_in1, const float *d_w, const float *d_bias, const float *d_proj,
+                           int32_t epi, int32_t path, void *d_out);
+
 /* ---- op-level drop-ins (device arrays), MPI/src/SparseMatrix.F90:213-232
  *      and MPI/src/vector_operations.F90:40-169 ------------------------------ */
 

@@ -1,0 +1,63 @@
+"""The U-Net kernels against the float64 numpy oracle (oracle/unet_oracle.py).
+
+Bars: a conv layer on tcgen05 (BF16 operands, FP32 accumulation) matches the
+oracle on the same BF16-rounded operands within 1e-3 relative to the output
+scale (plus BF16 output rounding, 2^-8 relative); the CUDA-core conv matches
+with FP32 weights; the full forward pass matches within 3e-2 of the output
+scale (BF16 activations between layers); every layer's gradient block matches
+the oracle's within 6e-2 relative (norm of the difference over norm).
+"""
+import numpy as np
+import pytest
+
+import unet_oracle as uo
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env():
+    import torch
+
+    import hpccg_b200 as hp
+    return torch, hp
+
+
+def _bf16_tensor(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda().to(torch.bfloat16).contiguous()
+
+
+SHAPES = [(16, 16, 16, 1), (32, 8, 8, 2), (128, 4, 2, 1), (8, 8, 8, 3), (64, 16, 8, 1)]
+
+
+@pytest.mark.parametrize("nx,ny,nz,nb", SHAPES)
+@pytest.mark.parametrize("nin", [1, 2])
+@pytest.mark.parametrize("epi", [0, 1, 2, 3])
+def test_conv_layer_tc_and_cc(env, nx, ny, nz, nb, nin, epi):
+    torch, hp = env
+    rng = np.random.default_rng(nx * 131 + nin * 7 + epi)
+    xs = [uo.bf16_round(rng.normal(0, 1, (nb, nz, ny, nx, 16))) for _ in range(nin)]
+    W = rng.normal(0, 0.1, (27, 16 * nin, 16)).astype(np.float32)
+    b = rng.normal(0, 0.1, 16).astype(np.float32)
+    proj = rng.normal(0, 0.3, 17).astype(np.float32)
+    x = np.concatenate(xs, -1).astype(np.float64)
+    dW, db, dp = (torch.from_numpy(v).cuda() for v in (W, b, proj))
+    din = [_bf16_tensor(torch, v) for v in xs] + [None]
+    for path, Wref in ((0, uo.bf16_round(W)), (1, W)):
+        pre = uo.conv3(x, Wref.astype(np.float64))
+        if epi == 3:
+            want = pre
+            out = torch.empty((nb, nz, ny, nx, 16), dtype=torch.float32, device="cuda")
+        elif epi == 2:
+            want = np.maximum(pre + b, 0) @ proj[:16].astype(np.float64) + proj[16]
+            out = torch.empty((nb, nz, ny, nx), dtype=torch.float32, device="cuda")
+        else:
+            want = pre + b
+            if epi == 0:
+                want = np.maximum(want, 0)
+            out = torch.empty((nb, nz, ny, nx, 16), dtype=torch.bfloat16, device="cuda")
+        hp.conv3_layer(din[0], din[1], dW, db, dp, epi, path, out, nx, ny, nz, nb)
+        got = out.float().cpu().numpy().astype(np.float64)
+        scale = np.abs(want).max() + 1e-30
+        tol = 1e-3 * scale + (2.0 ** -8 * np.abs(want) if epi in (0, 1) else 0)
+        assert np.all(np.abs(got - want) <= tol), (path, np.abs(got - want).max(), scale)
