@@ -574,3 +574,17 @@ extern "C" int hpccg_unet_conv3_layer(int32_t nx, int32_t ny, int32_t nz, int32_
   if (!rc && err) rc = HPCCG_ERR_TIMEOUT;
   return rc;
 }
+
+// Forward pass of one grid on a caller's stream (used inside solvers); no
+// host synchronisation.
+extern "C" int hpccg_unet_forward_on(hpccg_unet *u, int32_t nx, int32_t ny, int32_t nz, const float *d_in,
+                                     float *d_out, cudaStream_t stream) {
+  if (!u || !d_in || !d_out) return HPCCG_ERR_INVALID_ARG;
+  int rc = ensure_shape(u, nx, ny, nz, 1, false);
+  if (rc) return rc;
+  cudaStream_t keep = u->stream;
+  u->stream = stream;
+  rc = forward(u, d_in, d_out, false);
+  u->stream = keep;
+  return rc;
+}

@@ -226,6 +226,23 @@ int hpccg_unet_conv3_layer(int32_t nx, int32_t ny, int32_t nz, int32_t nb, int32
                            const void *d_in1, const float *d_w, const float *d_bias, const float *d_proj,
                            int32_t epi, int32_t path, void *d_out);
 
+/* Flexible (Polak-Ribiere) preconditioned CG on the nx*ny*nz grid of the
+ * context's generate_matrix system, preconditioner z = s * net(r/s) with
+ * s = rms(r).  All vectors, dot products and the convergence test are FP64;
+ * plain CG (z = r) takes over when the preconditioned iteration stalls (no
+ * 10% residual reduction in 5 iterations) or r.z <= 0, and the FP64 true
+ * residual b - A x decides convergence.  unet = NULL runs plain CG.  Device
+ * arrays; x holds x0 on entry. */
+typedef struct hpccg_fcg_info {
+  int32_t iters;      /* CG iterations (SpMVs) */
+  int32_t nn_applies; /* network applications */
+  int32_t fallback;   /* 1 if plain CG took over */
+  int32_t status;
+  double relres;      /* final FP64 ||b - A x|| / ||b|| */
+} hpccg_fcg_info;
+int hpccg_gpu_solve_fcg(hpccg_ctx *ctx, hpccg_unet *unet, int32_t nx, int32_t ny, int32_t nz, const double *d_b,
+                        double *d_x, double rel_tol, int32_t max_iter, hpccg_fcg_info *info);
+
 /* ---- op-level drop-ins (device arrays), MPI/src/SparseMatrix.F90:213-232
  *      and MPI/src/vector_operations.F90:40-169 ------------------------------ */
 

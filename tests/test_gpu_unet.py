@@ -61,3 +61,47 @@ def test_conv_layer_tc_and_cc(env, nx, ny, nz, nb, nin, epi):
         scale = np.abs(want).max() + 1e-30
         tol = 1e-3 * scale + (2.0 ** -8 * np.abs(want) if epi in (0, 1) else 0)
         assert np.all(np.abs(got - want) <= tol), (path, np.abs(got - want).max(), scale)
+
+
+def _net_and_params(hp, seed=3):
+    net = hp.Unet(seed)
+    p = net.get_params().astype(np.float64)
+    # non-trivial biases so every ReLU sees both signs
+    rng = np.random.default_rng(seed)
+    p = p + rng.normal(0, 0.02, p.size)
+    net.set_params(p.astype(np.float32))
+    return net, net.get_params().astype(np.float64)
+
+
+def test_forward_matches_oracle(env):
+    torch, hp = env
+    net, p = _net_and_params(hp)
+    assert net.nparams == 104337
+    rng = np.random.default_rng(5)
+    r = rng.normal(0, 1, (2, 16, 16, 16))
+    want = uo.forward(p, r)
+    din = torch.from_numpy(r.astype(np.float32)).cuda()
+    dout = torch.empty_like(din)
+    net.forward(din, dout, 16, 16, 16, 2)
+    got = dout.cpu().numpy()
+    scale = np.abs(want).max()
+    assert np.abs(got - want).max() <= 3e-2 * scale, (np.abs(got - want).max(), scale)
+
+
+def test_gradients_match_oracle(env):
+    torch, hp = env
+    net, p = _net_and_params(hp, seed=9)
+    rng = np.random.default_rng(6)
+    r = rng.normal(0, 1, (1, 16, 16, 16))
+    t = rng.normal(0, 0.05, (1, 16, 16, 16))
+    loss_ref, g_ref = uo.loss_grad(p, r, t)
+    din = torch.from_numpy(r.astype(np.float32)).cuda()
+    dt = torch.from_numpy(t.astype(np.float32)).cuda()
+    loss, g = net.loss_grad(din, dt, 16, 16, 16, 1, want_grad=True)
+    assert loss == pytest.approx(loss_ref, rel=5e-2)
+    off, n = uo.offsets()
+    for l in range(14):
+        a, b = off[l], (off[l + 1] if l < 13 else n)
+        ref = g_ref[a:b]
+        err = np.linalg.norm(g[a:b] - ref) / (np.linalg.norm(ref) + 1e-30)
+        assert err <= 6e-2, (l, err)
