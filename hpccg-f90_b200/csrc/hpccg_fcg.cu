@@ -5,6 +5,7 @@
 // iteration stalls or loses positivity, and the FP64 true residual b - A x
 // decides convergence.
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 
 #include <algorithm>
@@ -225,6 +226,7 @@ extern "C" int hpccg_gpu_solve_fcg(hpccg_ctx *c, hpccg_unet *u, int32_t nx, int3
     return read_state();
   };
   bool use_net = u != nullptr;
+  const bool trace = getenv("HPCCG_FCG_TRACE") != nullptr;
   rc = residual();
   if (!rc) rc = read_state();
   double rnorm = sqrt(h.rr);
@@ -263,6 +265,9 @@ extern "C" int hpccg_gpu_solve_fcg(hpccg_ctx *c, hpccg_unet *u, int32_t nx, int3
       break;
     }
     rnorm = sqrt(h.rr);
+    if (trace)
+      fprintf(stderr, "fcg it %d relres %.3e rz %.3e beta %.3e pAp %.3e net %d\n", iters, rnorm / bnorm, rz, beta,
+              h.pAp, use_net ? 1 : 0);
     if (rnorm < 0.9 * best) {
       best = rnorm;
       since_best = 0;

@@ -63,6 +63,7 @@ struct hpccg_unet {
   float *g[4] = {}, *gs[4] = {}, *gt[4] = {};
   __nv_bfloat16 *pre[4] = {};
   float *out_train = nullptr, *dout = nullptr;
+  int loss_kind = 0;  // 0 = mean squared error, 1 = energy norm of the HPCCG operator
   std::vector<void *> act_allocs;
 };
 
@@ -169,6 +170,12 @@ static int conv(hpccg_unet *u, int layer, int level, const __nv_bfloat16 *in0, c
     a.err = u->d_err;
     return launch_conv3_tc(nin, epi, maps, a, u->num_sms, u->stream);
   }
+  if (in_f32 && (epi == kEpiBiasRelu || epi == kEpiBias)) {  // the 1-channel input layer
+    k_conv3_in1<<<grid1d(u, Lv.nvox), 256, 0, u->stream>>>(in_f32, W, bias, static_cast<__nv_bfloat16 *>(out),
+                                                          Lv.nx, Lv.ny, Lv.nz, u->nb, epi == kEpiBiasRelu);
+    HPCCG_CUDA(cudaGetLastError());
+    return HPCCG_OK;
+  }
   CcConvArgs a;
   a.nx = Lv.nx;
   a.ny = Lv.ny;
@@ -200,13 +207,13 @@ static int forward(hpccg_unet *u, const float *in, float *out, bool train) {
   const Level *L = u->L;
   UNET_TRY(conv(u, 0, 0, nullptr, nullptr, in, kEpiBiasRelu, u->e1a));
   UNET_TRY(conv(u, 1, 0, u->e1a, nullptr, nullptr, kEpiBiasRelu, u->e1b));
-  k_pool<<<grid1d(u, L[1].nvox * 16), 256, 0, u->stream>>>(u->e1b, u->d1, L[0].nx, L[0].ny, L[0].nz, u->nb);
+  k_pool<<<grid1d(u, L[1].nvox * 2), 256, 0, u->stream>>>(u->e1b, u->d1, L[0].nx, L[0].ny, L[0].nz, u->nb);
   UNET_TRY(conv(u, 2, 1, u->d1, nullptr, nullptr, kEpiBiasRelu, u->e2a));
   UNET_TRY(conv(u, 3, 1, u->e2a, nullptr, nullptr, kEpiBiasRelu, u->e2b));
-  k_pool<<<grid1d(u, L[2].nvox * 16), 256, 0, u->stream>>>(u->e2b, u->d2, L[1].nx, L[1].ny, L[1].nz, u->nb);
+  k_pool<<<grid1d(u, L[2].nvox * 2), 256, 0, u->stream>>>(u->e2b, u->d2, L[1].nx, L[1].ny, L[1].nz, u->nb);
   UNET_TRY(conv(u, 4, 2, u->d2, nullptr, nullptr, kEpiBiasRelu, u->e3a));
   UNET_TRY(conv(u, 5, 2, u->e3a, nullptr, nullptr, kEpiBiasRelu, u->e3b));
-  k_pool<<<grid1d(u, L[3].nvox * 16), 256, 0, u->stream>>>(u->e3b, u->d3, L[2].nx, L[2].ny, L[2].nz, u->nb);
+  k_pool<<<grid1d(u, L[3].nvox * 2), 256, 0, u->stream>>>(u->e3b, u->d3, L[2].nx, L[2].ny, L[2].nz, u->nb);
   UNET_TRY(conv(u, 6, 3, u->d3, nullptr, nullptr, kEpiBiasRelu, u->e4a));
   UNET_TRY(conv(u, 7, 3, u->e4a, nullptr, nullptr, kEpiBiasRelu, u->e4b));
   k_upsample<<<grid1d(u, L[2].nvox * 2), 256, 0, u->stream>>>(u->e4b, u->u3, L[2].nx, L[2].ny, L[2].nz, u->nb);
@@ -466,7 +473,10 @@ extern "C" int hpccg_unet_loss_grad(hpccg_unet *u, int32_t nx, int32_t ny, int32
   if ((rc = forward(u, d_in, u->out_train, true))) return rc;
   const int64_t n = u->L[0].nvox;
   const int mb = std::min(u->partial_blocks, grid1d(u, n));
-  k_mse<<<mb, 256, 0, u->stream>>>(u->out_train, d_target, u->dout, u->partial, n);
+  if (u->loss_kind == 1)
+    k_energy<<<mb, 256, 0, u->stream>>>(u->out_train, d_target, u->dout, u->partial, nx, ny, nz, nb);
+  else
+    k_mse<<<mb, 256, 0, u->stream>>>(u->out_train, d_target, u->dout, u->partial, n);
   std::vector<float> lp(mb);
   HPCCG_CUDA(cudaMemcpyAsync(lp.data(), u->partial, sizeof(float) * mb, cudaMemcpyDeviceToHost, u->stream));
   HPCCG_CUDA(cudaStreamSynchronize(u->stream));
@@ -478,6 +488,12 @@ extern "C" int hpccg_unet_loss_grad(hpccg_unet *u, int32_t nx, int32_t ny, int32
     HPCCG_CUDA(cudaMemcpyAsync(grad_host, u->grads, sizeof(float) * u->nparams, cudaMemcpyDeviceToHost, u->stream));
   }
   return check_err(u);
+}
+
+extern "C" int hpccg_unet_set_loss(hpccg_unet *u, int32_t kind) {
+  if (!u || kind < 0 || kind > 1) return HPCCG_ERR_INVALID_ARG;
+  u->loss_kind = kind;
+  return HPCCG_OK;
 }
 
 extern "C" int hpccg_unet_adam_step(hpccg_unet *u, float lr, float beta1, float beta2, float eps) {

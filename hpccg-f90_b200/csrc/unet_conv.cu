@@ -211,12 +211,14 @@ int make_act_tmap(CUtensorMap *map, const void *base, const ConvGeom &g) {
 template <int NIN, int EPI>
 static int launch_one(const CUtensorMap *maps, const ConvArgs &a, int num_sms, cudaStream_t s) {
   constexpr size_t smem = NIN * 27 * kWTapBytes + kConvStages * kTapBytes + 32 * 8 + 64;
-  static bool configured = false;
-  if (!configured) {
+  static int per_sm = 0;
+  if (!per_sm) {
     HPCCG_CUDA(cudaFuncSetAttribute(k_conv3_tc<NIN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = true;
+    HPCCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3_tc<NIN, EPI>, kConvThreads, smem));
+    if (per_sm < 1) per_sm = 1;
   }
-  const int grid = std::min(a.g.ntiles, num_sms * 2);
+  // every resident CTA keeps kConvStages TMA loads in flight
+  const int grid = std::min(a.g.ntiles, num_sms * per_sm);
   k_conv3_tc<NIN, EPI><<<grid, kConvThreads, smem, s>>>(maps[0], NIN > 1 ? maps[1] : maps[0], a);
   HPCCG_CUDA(cudaGetLastError());
   return HPCCG_OK;

@@ -22,7 +22,7 @@
 namespace hpccg {
 
 constexpr int kConvThreads = 192;
-constexpr int kConvStages = 8;
+constexpr int kConvStages = 24;
 constexpr int kTapBytes = 2 * 128 * 16;  // one k-step of A: 2 boxes x 128 voxels x 16 bytes
 constexpr int kWTapBytes = 16 * 16 * 2;  // one tap of B: 16 x 16 BF16
 

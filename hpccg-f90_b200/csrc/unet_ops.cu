@@ -88,22 +88,75 @@ __global__ void k_conv3_cc(CcConvArgs a) {
   }
 }
 
+// The 1-channel input layer: out[v][co] = act(sum_tap in[v+off] W[tap][co] + b[co]),
+// weights and bias staged in shared memory, two 16-byte BF16 stores per voxel.
+__global__ void __launch_bounds__(256) k_conv3_in1(const float *in, const float *W, const float *bias,
+                                                   __nv_bfloat16 *out, int nx, int ny, int nz, int nb, int relu) {
+  __shared__ float sw[27 * 16 + 16];
+  for (int e = threadIdx.x; e < 27 * 16 + 16; e += blockDim.x) sw[e] = e < 27 * 16 ? W[e] : bias[e - 27 * 16];
+  __syncthreads();
+  const int64_t nvox = (int64_t)nx * ny * nz * nb;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvox; v += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)((v / ((int64_t)nx * ny)) % nz);
+    float acc[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) acc[c] = sw[27 * 16 + c];
+#pragma unroll
+    for (int tap = 0; tap < 27; ++tap) {
+      const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
+      const bool inside = (unsigned)(x + dx) < (unsigned)nx && (unsigned)(y + dy) < (unsigned)ny &&
+                          (unsigned)(z + dz) < (unsigned)nz;
+      const float s = inside ? __ldg(in + v + dx + (int64_t)dy * nx + (int64_t)dz * nx * ny) : 0.f;
+#pragma unroll
+      for (int c = 0; c < 16; ++c) acc[c] = fmaf(s, sw[tap * 16 + c], acc[c]);
+    }
+    uint32_t w[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      float lo = acc[2 * c], hi = acc[2 * c + 1];
+      if (relu) {
+        lo = fmaxf(lo, 0.f);
+        hi = fmaxf(hi, 0.f);
+      }
+      const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+      w[c] = *reinterpret_cast<const uint32_t *>(&h);
+    }
+    uint4 *o = reinterpret_cast<uint4 *>(out + v * 16);
+    o[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+  }
+}
+
 // ---- resampling --------------------------------------------------------------------------
-// 2x2x2 average pooling of a 16-channel BF16 tensor (fine dims nx,ny,nz even).
+// 2x2x2 average pooling of a 16-channel BF16 tensor (fine dims nx,ny,nz even);
+// one thread per coarse voxel and 8-channel half, 16-byte loads.
 __global__ void k_pool(const __nv_bfloat16 *in, __nv_bfloat16 *out, int nx, int ny, int nz, int nb) {
   const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
-  const int64_t n = (int64_t)cx * cy * cz * nb * 16;
+  const int64_t n = (int64_t)cx * cy * cz * nb * 2;
+  const uint4 *src = reinterpret_cast<const uint4 *>(in);
+  uint4 *dst = reinterpret_cast<uint4 *>(out);
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(e & 15);
-    int64_t v = e >> 4;
+    const int h = (int)(e & 1);
+    const int64_t v = e >> 1;
     const int x = (int)(v % cx), y = (int)((v / cx) % cy), z = (int)((v / ((int64_t)cx * cy)) % cz);
     const int64_t b = v / ((int64_t)cx * cy * cz);
-    float s = 0.f;
+    float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (int k = 0; k < 8; ++k) {
       const int64_t u = ((b * nz + 2 * z + (k >> 2)) * ny + 2 * y + ((k >> 1) & 1)) * nx + 2 * x + (k & 1);
-      s += __bfloat162float(in[u * 16 + c]);
+      const uint4 q = src[u * 2 + h];
+      const __nv_bfloat162 *p2 = reinterpret_cast<const __nv_bfloat162 *>(&q);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const float2 f = __bfloat1622float2(p2[c]);
+        s[2 * c] += f.x;
+        s[2 * c + 1] += f.y;
+      }
     }
-    out[e] = __float2bfloat16(0.125f * s);
+    uint4 o;
+    __nv_bfloat162 *o2 = reinterpret_cast<__nv_bfloat162 *>(&o);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) o2[c] = __floats2bfloat162_rn(0.125f * s[2 * c], 0.125f * s[2 * c + 1]);
+    dst[e] = o;
   }
 }
 // Nearest-neighbour 2x upsampling: fine (nx,ny,nz) from coarse (nx/2,...).
@@ -266,6 +319,38 @@ __global__ void __launch_bounds__(256) k_mse(const float *out, const float *tgt,
     const float e = out[v] - tgt[v];
     s += e * e;
     dout[v] = scale * e;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+// Energy-norm loss of the HPCCG operator A (the 27-point generate_matrix
+// stencil: 27 on the diagonal, -1 for each neighbour inside the grid):
+// L = (1/n) d.(A d), d = target - out, per grid of the batch; dL/dout = -(2/n) A d.
+__global__ void __launch_bounds__(256) k_energy(const float *out, const float *tgt, float *dout, float *partial,
+                                                int nx, int ny, int nz, int nb) {
+  __shared__ float red[256];
+  const int64_t n = (int64_t)nx * ny * nz * nb;
+  const float scale = 2.f / (float)n;
+  float s = 0.f;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)((v / ((int64_t)nx * ny)) % nz);
+    const int64_t b = v / ((int64_t)nx * ny * nz);
+    float ad = 0.f;
+    for (int t = 0; t < 27; ++t) {
+      const int xx = x + t % 3 - 1, yy = y + (t / 3) % 3 - 1, zz = z + t / 9 - 1;
+      if (xx < 0 || xx >= nx || yy < 0 || yy >= ny || zz < 0 || zz >= nz) continue;
+      const int64_t u = ((b * nz + zz) * ny + yy) * nx + xx;
+      const float du = tgt[u] - out[u];
+      ad += (t == 13 ? 27.f : -1.f) * du;
+    }
+    s += (tgt[v] - out[v]) * ad;
+    dout[v] = -scale * ad;
   }
   red[threadIdx.x] = s;
   __syncthreads();

@@ -28,6 +28,8 @@ __global__ void k_pack_fwd(const float *W, int cin, int nin, __nv_bfloat16 *pack
 __global__ void k_pack_bwd(const float *W, int cin, int g, __nv_bfloat16 *packed);
 __global__ void k_flip_fp32(const float *W, int cin, int g, float *Wf);
 __global__ void k_conv3_cc(CcConvArgs a);
+__global__ void k_conv3_in1(const float *in, const float *W, const float *bias, __nv_bfloat16 *out, int nx, int ny,
+                            int nz, int nb, int relu);
 __global__ void k_pool(const __nv_bfloat16 *in, __nv_bfloat16 *out, int nx, int ny, int nz, int nb);
 __global__ void k_upsample(const __nv_bfloat16 *in, __nv_bfloat16 *out, int nx, int ny, int nz, int nb);
 __global__ void k_pool_bwd(const float *dc, float *df, int nx, int ny, int nz, int nb);
@@ -40,6 +42,8 @@ __global__ void k_proj_fwd(const __nv_bfloat16 *act, const float *proj, float *o
 __global__ void k_proj_bwd(const __nv_bfloat16 *act, const float *proj, const float *dout, __nv_bfloat16 *dact,
                            float *partial, int64_t nvox);
 __global__ void k_mse(const float *out, const float *tgt, float *dout, float *partial, int64_t n);
+__global__ void k_energy(const float *out, const float *tgt, float *dout, float *partial, int nx, int ny, int nz,
+                         int nb);
 __global__ void k_adam(float *p, const float *g, float *m, float *v, int n, float lr, float b1, float b2, float eps,
                        float c1, float c2);
 

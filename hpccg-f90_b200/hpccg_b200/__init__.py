@@ -99,6 +99,7 @@ _SIGS = {
     "hpccg_unet_set_params": (_c.c_int, [_vp, _vp]),
     "hpccg_unet_forward": (_c.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, _vp]),
     "hpccg_unet_loss_grad": (_c.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, _vp, _c.POINTER(_c.c_float), _vp]),
+    "hpccg_unet_set_loss": (_c.c_int, [_vp, _i32]),
     "hpccg_unet_adam_step": (_c.c_int, [_vp, _c.c_float, _c.c_float, _c.c_float, _c.c_float]),
     "hpccg_unet_time_forward": (_c.c_int, [_vp, _i32, _i32, _i32, _i32, _vp, _vp, _c.POINTER(_c.c_float)]),
     "hpccg_unet_conv3_layer": (_c.c_int, [_i32, _i32, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _i32, _i32, _vp]),
@@ -487,6 +488,10 @@ class Unet:
         _check(_lib.hpccg_unet_loss_grad(self._h, nx, ny, nz, nb, _dptr(d_in), _dptr(d_target), _c.byref(loss),
                                          g.ctypes.data if want_grad else None), "unet_loss_grad")
         return (loss.value, g) if want_grad else loss.value
+
+    def set_loss(self, kind: int):
+        """0 = mean squared error, 1 = energy norm of the HPCCG operator."""
+        _check(_lib.hpccg_unet_set_loss(self._h, kind), "unet_set_loss")
 
     def adam_step(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
         _check(_lib.hpccg_unet_adam_step(self._h, lr, beta1, beta2, eps), "unet_adam_step")

@@ -80,6 +80,59 @@ def make_pairs(M: Matrix, n: int, seeds, ks, torch):
     return torch.stack(ins), torch.stack(tgts)
 
 
+def fcg_pairs(M: Matrix, net: Unet, n: int, seeds, ks, torch):
+    """Residual->error pairs from the flexible PCG with the current network: the
+    residuals the preconditioner meets when it is used (x_k = k FCG iterations
+    from 0), so later training rounds cover them."""
+    N = n ** 3
+    ins, tgts = [], []
+    x = torch.zeros(N, dtype=torch.float64, device="cuda")
+    xk = torch.zeros_like(x)
+    r = torch.empty_like(x)
+    for sd in seeds:
+        b = gaussian_random_field(M, n, sd, torch)
+        bn = float(torch.linalg.vector_norm(b))
+        x.zero_()
+        M.cg_device(b, x, 2000, 1e-12 * bn, history=False)
+        for k in ks:
+            xk.zero_()
+            solve_fcg(M, net, n, b, xk, rel_tol=1e-14, max_iter=k)
+            M.spmv(xk, r)
+            M.waxpby(1.0, b, -1.0, r, r)
+            s = float(torch.sqrt((r * r).mean()))
+            if not s > 0:
+                continue
+            ins.append((r / s).float())
+            tgts.append(((x - xk) / s).float())
+    return torch.stack(ins), torch.stack(tgts)
+
+
+def train_preconditioner(n: int = 64, seed: int = 1, rhs: int = 64, rounds: int = 3, steps: int = 400,
+                         batch: int = 4, lr: float = 2e-3, log=None):
+    """Train the U-Net as an FCG preconditioner on n^3 grids.
+
+    Round 0 learns from plain-CG residual->error pairs of `rhs` Gaussian random
+    field right-hand sides; each further round adds pairs from FCG runs with
+    the current network.  Loss: energy norm of the HPCCG operator."""
+    import torch
+
+    M = Matrix.generated(n, n, n)
+    net = Unet(seed)
+    net.set_loss(1)
+    seeds = list(range(1000 * seed, 1000 * seed + rhs))
+    ins, tgts = make_pairs(M, n, seeds, [0, 1, 2, 3, 5, 8, 12, 20, 30], torch)
+    hist = []
+    for rnd in range(rounds):
+        hist += train(net, ins, tgts, n, steps, batch=batch, lr=lr * (0.7 ** rnd), seed=rnd, log=log)
+        if rnd + 1 < rounds:
+            sub = seeds[rnd::rounds][: max(8, rhs // rounds)]
+            fi, ft = fcg_pairs(M, net, n, sub, [2, 4, 6, 9, 12, 16, 22, 30], torch)
+            ins, tgts = torch.cat([ins, fi]), torch.cat([tgts, ft])
+            if log:
+                log(f"round {rnd}: {fi.shape[0]} FCG pairs added, {ins.shape[0]} total")
+    return net, hist
+
+
 def train(net: Unet, inputs, targets, n: int, steps: int, batch: int = 4, lr: float = 2e-3, seed: int = 0,
           time_budget_s: float | None = None, log=None):
     """Adam on the mean squared error of net(r_k) against e_k, cosine learning-rate decay."""

@@ -212,6 +212,10 @@ int hpccg_unet_forward(hpccg_unet *unet, int32_t nx, int32_t ny, int32_t nz, int
  * parameter (kept on the device; copied to grad_host when non-null). */
 int hpccg_unet_loss_grad(hpccg_unet *unet, int32_t nx, int32_t ny, int32_t nz, int32_t nb, const float *d_in,
                          const float *d_target, float *loss, float *grad_host);
+/* Loss of hpccg_unet_loss_grad: 0 = mean squared error (default), 1 = energy
+ * norm (1/n) d.(A d), d = target - out, with A the generate_matrix operator
+ * on the same grid -- the norm in which CG measures the error. */
+int hpccg_unet_set_loss(hpccg_unet *unet, int32_t kind);
 /* One Adam update with the gradient of the last hpccg_unet_loss_grad. */
 int hpccg_unet_adam_step(hpccg_unet *unet, float lr, float beta1, float beta2, float eps);
 /* Average ms of `reps` forward passes on one grid. */

@@ -121,14 +121,30 @@ def forward(params, r, keep=False):
     return (out, a) if keep else out
 
 
-def loss_grad(params, r, target):
-    """MSE loss and its gradient w.r.t. the flat parameter vector."""
+def apply_A(d):
+    """The generate_matrix operator on each grid of d [B,Z,Y,X]: 27 d - sum of in-grid neighbours."""
+    dp = np.pad(d, ((0, 0), (1, 1), (1, 1), (1, 1)))
+    Z, Y, X = d.shape[1:]
+    s = np.zeros_like(d)
+    for t in range(27):
+        dz, dy, dx = t // 9 - 1, (t // 3) % 3 - 1, t % 3 - 1
+        s += dp[:, 1 + dz:1 + dz + Z, 1 + dy:1 + dy + Y, 1 + dx:1 + dx + X]
+    return 28.0 * d - s
+
+
+def loss_grad(params, r, target, kind=0):
+    """Loss (0: mean squared error, 1: energy norm d.(A d)/n) and its gradient."""
     off, n = offsets()
     Ws, bs, proj = unpack(params)
     out, a = forward(params, r, keep=True)
     N = out.size
-    loss = float(((out - target) ** 2).mean())
-    dout = 2.0 * (out - target) / N
+    if kind == 1:
+        Ad = apply_A(target - out)
+        loss = float(((target - out) * Ad).sum() / N)
+        dout = -2.0 * Ad / N
+    else:
+        loss = float(((out - target) ** 2).mean())
+        dout = 2.0 * (out - target) / N
     g = np.zeros(n)
     g[off[-1]:off[-1] + 16] = np.einsum("bzyxc,bzyx->c", a["c1"], dout)
     g[off[-1] + 16] = dout.sum()
