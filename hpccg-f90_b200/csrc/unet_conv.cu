@@ -29,6 +29,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
   uint64_t *acc_empty = acc_full + 2;
   uint64_t *drain = acc_empty + 2;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  static_assert((2 * kConvStages + 5) * 8 + 4 <= kConvBarBytes, "barrier area");
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int i = threadIdx.x; i < kWBytes / 16; i += kConvThreads)
@@ -210,7 +211,8 @@ int make_act_tmap(CUtensorMap *map, const void *base, const ConvGeom &g) {
 
 template <int NIN, int EPI>
 static int launch_one(const CUtensorMap *maps, const ConvArgs &a, int num_sms, cudaStream_t s) {
-  constexpr size_t smem = NIN * 27 * kWTapBytes + kConvStages * kTapBytes + 32 * 8 + 64;
+  constexpr size_t smem = conv_smem_bytes(NIN);
+  static_assert(conv_smem_bytes(NIN) <= 227 * 1024, "conv CTA exceeds the shared-memory limit");
   static int per_sm = 0;
   if (!per_sm) {
     HPCCG_CUDA(cudaFuncSetAttribute(k_conv3_tc<NIN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

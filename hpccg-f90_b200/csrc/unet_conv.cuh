@@ -25,6 +25,11 @@ constexpr int kConvThreads = 192;
 constexpr int kConvStages = 24;
 constexpr int kTapBytes = 2 * 128 * 16;  // one k-step of A: 2 boxes x 128 voxels x 16 bytes
 constexpr int kWTapBytes = 16 * 16 * 2;  // one tap of B: 16 x 16 BF16
+// mbarriers after the stages: full[S], empty[S], acc_full[2], acc_empty[2],
+// drain[1], then the 4-byte TMEM address slot (rounded up to 16 bytes).
+constexpr int kConvBarBytes = (2 * kConvStages + 5) * 8 + 16;
+// Dynamic shared memory of a conv CTA with `nin` input groups.
+constexpr int conv_smem_bytes(int nin) { return nin * 27 * kWTapBytes + kConvStages * kTapBytes + kConvBarBytes; }
 
 enum ConvEpi : int {
   kEpiBiasRelu = 0,   // out_bf16 = relu(acc + bias)
