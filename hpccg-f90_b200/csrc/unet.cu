@@ -157,9 +157,10 @@ static int conv(hpccg_unet *u, int layer, int level, const __nv_bfloat16 *in0, c
   const int nin = bwd_group >= 0 ? 1 : d.nin;
   ConvGeom g;
   if (nin > 0 && conv_geom(Lv.nx, Lv.ny, Lv.nz, u->nb, &g)) {
+    const bool row = conv_row_ok(g);
     CUtensorMap maps[2];
-    int rc = make_act_tmap(&maps[0], in0, g);
-    if (!rc && nin > 1) rc = make_act_tmap(&maps[1], in1, g);
+    int rc = make_act_tmap(&maps[0], in0, g, row);
+    if (!rc && nin > 1) rc = make_act_tmap(&maps[1], in1, g, row);
     if (rc) return rc;
     ConvArgs a;
     a.g = g;
@@ -168,7 +169,8 @@ static int conv(hpccg_unet *u, int layer, int level, const __nv_bfloat16 *in0, c
     a.proj = proj;
     a.out = out;
     a.err = u->d_err;
-    return launch_conv3_tc(nin, epi, maps, a, u->num_sms, u->stream);
+    return row ? launch_conv3_tc_row(nin, epi, maps, a, u->num_sms, u->stream)
+               : launch_conv3_tc(nin, epi, maps, a, u->num_sms, u->stream);
   }
   if (in_f32 && (epi == kEpiBiasRelu || epi == kEpiBias)) {  // the 1-channel input layer
     k_conv3_in1<<<grid1d(u, Lv.nvox), 256, 0, u->stream>>>(in_f32, W, bias, static_cast<__nv_bfloat16 *>(out),
@@ -541,7 +543,7 @@ extern "C" int hpccg_unet_conv3_layer(int32_t nx, int32_t ny, int32_t nz, int32_
   HPCCG_CUDA(cudaMalloc(&d_err, sizeof(int)));
   HPCCG_CUDA(cudaMemset(d_err, 0, sizeof(int)));
   int rc = HPCCG_OK;
-  if (path == 0) {
+  if (path == 0 || path == 2) {
     ConvGeom g;
     if (!conv_geom(nx, ny, nz, nb, &g)) {
       cudaFree(d_err);
@@ -550,9 +552,10 @@ extern "C" int hpccg_unet_conv3_layer(int32_t nx, int32_t ny, int32_t nz, int32_
     __nv_bfloat16 *packed = nullptr;
     HPCCG_CUDA(cudaMalloc(&packed, sizeof(__nv_bfloat16) * nin * 27 * 256));
     k_pack_fwd<<<32, 256>>>(d_w, 16 * nin, nin, packed);
+    const bool row = path == 0 && conv_row_ok(g);
     CUtensorMap maps[2];
-    rc = make_act_tmap(&maps[0], d_in0, g);
-    if (!rc && nin > 1) rc = make_act_tmap(&maps[1], d_in1, g);
+    rc = make_act_tmap(&maps[0], d_in0, g, row);
+    if (!rc && nin > 1) rc = make_act_tmap(&maps[1], d_in1, g, row);
     if (!rc) {
       ConvArgs a;
       a.g = g;
@@ -561,7 +564,7 @@ extern "C" int hpccg_unet_conv3_layer(int32_t nx, int32_t ny, int32_t nz, int32_
       a.proj = d_proj;
       a.out = d_out;
       a.err = d_err;
-      rc = launch_conv3_tc(nin, epi, maps, a, sms, 0);
+      rc = row ? launch_conv3_tc_row(nin, epi, maps, a, sms, 0) : launch_conv3_tc(nin, epi, maps, a, sms, 0);
     }
     if (cudaDeviceSynchronize() != cudaSuccess) rc = set_cuda_error(cudaGetLastError(), "conv3 tc", __FILE__, __LINE__);
     cudaFree(packed);

@@ -29,7 +29,20 @@ constexpr int kWTapBytes = 16 * 16 * 2;  // one tap of B: 16 x 16 BF16
 // drain[1], then the 4-byte TMEM address slot (rounded up to 16 bytes).
 constexpr int kConvBarBytes = (2 * kConvStages + 5) * 8 + 16;
 // Dynamic shared memory of a conv CTA with `nin` input groups.
-constexpr int conv_smem_bytes(int nin) { return nin * 27 * kWTapBytes + kConvStages * kTapBytes + kConvBarBytes; }
+__host__ __device__ constexpr int conv_smem_bytes(int nin) { return nin * 27 * kWTapBytes + kConvStages * kTapBytes + kConvBarBytes; }
+
+// Row-tile variant for bricks that are one 128-voxel x-row (nx a multiple of
+// 128): one TMA box per 8-channel half brings the 3x3 neighbouring rows of
+// 130 voxels (the brick plus its x halo) and all 27 taps read that halo tile
+// through shifted descriptors: 2 TMA loads per tile and input instead of 54.
+constexpr int kRowVox = 130;
+constexpr int kRowPlaneBytes = ((9 * kRowVox * 16 + 127) / 128) * 128;  // one 8-channel plane, 128-B aligned
+constexpr int kRowStages = 2;
+__host__ __device__ constexpr int row_stage_bytes(int nin) { return nin * 2 * kRowPlaneBytes; }
+constexpr int kRowBarBytes = (2 * kRowStages + 5) * 8 + 16;
+__host__ __device__ constexpr int conv_row_smem_bytes(int nin) {
+  return nin * 27 * kWTapBytes + kRowStages * row_stage_bytes(nin) + kRowBarBytes;
+}
 
 enum ConvEpi : int {
   kEpiBiasRelu = 0,   // out_bf16 = relu(acc + bias)
@@ -76,7 +89,10 @@ inline bool conv_geom(int nx, int ny, int nz, int nb, ConvGeom *g) {
   return true;
 }
 
-int make_act_tmap(CUtensorMap *map, const void *base, const ConvGeom &g);
+int make_act_tmap(CUtensorMap *map, const void *base, const ConvGeom &g, bool row_tile = false);
 int launch_conv3_tc(int nin, int epi, const CUtensorMap *maps, const ConvArgs &a, int num_sms, cudaStream_t s);
+int launch_conv3_tc_row(int nin, int epi, const CUtensorMap *maps, const ConvArgs &a, int num_sms, cudaStream_t s);
+// The row-tile kernel applies when each brick is one full 128-voxel x-row.
+inline bool conv_row_ok(const ConvGeom &g) { return g.bx == 128 && g.by == 1 && g.bz == 1; }
 
 }  // namespace hpccg

@@ -225,7 +225,8 @@ int hpccg_unet_time_forward(hpccg_unet *unet, int32_t nx, int32_t ny, int32_t nz
  * (nin = 1 or 2 groups of 16 channels), weights FP32 [27][16*nin][16],
  * epi 0 = bias+ReLU (BF16 out), 1 = bias (BF16), 2 = bias+ReLU then the 16->1
  * projection d_proj (FP32 out), 3 = raw FP32 16-channel out; path 0 =
- * tcgen05, 1 = CUDA cores. */
+ * tcgen05 (row tiles when nx is a multiple of 128), 1 = CUDA cores,
+ * 2 = tcgen05 with per-tap loads. */
 int hpccg_unet_conv3_layer(int32_t nx, int32_t ny, int32_t nz, int32_t nb, int32_t nin, const void *d_in0,
                            const void *d_in1, const float *d_w, const float *d_bias, const float *d_proj,
                            int32_t epi, int32_t path, void *d_out);

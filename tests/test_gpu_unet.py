@@ -27,7 +27,7 @@ def _bf16_tensor(torch, a):
     return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda().to(torch.bfloat16).contiguous()
 
 
-SHAPES = [(16, 16, 16, 1), (32, 8, 8, 2), (128, 4, 2, 1), (8, 8, 8, 3), (64, 16, 8, 1)]
+SHAPES = [(16, 16, 16, 1), (32, 8, 8, 2), (128, 4, 2, 1), (8, 8, 8, 3), (64, 16, 8, 1), (256, 3, 5, 2)]
 
 
 @pytest.mark.parametrize("nx,ny,nz,nb", SHAPES)
@@ -43,7 +43,7 @@ def test_conv_layer_tc_and_cc(env, nx, ny, nz, nb, nin, epi):
     x = np.concatenate(xs, -1).astype(np.float64)
     dW, db, dp = (torch.from_numpy(v).cuda() for v in (W, b, proj))
     din = [_bf16_tensor(torch, v) for v in xs] + [None]
-    for path, Wref in ((0, uo.bf16_round(W)), (1, W)):
+    for path, Wref in ((0, uo.bf16_round(W)), (2, uo.bf16_round(W)), (1, W)):
         pre = uo.conv3(x, Wref.astype(np.float64))
         if epi == 3:
             want = pre
