@@ -267,6 +267,24 @@ def run_ours(args):
     methods = [("fp64_cg", "plain FP64 CG (reference operation order), one CUDA graph", fp64_cg),
                ("fp32_ir", "FP64 iterative refinement, FP32 inner CG", mixed(hp.PREC_FP32)),
                ("bf16_ir", "FP64 iterative refinement, inner CG on BF16 values / FP32 vectors", mixed(hp.PREC_BF16))]
+    learned_info = None
+    if not args.no_learned:
+        from hpccg_b200 import learned
+
+        t0 = time.time()
+        net, hist = learned.train_preconditioner(64, seed=1, rhs=64, rounds=3, steps=args.train_steps)
+        learned_info = {"train_s": time.time() - t0, "train_grid": "64^3", "train_rhs": 64, "rounds": 3,
+                        "steps_per_round": args.train_steps, "loss_first": float(np.mean(hist[:5])),
+                        "loss_last": float(np.mean(hist[-20:])), "params": net.nparams}
+
+        def learned_fcg():
+            info, st = learned.solve_fcg(M, net, n, d_b, d_x, REL_TOL, max_iter)
+            assert st == hp.HPCCG_OK, st
+            return ({"iterations": info.iters, "nn_applies": info.nn_applies, "fallback": info.fallback},
+                    4 + 25 * info.iters)
+
+        methods.append(("learned_fcg", "flexible PCG (FP64) with the trained U-Net preconditioner (BF16 tensor cores)",
+                        learned_fcg))
     results = {}
     clk_summary = None
     for name, desc, fn in methods:
@@ -291,6 +309,21 @@ def run_ours(args):
         err = float((d_x - xstar).abs().max().item())
         results[name] = {"ms": ms, "method": desc, "true_relres": relres, "max_abs_err_vs_xstar": err,
                          "gpu_launches": launches, "clocks": clk.summary(), **info}
+    if learned_info is not None:
+        # the learned method on its own workload: Gaussian-random-field right-hand side
+        grf = learned.gaussian_random_field(M, n, 4242, torch)
+        d_x.zero_()
+        it_plain, _, _, _ = M.cg_device(grf, d_x, max_iter, REL_TOL * float(torch.linalg.vector_norm(grf)),
+                                        history=False)
+        plain_grf_ms = M.last_solve_ms()
+        d_x.zero_()
+        info, _ = learned.solve_fcg(M, net, n, grf, d_x, REL_TOL, max_iter)
+        learned_info.update({"grf_rhs": {"plain_fp64_cg_iters": it_plain, "plain_fp64_cg_ms": plain_grf_ms,
+                                         "learned_fcg_iters": info.iters, "learned_fcg_ms": M.last_solve_ms(),
+                                         "relres": info.relres, "fallback": info.fallback}})
+        d_in = torch.randn(N, dtype=torch.float32, device=dev)
+        d_out = torch.empty_like(d_in)
+        learned_info["unet_forward_ms"] = net.time_forward(d_in, d_out, n, n, n, 3)
     ok = {k: v for k, v in results.items() if v["true_relres"] <= REL_TOL}
     head = min(ok, key=lambda k: ok[k]["ms"])
     plain_ms = results["fp64_cg"]["ms"]
@@ -353,7 +386,7 @@ def run_ours(args):
         "config": {"workload": f"{n}^3 27-point HPCCG matrix ({N} rows, {nnz} nonzeros), x* U[-1,1) seed 1234, "
                                f"b = A x*, x0 = 0, solved to FP64 ||b - A x|| <= 1e-8 ||b||",
                    "method": head, "speedup_vs_plain_gpu_cg": plain_ms / hr["ms"],
-                   "methods": results,
+                   "methods": results, "learned": learned_info,
                    "l2": "inputs (5.4 GB matrix) exceed the 126 MB L2; no flush",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
                    "spmv_kernel": list(M.get_spmv())},
@@ -379,6 +412,8 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--ref-sample-iters", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip training/timing the learned preconditioner")
+    ap.add_argument("--train-steps", type=int, default=400)
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
