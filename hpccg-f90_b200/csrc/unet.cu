@@ -157,20 +157,16 @@ static int conv(hpccg_unet *u, int layer, int level, const __nv_bfloat16 *in0, c
   const int nin = bwd_group >= 0 ? 1 : d.nin;
   ConvGeom g;
   if (nin > 0 && conv_geom(Lv.nx, Lv.ny, Lv.nz, u->nb, &g)) {
-    const bool row = conv_row_ok(g);
-    CUtensorMap maps[2];
-    int rc = make_act_tmap(&maps[0], in0, g, row);
-    if (!rc && nin > 1) rc = make_act_tmap(&maps[1], in1, g, row);
-    if (rc) return rc;
     ConvArgs a;
     a.g = g;
+    a.in0 = in0;
+    a.in1 = in1;
     a.wpack = bwd_group >= 0 ? u->packed_bwd[layer][bwd_group] : u->packed_fwd[layer];
     a.bias = bwd_group >= 0 ? nullptr : bias;
     a.proj = proj;
     a.out = out;
     a.err = u->d_err;
-    return row ? launch_conv3_tc_row(nin, epi, maps, a, u->num_sms, u->stream)
-               : launch_conv3_tc(nin, epi, maps, a, u->num_sms, u->stream);
+    return launch_conv3_tc(nin, epi, a, u->num_sms, u->stream);
   }
   if (in_f32 && (epi == kEpiBiasRelu || epi == kEpiBias)) {  // the 1-channel input layer
     k_conv3_in1<<<grid1d(u, Lv.nvox), 256, 0, u->stream>>>(in_f32, W, bias, static_cast<__nv_bfloat16 *>(out),
@@ -227,7 +223,8 @@ static int forward(hpccg_unet *u, const float *in, float *out, bool train) {
   k_upsample<<<grid1d(u, L[0].nvox * 2), 256, 0, u->stream>>>(u->c2b, u->u1, L[0].nx, L[0].ny, L[0].nz, u->nb);
   if (train) {
     UNET_TRY(conv(u, 12, 0, u->e1b, u->u1, nullptr, kEpiBiasRelu, u->c1));
-    k_proj_fwd<<<grid1d(u, L[0].nvox), 256, 0, u->stream>>>(u->c1, u->params + u->off[kNumLayers], out, L[0].nvox);
+    k_proj_fwd<<<grid1d(u, L[0].nvox), 256, 0, u->stream>>>(u->c1, u->params + u->off[kNumLayers], out, L[0].nvox,
+                                                           L[0].nx);
   } else {
     UNET_TRY(conv(u, 12, 0, u->e1b, u->u1, nullptr, kEpiProject, out));
   }
@@ -271,7 +268,8 @@ static int backward(hpccg_unet *u, const float *in) {
   cudaStream_t s = u->stream;
   // projection and dec1a (level 0)
   const int pb = (int)std::min<int64_t>(u->partial_blocks, (L[0].nvox + 255) / 256);
-  k_proj_bwd<<<pb, 256, 0, s>>>(u->c1, u->params + u->off[kNumLayers], u->dout, u->pre[0], u->partial, L[0].nvox);
+  k_proj_bwd<<<pb, 256, 0, s>>>(u->c1, u->params + u->off[kNumLayers], u->dout, u->pre[0], u->partial, L[0].nvox,
+                                L[0].nx);
   k_reduce_partials<<<1, 32, 0, s>>>(u->partial, pb, 17, u->grads + u->off[kNumLayers], 1);
   UNET_TRY(weight_grad(u, 12, 0, u->e1b, u->u1, nullptr, u->pre[0]));
   UNET_TRY(conv(u, 12, 0, u->pre[0], nullptr, nullptr, kEpiRawF32, u->gs[0], 0));  // d e1b (skip)
@@ -552,20 +550,16 @@ extern "C" int hpccg_unet_conv3_layer(int32_t nx, int32_t ny, int32_t nz, int32_
     __nv_bfloat16 *packed = nullptr;
     HPCCG_CUDA(cudaMalloc(&packed, sizeof(__nv_bfloat16) * nin * 27 * 256));
     k_pack_fwd<<<32, 256>>>(d_w, 16 * nin, nin, packed);
-    const bool row = path == 0 && conv_row_ok(g);
-    CUtensorMap maps[2];
-    rc = make_act_tmap(&maps[0], d_in0, g, row);
-    if (!rc && nin > 1) rc = make_act_tmap(&maps[1], d_in1, g, row);
-    if (!rc) {
-      ConvArgs a;
-      a.g = g;
-      a.wpack = packed;
-      a.bias = d_bias;
-      a.proj = d_proj;
-      a.out = d_out;
-      a.err = d_err;
-      rc = row ? launch_conv3_tc_row(nin, epi, maps, a, sms, 0) : launch_conv3_tc(nin, epi, maps, a, sms, 0);
-    }
+    ConvArgs a;
+    a.g = g;
+    a.in0 = static_cast<const __nv_bfloat16 *>(d_in0);
+    a.in1 = static_cast<const __nv_bfloat16 *>(d_in1);
+    a.wpack = packed;
+    a.bias = d_bias;
+    a.proj = d_proj;
+    a.out = d_out;
+    a.err = d_err;
+    rc = launch_conv3_tc(nin, epi, a, sms, 0, path == 2);
     if (cudaDeviceSynchronize() != cudaSuccess) rc = set_cuda_error(cudaGetLastError(), "conv3 tc", __FILE__, __LINE__);
     cudaFree(packed);
   } else {

@@ -1,68 +1,79 @@
 // unet_conv.cuh -- 3x3x3 convolutions with 16 output channels on tcgen05.
 //
-// Layout: activations are channels-last BF16, [batch][z][y][x][16].  A conv
-// is an implicit GEMM per tile of 128 voxels (a bx*by*bz brick, one TMEM lane
-// per voxel): for each of the 27 taps and each 16-channel input, the shifted
-// brick is fetched by TMA (zero fill outside the volume = zero padding) and
-// one tcgen05.mma (M=128, N=16, K=16) accumulates it into a 16-column FP32
-// TMEM accumulator.
+// Activation layout ("row-planar"): a 16-channel tensor of nb grids of
+// nx*ny*nz voxels is stored as [b][z][y][h][x][8] -- for every grid row
+// (b,z,y), first the 8-channel half h=0 of all nx voxels, then h=1.  A voxel
+// half is one 16-byte unit, and a run of consecutive voxels of one row and
+// half is one contiguous span, which is exactly the layout the tensor cores
+// read (no-swizzle K-major core matrices: 8 rows x 16 bytes; the two halves
+// are the two K chunks).  So every operand tile arrives by 1D bulk copies
+// (cp.async.bulk) of whole row spans, with zero fill at the grid faces.
 //
-// Roles per CTA (192 threads): warp 0 lane 0 issues TMA loads into an S-stage
-// ring, warp 1 allocates TMEM and lane 0 issues the MMAs, warps 2-5 (one per
-// TMEM lane quarter) run the epilogue.  Two accumulators let the epilogue of
-// one tile overlap the MMAs of the next.
-//
-// Shared-memory operands use the no-swizzle K-major core-matrix layout: A is
-// [k-chunk 2][voxel 128][8 channels] (two TMA boxes of 8 channels each),
-// B is [k-chunk 2][out-channel 16][8 in-channels] per tap.
+// A conv is an implicit GEMM per tile of 128 voxels (one TMEM lane each):
+// for each of the 27 taps and each 16-channel input group, one tcgen05.mma
+// (M=128, N=16, K=16) accumulates into a 16-column FP32 TMEM accumulator.
+//  * row tiles (nx a multiple of 128): a tile is one 128-voxel x-row; the
+//    3x3 neighbouring rows with a 1-voxel x halo (9 x 130 units per half) are
+//    fetched once and the 27 taps read them through shifted descriptors;
+//  * brick tiles (smaller nx): a tile is a bx*by*bz brick and each tap's
+//    shifted brick is fetched separately (by*bz row spans per half).
+// Roles per CTA (192 threads): warp 0 fetches (its lanes issue the row spans
+// in parallel), warp 1 allocates TMEM and lane 0 issues the MMAs, warps 2-5
+// (one per TMEM lane quarter) run the epilogue.
 #pragma once
 #include "hpccg_internal.cuh"
 #include "unet_tc.cuh"
 
 namespace hpccg {
 
-constexpr int kConvThreads = 192;
-constexpr int kConvStages = 24;
-constexpr int kTapBytes = 2 * 128 * 16;  // one k-step of A: 2 boxes x 128 voxels x 16 bytes
-constexpr int kWTapBytes = 16 * 16 * 2;  // one tap of B: 16 x 16 BF16
-// mbarriers after the stages: full[S], empty[S], acc_full[2], acc_empty[2],
-// drain[1], then the 4-byte TMEM address slot (rounded up to 16 bytes).
-constexpr int kConvBarBytes = (2 * kConvStages + 5) * 8 + 16;
-// Dynamic shared memory of a conv CTA with `nin` input groups.
-__host__ __device__ constexpr int conv_smem_bytes(int nin) { return nin * 27 * kWTapBytes + kConvStages * kTapBytes + kConvBarBytes; }
+// Offsets in the row-planar layout; row = (b*nz + z)*ny + y.
+__host__ __device__ __forceinline__ int64_t act_unit(int64_t row, int h, int x, int nx) {
+  return (row * 2 + h) * (int64_t)nx + x;
+}
+__host__ __device__ __forceinline__ int64_t act_elem(int64_t row, int x, int c, int nx) {
+  return act_unit(row, c >> 3, x, nx) * 8 + (c & 7);
+}
 
-// Row-tile variant for bricks that are one 128-voxel x-row (nx a multiple of
-// 128): one TMA box per 8-channel half brings the 3x3 neighbouring rows of
-// 130 voxels (the brick plus its x halo) and all 27 taps read that halo tile
-// through shifted descriptors: 2 TMA loads per tile and input instead of 54.
+constexpr int kConvThreads = 192;
+constexpr int kWTapBytes = 16 * 16 * 2;  // one tap of B: 16 x 16 BF16
+
+// Brick tiles: one stage per k-step (tap, input): 2 halves x 128 units.
+constexpr int kBrickStages = 24;
+constexpr int kBrickStageBytes = 2 * 128 * 16;
+// Row tiles: one stage per tile: inputs x 2 halves x (9 rows x 130 units), 128-B aligned planes.
 constexpr int kRowVox = 130;
-constexpr int kRowPlaneBytes = ((9 * kRowVox * 16 + 127) / 128) * 128;  // one 8-channel plane, 128-B aligned
+constexpr int kRowPlaneBytes = ((9 * kRowVox * 16 + 127) / 128) * 128;
 constexpr int kRowStages = 2;
 __host__ __device__ constexpr int row_stage_bytes(int nin) { return nin * 2 * kRowPlaneBytes; }
-constexpr int kRowBarBytes = (2 * kRowStages + 5) * 8 + 16;
-__host__ __device__ constexpr int conv_row_smem_bytes(int nin) {
-  return nin * 27 * kWTapBytes + kRowStages * row_stage_bytes(nin) + kRowBarBytes;
+// mbarriers: full[S], empty[S], acc_full[2], acc_empty[2], drain, + TMEM slot.
+__host__ __device__ constexpr int bar_bytes(int stages) { return (2 * stages + 5) * 8 + 16; }
+__host__ __device__ constexpr int brick_smem_bytes(int nin) {
+  return nin * 27 * kWTapBytes + kBrickStages * kBrickStageBytes + bar_bytes(kBrickStages);
+}
+__host__ __device__ constexpr int row_smem_bytes(int nin) {
+  return nin * 27 * kWTapBytes + kRowStages * row_stage_bytes(nin) + bar_bytes(kRowStages);
 }
 
 enum ConvEpi : int {
   kEpiBiasRelu = 0,   // out_bf16 = relu(acc + bias)
   kEpiBias = 1,       // out_bf16 = acc + bias
-  kEpiProject = 2,    // out_f32 = proj . relu(acc + bias) + proj_bias
-  kEpiRawF32 = 3,     // out_f32 = acc (16 channels)
+  kEpiProject = 2,    // out_f32[voxel] = proj . relu(acc + bias) + proj_bias
+  kEpiRawF32 = 3,     // out_f32 = acc (16 channels, row-planar)
 };
 
 struct ConvGeom {
   int nx, ny, nz, nb;  // volume and batch
-  int bx, by, bz;      // brick of 128 voxels
-  int tx, ty, tz;      // bricks per dimension
+  int bx, by, bz;      // tile brick (bx*by*bz = 128)
+  int tx, ty, tz;      // tiles per dimension
   int ntiles;
 };
 
 struct ConvArgs {
   ConvGeom g;
-  const __nv_bfloat16 *wpack;  // [nin][27][2][16][8] BF16
-  const float *bias;           // [16] (nullable for kEpiRawF32)
-  const float *proj;           // [17] for kEpiProject: 16 weights + bias
+  const __nv_bfloat16 *in0, *in1;  // row-planar inputs
+  const __nv_bfloat16 *wpack;      // [nin][27][2][16][8] BF16
+  const float *bias;               // [16] (null for kEpiRawF32)
+  const float *proj;               // [17] for kEpiProject
   void *out;
   int *err;
 };
@@ -74,7 +85,7 @@ inline bool conv_geom(int nx, int ny, int nz, int nb, ConvGeom *g) {
   int by = 128 / bx;
   if (by > ny) by = ny;
   int bz = 128 / (bx * by);
-  if (bx * by * bz != 128 || nx % bx || ny % by || nz % bz) return false;
+  if (bx < 8 || bx * by * bz != 128 || nx % bx || ny % by || nz % bz) return false;
   g->nx = nx;
   g->ny = ny;
   g->nz = nz;
@@ -88,11 +99,9 @@ inline bool conv_geom(int nx, int ny, int nz, int nb, ConvGeom *g) {
   g->ntiles = g->tx * g->ty * g->tz * nb;
   return true;
 }
-
-int make_act_tmap(CUtensorMap *map, const void *base, const ConvGeom &g, bool row_tile = false);
-int launch_conv3_tc(int nin, int epi, const CUtensorMap *maps, const ConvArgs &a, int num_sms, cudaStream_t s);
-int launch_conv3_tc_row(int nin, int epi, const CUtensorMap *maps, const ConvArgs &a, int num_sms, cudaStream_t s);
-// The row-tile kernel applies when each brick is one full 128-voxel x-row.
 inline bool conv_row_ok(const ConvGeom &g) { return g.bx == 128 && g.by == 1 && g.bz == 1; }
+
+// Launches the tensor-core conv (row tiles when possible unless force_brick).
+int launch_conv3_tc(int nin, int epi, const ConvArgs &a, int num_sms, cudaStream_t s, bool force_brick = false);
 
 }  // namespace hpccg

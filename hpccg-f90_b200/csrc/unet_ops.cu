@@ -1,7 +1,8 @@
 // unet_ops.cu -- CUDA-core kernels of the U-Net: the 1-channel input conv and
 // small-volume convs, weight packing for the tcgen05 convs, pooling,
 // upsampling, ReLU masks, weight/bias gradients, the output projection, the
-// loss and the Adam update.  All are memory-bound or tiny.
+// loss and the Adam update.  All are memory-bound or tiny.  16-channel
+// tensors use the row-planar layout of unet_conv.cuh (act_unit / act_elem).
 #include "unet_ops.cuh"
 
 namespace hpccg {
@@ -35,8 +36,8 @@ __global__ void k_flip_fp32(const float *W, int cin, int g, float *Wf) {
 
 // ---- direct conv on CUDA cores --------------------------------------------------------
 // out[v][co] = sum_tap sum_ci in[v + off(tap)][ci] * W[tap][ci][co] (+ bias, ReLU).
-// Inputs: in0/in1 BF16 channels-last 16-channel tensors (in1 nullable), or
-// in_f32 one-channel FP32 (cin = 1).  One thread per output voxel.
+// Inputs: in0/in1 row-planar BF16 16-channel tensors (in1 nullable), or in_f32
+// one-channel FP32 (cin = 1).  One thread per output voxel.
 __global__ void k_conv3_cc(CcConvArgs a) {
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int64_t nvox = (int64_t)nx * ny * nz * a.nb;
@@ -49,40 +50,41 @@ __global__ void k_conv3_cc(CcConvArgs a) {
     for (int tap = 0; tap < 27; ++tap) {
       const int xx = x + tap % 3 - 1, yy = y + (tap / 3) % 3 - 1, zz = z + tap / 9 - 1;
       if (xx < 0 || xx >= nx || yy < 0 || yy >= ny || zz < 0 || zz >= nz) continue;
-      const int64_t u = ((b * nz + zz) * ny + yy) * nx + xx;
+      const int64_t row = (b * nz + zz) * ny + yy;
       if (a.in_f32) {
-        const float s = a.in_f32[u];
+        const float s = a.in_f32[row * nx + xx];
         const float *w = a.W + (size_t)tap * 16;
 #pragma unroll
         for (int c = 0; c < 16; ++c) acc[c] = fmaf(s, w[c], acc[c]);
         continue;
       }
       for (int g = 0; g < a.nin; ++g) {
-        const __nv_bfloat16 *src = (g ? a.in1 : a.in0) + u * 16;
+        const __nv_bfloat16 *src = g ? a.in1 : a.in0;
         for (int ci = 0; ci < 16; ++ci) {
-          const float s = __bfloat162float(src[ci]);
+          const float s = __bfloat162float(src[act_elem(row, xx, ci, nx)]);
           const float *w = a.W + ((size_t)tap * a.cin + g * 16 + ci) * 16;
 #pragma unroll
           for (int c = 0; c < 16; ++c) acc[c] = fmaf(s, w[c], acc[c]);
         }
       }
     }
+    const int64_t orow = (b * nz + z) * ny + y;
     if (a.epi == kEpiRawF32) {
-      float *o = static_cast<float *>(a.out) + v * 16;
+      float *o = static_cast<float *>(a.out);
 #pragma unroll
-      for (int c = 0; c < 16; ++c) o[c] = acc[c];
+      for (int c = 0; c < 16; ++c) o[act_elem(orow, x, c, nx)] = acc[c];
     } else if (a.epi == kEpiProject) {
       float r = a.proj[16];
 #pragma unroll
       for (int c = 0; c < 16; ++c) r = fmaf(a.proj[c], fmaxf(acc[c] + a.bias[c], 0.f), r);
       static_cast<float *>(a.out)[v] = r;
     } else {
-      __nv_bfloat16 *o = static_cast<__nv_bfloat16 *>(a.out) + v * 16;
+      __nv_bfloat16 *o = static_cast<__nv_bfloat16 *>(a.out);
 #pragma unroll
       for (int c = 0; c < 16; ++c) {
         float t = acc[c] + (a.bias ? a.bias[c] : 0.f);
         if (a.epi == kEpiBiasRelu) t = fmaxf(t, 0.f);
-        o[c] = __float2bfloat16(t);
+        o[act_elem(orow, x, c, nx)] = __float2bfloat16(t);
       }
     }
   }
@@ -121,29 +123,43 @@ __global__ void __launch_bounds__(256) k_conv3_in1(const float *in, const float 
       const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
       w[c] = *reinterpret_cast<const uint32_t *>(&h);
     }
-    uint4 *o = reinterpret_cast<uint4 *>(out + v * 16);
-    o[0] = make_uint4(w[0], w[1], w[2], w[3]);
-    o[1] = make_uint4(w[4], w[5], w[6], w[7]);
+    const int64_t row = v / nx;
+    *reinterpret_cast<uint4 *>(out + act_unit(row, 0, x, nx) * 8) = make_uint4(w[0], w[1], w[2], w[3]);
+    *reinterpret_cast<uint4 *>(out + act_unit(row, 1, x, nx) * 8) = make_uint4(w[4], w[5], w[6], w[7]);
   }
 }
 
-// ---- resampling --------------------------------------------------------------------------
-// 2x2x2 average pooling of a 16-channel BF16 tensor (fine dims nx,ny,nz even);
-// one thread per coarse voxel and 8-channel half, 16-byte loads.
+// ---- resampling (row-planar 16-channel tensors; fine dims nx, ny, nz even) -------------------
+// Decomposes a unit index of a row-planar tensor into (row, half, x).
+__device__ __forceinline__ void unit_coords(int64_t u, int nx, int64_t *row, int *h, int *x) {
+  *x = (int)(u % nx);
+  const int64_t t = u / nx;
+  *h = (int)(t & 1);
+  *row = t >> 1;
+}
+// Row index of (b, z, y) and its inverse.
+__device__ __forceinline__ void row_coords(int64_t row, int ny, int nz, int64_t *b, int *z, int *y) {
+  *y = (int)(row % ny);
+  const int64_t t = row / ny;
+  *z = (int)(t % nz);
+  *b = t / nz;
+}
+
+// 2x2x2 average pooling, one thread per coarse 16-byte unit (8 channels).
 __global__ void k_pool(const __nv_bfloat16 *in, __nv_bfloat16 *out, int nx, int ny, int nz, int nb) {
   const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
   const int64_t n = (int64_t)cx * cy * cz * nb * 2;
   const uint4 *src = reinterpret_cast<const uint4 *>(in);
   uint4 *dst = reinterpret_cast<uint4 *>(out);
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int h = (int)(e & 1);
-    const int64_t v = e >> 1;
-    const int x = (int)(v % cx), y = (int)((v / cx) % cy), z = (int)((v / ((int64_t)cx * cy)) % cz);
-    const int64_t b = v / ((int64_t)cx * cy * cz);
+    int64_t row, b;
+    int h, xc, zc, yc;
+    unit_coords(e, cx, &row, &h, &xc);
+    row_coords(row, cy, cz, &b, &zc, &yc);
     float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (int k = 0; k < 8; ++k) {
-      const int64_t u = ((b * nz + 2 * z + (k >> 2)) * ny + 2 * y + ((k >> 1) & 1)) * nx + 2 * x + (k & 1);
-      const uint4 q = src[u * 2 + h];
+      const int64_t rf = (b * nz + 2 * zc + (k >> 2)) * ny + 2 * yc + ((k >> 1) & 1);
+      const uint4 q = src[act_unit(rf, h, 2 * xc + (k & 1), nx)];
       const __nv_bfloat162 *p2 = reinterpret_cast<const __nv_bfloat162 *>(&q);
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
@@ -162,29 +178,27 @@ __global__ void k_pool(const __nv_bfloat16 *in, __nv_bfloat16 *out, int nx, int 
 // Nearest-neighbour 2x upsampling: fine (nx,ny,nz) from coarse (nx/2,...).
 __global__ void k_upsample(const __nv_bfloat16 *in, __nv_bfloat16 *out, int nx, int ny, int nz, int nb) {
   const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
-  const int64_t n = (int64_t)nx * ny * nz * nb * 2;  // 16-byte (8-channel) units
+  const int64_t n = (int64_t)nx * ny * nz * nb * 2;
   const uint4 *src = reinterpret_cast<const uint4 *>(in);
   uint4 *dst = reinterpret_cast<uint4 *>(out);
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int h = (int)(e & 1);
-    const int64_t v = e >> 1;
-    const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)((v / ((int64_t)nx * ny)) % nz);
-    const int64_t b = v / ((int64_t)nx * ny * nz);
-    const int64_t u = ((b * cz + z / 2) * cy + y / 2) * cx + x / 2;
-    dst[e] = src[u * 2 + h];
+    int64_t row, b;
+    int h, x, z, y;
+    unit_coords(e, nx, &row, &h, &x);
+    row_coords(row, ny, nz, &b, &z, &y);
+    dst[e] = src[act_unit((b * cz + z / 2) * cy + y / 2, h, x / 2, cx)];
   }
 }
-// Backward of pooling: d_fine += d_coarse / 8 (FP32 16-channel tensors).
+// Backward of pooling: d_fine += d_coarse / 8 (FP32 row-planar tensors).
 __global__ void k_pool_bwd(const float *dc, float *df, int nx, int ny, int nz, int nb) {
   const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
   const int64_t n = (int64_t)nx * ny * nz * nb * 16;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(e & 15);
-    const int64_t v = e >> 4;
-    const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)((v / ((int64_t)nx * ny)) % nz);
-    const int64_t b = v / ((int64_t)nx * ny * nz);
-    const int64_t u = ((b * cz + z / 2) * cy + y / 2) * cx + x / 2;
-    df[e] += 0.125f * dc[u * 16 + c];
+    int64_t row, b;
+    int h, x, z, y;
+    unit_coords(e >> 3, nx, &row, &h, &x);
+    row_coords(row, ny, nz, &b, &z, &y);
+    df[e] += 0.125f * dc[act_unit((b * cz + z / 2) * cy + y / 2, h, x / 2, cx) * 8 + (e & 7)];
   }
 }
 // Backward of nearest upsampling: d_coarse = sum of the 8 fine children.
@@ -192,14 +206,14 @@ __global__ void k_up_bwd(const float *df, float *dc, int nx, int ny, int nz, int
   const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
   const int64_t n = (int64_t)cx * cy * cz * nb * 16;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int c = (int)(e & 15);
-    const int64_t v = e >> 4;
-    const int x = (int)(v % cx), y = (int)((v / cx) % cy), z = (int)((v / ((int64_t)cx * cy)) % cz);
-    const int64_t b = v / ((int64_t)cx * cy * cz);
+    int64_t row, b;
+    int h, xc, zc, yc;
+    unit_coords(e >> 3, cx, &row, &h, &xc);
+    row_coords(row, cy, cz, &b, &zc, &yc);
     float s = 0.f;
     for (int k = 0; k < 8; ++k) {
-      const int64_t u = ((b * nz + 2 * z + (k >> 2)) * ny + 2 * y + ((k >> 1) & 1)) * nx + 2 * x + (k & 1);
-      s += df[u * 16 + c];
+      const int64_t rf = (b * nz + 2 * zc + (k >> 2)) * ny + 2 * yc + ((k >> 1) & 1);
+      s += df[act_unit(rf, h, 2 * xc + (k & 1), nx) * 8 + (e & 7)];
     }
     dc[e] = s;
   }
@@ -236,7 +250,7 @@ __global__ void __launch_bounds__(256) k_dW(DwArgs a) {
       __syncthreads();
       for (int e = threadIdx.x; e < 64 * 16; e += blockDim.x) {
         const int64_t v = v0 + e / 16;
-        sdy[e / 16][e % 16] = v < nvox ? __bfloat162float(a.dy[v * 16 + e % 16]) : 0.f;
+        sdy[e / 16][e % 16] = v < nvox ? __bfloat162float(a.dy[act_elem(v / nx, (int)(v % nx), e % 16, nx)]) : 0.f;
       }
       __syncthreads();
       if (task >= ntask) continue;
@@ -247,9 +261,9 @@ __global__ void __launch_bounds__(256) k_dW(DwArgs a) {
           const int x = (int)(v % nx) + ox, y = (int)((v / nx) % ny) + oy, z = (int)((v / ((int64_t)nx * ny)) % nz) + oz;
           if (x < 0 || x >= nx || y < 0 || y >= ny || z < 0 || z >= nz) continue;
           const int64_t b = v / ((int64_t)nx * ny * nz);
-          const int64_t u = ((b * nz + z) * ny + y) * nx + x;
-          if (a.x_f32) s = a.x_f32[u];
-          else s = __bfloat162float(ci < 16 ? a.x0[u * 16 + ci] : a.x1[u * 16 + ci - 16]);
+          const int64_t row = (b * nz + z) * ny + y;
+          if (a.x_f32) s = a.x_f32[row * nx + x];
+          else s = __bfloat162float(ci < 16 ? a.x0[act_elem(row, x, ci, nx)] : a.x1[act_elem(row, x, ci - 16, nx)]);
         }
 #pragma unroll
         for (int c = 0; c < 16; ++c) acc[c] = fmaf(s, sdy[j][c], acc[c]);
@@ -272,29 +286,32 @@ __global__ void k_reduce_partials(const float *partial, int nblocks, int n, floa
 }
 
 // Output projection (training path): out[v] = proj . act[v] + proj_b.
-__global__ void k_proj_fwd(const __nv_bfloat16 *act, const float *proj, float *out, int64_t nvox) {
+__global__ void k_proj_fwd(const __nv_bfloat16 *act, const float *proj, float *out, int64_t nvox, int nx) {
   for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvox; v += (int64_t)gridDim.x * blockDim.x) {
     float r = proj[16];
 #pragma unroll
-    for (int c = 0; c < 16; ++c) r = fmaf(proj[c], __bfloat162float(act[v * 16 + c]), r);
+    for (int c = 0; c < 16; ++c) r = fmaf(proj[c], __bfloat162float(act[act_elem(v / nx, (int)(v % nx), c, nx)]), r);
     out[v] = r;
   }
 }
 // d act = proj * dOut (masked by act > 0, to BF16); per-block partials of
 // dproj[c] = sum act[v][c] dOut[v] and dproj_b = sum dOut[v] ([block][17]).
 __global__ void __launch_bounds__(256) k_proj_bwd(const __nv_bfloat16 *act, const float *proj, const float *dout,
-                                                  __nv_bfloat16 *dact, float *partial, int64_t nvox) {
+                                                  __nv_bfloat16 *dact, float *partial, int64_t nvox, int nx) {
   __shared__ float red[17][256];
   float acc[17];
 #pragma unroll
   for (int c = 0; c < 17; ++c) acc[c] = 0.f;
   for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvox; v += (int64_t)gridDim.x * blockDim.x) {
     const float d = dout[v];
+    const int64_t row = v / nx;
+    const int x = (int)(v % nx);
 #pragma unroll
     for (int c = 0; c < 16; ++c) {
-      const float av = __bfloat162float(act[v * 16 + c]);
+      const int64_t e = act_elem(row, x, c, nx);
+      const float av = __bfloat162float(act[e]);
       acc[c] = fmaf(av, d, acc[c]);
-      dact[v * 16 + c] = __float2bfloat16(av > 0.f ? proj[c] * d : 0.f);
+      dact[e] = __float2bfloat16(av > 0.f ? proj[c] * d : 0.f);
     }
     acc[16] += d;
   }

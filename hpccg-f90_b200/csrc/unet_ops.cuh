@@ -7,7 +7,7 @@ namespace hpccg {
 struct CcConvArgs {
   int nx, ny, nz, nb;
   int nin, cin;                      // 16-channel input groups and total input channels
-  const __nv_bfloat16 *in0, *in1;    // channels-last BF16 inputs
+  const __nv_bfloat16 *in0, *in1;    // row-planar BF16 inputs
   const float *in_f32;               // or a 1-channel FP32 input (cin = 1)
   const float *W;                    // FP32 [27][cin][16]
   const float *bias;                 // [16] or null
@@ -38,9 +38,9 @@ __global__ void k_relu_mask(const float *d, const __nv_bfloat16 *act, __nv_bfloa
 __global__ void k_add_f32(const float *src, float *dst, int64_t n);
 __global__ void k_dW(DwArgs a);
 __global__ void k_reduce_partials(const float *partial, int nblocks, int n, float *grad, int accumulate);
-__global__ void k_proj_fwd(const __nv_bfloat16 *act, const float *proj, float *out, int64_t nvox);
+__global__ void k_proj_fwd(const __nv_bfloat16 *act, const float *proj, float *out, int64_t nvox, int nx);
 __global__ void k_proj_bwd(const __nv_bfloat16 *act, const float *proj, const float *dout, __nv_bfloat16 *dact,
-                           float *partial, int64_t nvox);
+                           float *partial, int64_t nvox, int nx);
 __global__ void k_mse(const float *out, const float *tgt, float *dout, float *partial, int64_t n);
 __global__ void k_energy(const float *out, const float *tgt, float *dout, float *partial, int nx, int ny, int nz,
                          int nb);

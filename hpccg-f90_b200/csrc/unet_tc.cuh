@@ -1,5 +1,5 @@
-// unet_tc.cuh -- sm_100a primitives for the U-Net convolutions: mbarriers, TMA
-// tensor loads, tcgen05 MMA with TMEM accumulators.  Written from the public
+// unet_tc.cuh -- sm_100a primitives for the U-Net convolutions: mbarriers,
+// bulk copies (cp.async.bulk), tcgen05 MMA with TMEM accumulators.  Written from the public
 // PTX ISA descriptions of these instructions.
 //
 // Every wait is bounded: after kSpinLimit polls it records `where` in an error
@@ -51,19 +51,18 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
   return false;
 }
 
-// ---- TMA --------------------------------------------------------------------------
-__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1,
-                                            int c2, int c3, int c4) {
+// ---- bulk copies ------------------------------------------------------------------
+// 1D bulk copy global -> shared (both 16-byte aligned, size a multiple of 16),
+// completing `bytes` of transaction on the mbarrier.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
   asm volatile(
-      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
-      "%6}], [%7];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
 }
-__device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map) {
-  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
-
 // ---- tcgen05 ------------------------------------------------------------------------
 // Allocate / free TMEM columns (whole warp).  The base address lands in *dst.
 __device__ __forceinline__ void tmem_alloc(uint32_t *dst, uint32_t ncols) {

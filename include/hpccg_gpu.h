@@ -221,12 +221,13 @@ int hpccg_unet_adam_step(hpccg_unet *unet, float lr, float beta1, float beta2, f
 /* Average ms of `reps` forward passes on one grid. */
 int hpccg_unet_time_forward(hpccg_unet *unet, int32_t nx, int32_t ny, int32_t nz, int32_t reps,
                             const float *d_in, float *d_out, float *ms);
-/* One 3x3x3 conv layer with 16 outputs, for tests: BF16 channels-last inputs
- * (nin = 1 or 2 groups of 16 channels), weights FP32 [27][16*nin][16],
+/* One 3x3x3 conv layer with 16 outputs, for tests: BF16 inputs in the
+ * row-planar layout [b][z][y][half][x][8 channels] (nin = 1 or 2 groups of 16
+ * channels; 16-channel outputs use the same layout), weights FP32 [27][16*nin][16],
  * epi 0 = bias+ReLU (BF16 out), 1 = bias (BF16), 2 = bias+ReLU then the 16->1
  * projection d_proj (FP32 out), 3 = raw FP32 16-channel out; path 0 =
  * tcgen05 (row tiles when nx is a multiple of 128), 1 = CUDA cores,
- * 2 = tcgen05 with per-tap loads. */
+ * 2 = tcgen05 with brick tiles (per-tap fetches). */
 int hpccg_unet_conv3_layer(int32_t nx, int32_t ny, int32_t nz, int32_t nb, int32_t nin, const void *d_in0,
                            const void *d_in1, const float *d_w, const float *d_bias, const float *d_proj,
                            int32_t epi, int32_t path, void *d_out);

@@ -27,6 +27,17 @@ def _bf16_tensor(torch, a):
     return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda().to(torch.bfloat16).contiguous()
 
 
+def to_planar(x):
+    """[b,z,y,x,16] channels-last -> the kernels' row-planar [b,z,y,half,x,8]."""
+    b, z, y, nx, c = x.shape
+    return np.ascontiguousarray(x.reshape(b, z, y, nx, 2, 8).transpose(0, 1, 2, 4, 3, 5))
+
+
+def from_planar(p):
+    b, z, y, _, nx, _ = p.shape
+    return p.transpose(0, 1, 2, 4, 3, 5).reshape(b, z, y, nx, 16)
+
+
 SHAPES = [(16, 16, 16, 1), (32, 8, 8, 2), (128, 4, 2, 1), (8, 8, 8, 3), (64, 16, 8, 1), (256, 3, 5, 2)]
 
 
@@ -42,12 +53,12 @@ def test_conv_layer_tc_and_cc(env, nx, ny, nz, nb, nin, epi):
     proj = rng.normal(0, 0.3, 17).astype(np.float32)
     x = np.concatenate(xs, -1).astype(np.float64)
     dW, db, dp = (torch.from_numpy(v).cuda() for v in (W, b, proj))
-    din = [_bf16_tensor(torch, v) for v in xs] + [None]
+    din = [_bf16_tensor(torch, to_planar(v)) for v in xs] + [None]
     for path, Wref in ((0, uo.bf16_round(W)), (2, uo.bf16_round(W)), (1, W)):
         pre = uo.conv3(x, Wref.astype(np.float64))
         if epi == 3:
             want = pre
-            out = torch.empty((nb, nz, ny, nx, 16), dtype=torch.float32, device="cuda")
+            out = torch.empty((nb, nz, ny, 2, nx, 8), dtype=torch.float32, device="cuda")
         elif epi == 2:
             want = np.maximum(pre + b, 0) @ proj[:16].astype(np.float64) + proj[16]
             out = torch.empty((nb, nz, ny, nx), dtype=torch.float32, device="cuda")
@@ -55,9 +66,11 @@ def test_conv_layer_tc_and_cc(env, nx, ny, nz, nb, nin, epi):
             want = pre + b
             if epi == 0:
                 want = np.maximum(want, 0)
-            out = torch.empty((nb, nz, ny, nx, 16), dtype=torch.bfloat16, device="cuda")
+            out = torch.empty((nb, nz, ny, 2, nx, 8), dtype=torch.bfloat16, device="cuda")
         hp.conv3_layer(din[0], din[1], dW, db, dp, epi, path, out, nx, ny, nz, nb)
         got = out.float().cpu().numpy().astype(np.float64)
+        if epi != 2:
+            got = from_planar(got)
         scale = np.abs(want).max() + 1e-30
         tol = 1e-3 * scale + (2.0 ** -8 * np.abs(want) if epi in (0, 1) else 0)
         assert np.all(np.abs(got - want) <= tol), (path, np.abs(got - want).max(), scale)
