@@ -36,19 +36,22 @@ struct Span {
   const __nv_bfloat16 *src;
   uint8_t *dst;
   uint32_t bytes;
+  bool zeroed;  // this lane wrote zero fill with ordinary stores
 };
 
 __device__ __forceinline__ Span plan_span(const ConvGeom &g, const __nv_bfloat16 *base, int b, int z, int y, int h,
                                           int xs, int len, uint8_t *dst) {
-  Span sp{nullptr, nullptr, 0};
+  Span sp{nullptr, nullptr, 0, false};
   const uint4 zero = make_uint4(0, 0, 0, 0);
   if (z < 0 || z >= g.nz || y < 0 || y >= g.ny) {
     for (int u = 0; u < len; ++u) reinterpret_cast<uint4 *>(dst)[u] = zero;
+    sp.zeroed = true;
     return sp;
   }
   const int lo = max(xs, 0), hi = min(xs + len, g.nx);
   for (int u = 0; u < lo - xs; ++u) reinterpret_cast<uint4 *>(dst)[u] = zero;
   for (int u = hi - xs; u < len; ++u) reinterpret_cast<uint4 *>(dst)[u] = zero;
+  sp.zeroed = lo > xs || hi < xs + len;
   if (hi <= lo) return sp;
   const int64_t row = ((int64_t)b * g.nz + z) * g.ny + y;
   sp.src = base + act_unit(row, h, lo, g.nx) * 8;
@@ -57,12 +60,17 @@ __device__ __forceinline__ Span plan_span(const ConvGeom &g, const __nv_bfloat16
   return sp;
 }
 
-// Posts the stage: zero fills are fenced, lane 0 arms the barrier with the
-// warp's total bulk bytes, then every lane issues its copies.
+// Posts the stage: lanes that zero-filled fence their stores into the async
+// proxy, lane 0 arms the barrier with the warp's total bulk bytes, then every
+// lane issues its copies.
 __device__ __forceinline__ void post_spans(const Span *sp, int nsp, uint64_t *bar, int lane) {
   uint32_t bytes = 0;
-  for (int i = 0; i < nsp; ++i) bytes += sp[i].bytes;
-  fence_proxy_async_smem();
+  bool zeroed = false;
+  for (int i = 0; i < nsp; ++i) {
+    bytes += sp[i].bytes;
+    zeroed |= sp[i].zeroed;
+  }
+  if (zeroed) fence_proxy_async_smem();  // only lanes that stored zeros
   const uint32_t total = __reduce_add_sync(0xffffffffu, bytes);
   __syncwarp();
   if (lane == 0) mbar_expect_tx(bar, total);
@@ -263,80 +271,148 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_brick(ConvArgs a) {
   }
 }
 
-// ---- row tiles: one fetch per tile, 27 taps from the halo rows ------------------------------
+// ---- row tiles: rolling window of slabs along y -------------------------------------------
+struct RowUnits {
+  int nxb, nchunks, nunits;
+};
+__host__ __device__ __forceinline__ RowUnits row_units(const ConvGeom &g) {
+  RowUnits r;
+  r.nxb = g.nx / 128;
+  r.nchunks = (g.ny + kRowChunk - 1) / kRowChunk;
+  r.nunits = r.nxb * g.nz * g.nb * r.nchunks;
+  return r;
+}
+struct RowUnit {
+  int b, z, x0, ya, yb;
+};
+__device__ __forceinline__ RowUnit row_unit(const ConvGeom &g, const RowUnits &ru, int u) {
+  RowUnit w;
+  const int c = u % ru.nchunks;
+  int r = u / ru.nchunks;
+  w.x0 = (r % ru.nxb) * 128;
+  r /= ru.nxb;
+  w.z = r % g.nz;
+  w.b = r / g.nz;
+  w.ya = c * kRowChunk;
+  w.yb = min(g.ny, w.ya + kRowChunk);
+  return w;
+}
+// Tile index (as tile_origin decodes it) of row y of a unit.
+__device__ __forceinline__ int row_tile_index(const ConvGeom &g, const RowUnit &w, int y) {
+  return ((w.b * g.nz + w.z) * g.ny + y) * g.tx + w.x0 / 128;
+}
+
 template <int NIN, int EPI>
 __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];
   constexpr int kWBytes = NIN * 27 * kWTapBytes;
-  constexpr int kStage = row_stage_bytes(NIN);
-  constexpr int S = kRowStages;
+  constexpr int kSlab = slab_bytes(NIN);
+  constexpr int R = row_slots(NIN);
   uint8_t *sW = smem;
   uint8_t *sA = smem + kWBytes;
-  uint64_t *full = reinterpret_cast<uint64_t *>(sA + S * kStage);
-  uint64_t *empty = full + S;
-  uint64_t *acc_full = empty + S;
+  uint64_t *full = reinterpret_cast<uint64_t *>(sA + R * kSlab);
+  uint64_t *empty = full + R;
+  uint64_t *acc_full = empty + R;
   uint64_t *acc_empty = acc_full + 2;
   uint64_t *drain = acc_empty + 2;
   uint32_t *slot = reinterpret_cast<uint32_t *>(drain + 1);
-  static_assert((2 * S + 5) * 8 + 4 <= bar_bytes(S), "barrier area");
+  static_assert((2 * R + 5) * 8 + 4 <= bar_bytes(R), "barrier area");
+  static_assert(R >= 4, "the window needs the three slabs of a tile plus one in flight");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t tmem = conv_setup<NIN, S>(a, sW, full, slot, warp);
+  const uint32_t tmem = conv_setup<NIN, R>(a, sW, full, slot, warp);
   const ConvGeom &g = a.g;
+  const RowUnits ru = row_units(g);
 
   if (warp == 0) {
-    // fetch: NIN inputs x 2 halves x 9 halo rows of 130 units (18*NIN spans)
-    uint32_t it = 0;
-    for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x, ++it) {
-      const int s = it % S;
-      const uint32_t n = it / S;
-      if (n > 0 && !warp_wait(&empty[s], (n - 1) & 1, a.err, 11, lane)) break;
-      const TileOrigin o = tile_origin(g, t);
-      uint8_t *stage = sA + s * kStage;
-      Span sp[2];
-      int nsp = 0;
-      for (int seg = lane; seg < 18 * NIN; seg += 32) {
-        const int r = seg % 9, h = (seg / 9) & 1, in = seg / 18;
-        const int dz = r / 3 - 1, dy = r % 3 - 1;
-        sp[nsp++] = plan_span(g, in ? a.in1 : a.in0, o.b, o.z0 + dz, o.y0 + dy, h, o.x0 - 1, kRowVox,
-                              stage + (in * 2 + h) * kRowPlaneBytes + r * kRowVox * 16);
+    // fetch slabs ya-1 .. yb of every unit: NIN x 2 halves x 3 z-rows spans
+    uint32_t sc = 0;
+    bool ok = true;
+    for (int u = blockIdx.x; u < ru.nunits && ok; u += gridDim.x) {
+      const RowUnit w = row_unit(g, ru, u);
+      for (int ys = w.ya - 1; ys <= w.yb; ++ys, ++sc) {
+        const int s = sc % R;
+        const uint32_t n = sc / R;
+        if (n > 0 && !(ok = warp_wait(&empty[s], (n - 1) & 1, a.err, 11, lane))) break;
+        uint8_t *base = sA + s * kSlab;
+        Span sp[1];
+        int nsp = 0;
+        if (lane < 6 * NIN) {
+          const int r = lane % 3, h = (lane / 3) & 1, in = lane / 6;
+          sp[0] = plan_span(g, in ? a.in1 : a.in0, w.b, w.z + r - 1, ys, h, w.x0 - 1, kRowVox,
+                            base + (in * 2 + h) * kSlabPlaneBytes + r * kRowVox * 16);
+          nsp = 1;
+        }
+        post_spans(sp, nsp, &full[s], lane);
       }
-      post_spans(sp, nsp, &full[s], lane);
     }
     if (lane == 0) {
-      const uint32_t first = it > (uint32_t)S ? it - S : 0;
-      for (uint32_t j = first; j < it; ++j) mbar_wait(&full[j % S], (j / S) & 1, a.err, 15);
+      const uint32_t first = sc > (uint32_t)R ? sc - R : 0;
+      for (uint32_t j = first; j < sc; ++j) mbar_wait(&full[j % R], (j / R) & 1, a.err, 15);
     }
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_bf16(128, 16);
-      uint32_t tcount = 0;
-      for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x, ++tcount) {
-        const int s = tcount % S;
-        const int buf = tcount & 1;
-        const uint32_t use = tcount >> 1;
-        if (use > 0 && !mbar_wait(&acc_empty[buf], (use - 1) & 1, a.err, 12)) break;
-        if (!mbar_wait(&full[s], (tcount / S) & 1, a.err, 13)) break;
-        tc_fence_after();
-        const uint32_t d = tmem + (uint32_t)(buf * 16);
-        const uint8_t *stage = sA + s * kStage;
+      uint32_t sc0 = 0, tcount = 0;
+      bool ok = true;
+      for (int u = blockIdx.x; u < ru.nunits && ok; u += gridDim.x) {
+        const RowUnit w = row_unit(g, ru, u);
+        const int ntile = w.yb - w.ya;
+        uint32_t ready = sc0;  // slabs [sc0, ready) have been waited for
+        for (int i = 0; i < ntile; ++i, ++tcount) {
+          const int buf = tcount & 1;
+          const uint32_t use = tcount >> 1;
+          if (use > 0 && !(ok = mbar_wait(&acc_empty[buf], (use - 1) & 1, a.err, 12))) break;
+          for (; ready < sc0 + i + 3; ++ready)
+            if (!(ok = mbar_wait(&full[ready % R], (ready / R) & 1, a.err, 13))) break;
+          if (!ok) break;
+          tc_fence_after();
+          const uint32_t d = tmem + (uint32_t)(buf * 16);
 #pragma unroll 1
-        for (int ks = 0; ks < 27 * NIN; ++ks) {
-          const int tap = ks / NIN, in = ks % NIN;
-          const int r = (tap / 9) * 3 + (tap / 3) % 3;  // (dz+1)*3 + (dy+1)
-          const int dxp = tap % 3;                       // dx + 1
-          const uint64_t ad =
-              smem_desc(stage + in * 2 * kRowPlaneBytes + (r * kRowVox + dxp) * 16, kRowPlaneBytes, 128);
-          const uint64_t bd = smem_desc(sW + (in * 27 + tap) * kWTapBytes, 256, 128);
-          mma_bf16(d, ad, bd, idesc, ks > 0 ? 1u : 0u);
+          for (int ks = 0; ks < 27 * NIN; ++ks) {
+            const int tap = ks / NIN, in = ks % NIN;
+            const int dzp = tap / 9, dyp = (tap / 3) % 3, dxp = tap % 3;  // offsets + 1
+            const uint8_t *sl = sA + ((sc0 + i + dyp) % R) * kSlab;
+            const uint64_t ad =
+                smem_desc(sl + in * 2 * kSlabPlaneBytes + (dzp * kRowVox + dxp) * 16, kSlabPlaneBytes, 128);
+            const uint64_t bd = smem_desc(sW + (in * 27 + tap) * kWTapBytes, 256, 128);
+            mma_bf16(d, ad, bd, idesc, ks > 0 ? 1u : 0u);
+          }
+          mma_commit(&acc_full[buf]);
+          mma_commit(&empty[(sc0 + i) % R]);  // slab y-1 of this tile is done for the unit
         }
-        mma_commit(&empty[s]);
-        mma_commit(&acc_full[buf]);
+        if (!ok) break;
+        mma_commit(&empty[(sc0 + ntile) % R]);  // the unit's last two slabs
+        mma_commit(&empty[(sc0 + ntile + 1) % R]);
+        sc0 += ntile + 2;
       }
       mma_commit(drain);
       mbar_wait(drain, 0, a.err, 16);
     }
   } else {
-    conv_epilogue<EPI>(a, acc_full, acc_empty, tmem, warp, lane, 14);
+    // epilogue: tiles in unit order
+    const int q = warp & 3;
+    uint32_t tcount = 0;
+    float bias[16], proj[17];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) bias[c] = (EPI == kEpiRawF32 || !a.bias) ? 0.f : a.bias[c];
+    if (EPI == kEpiProject)
+#pragma unroll
+      for (int c = 0; c < 17; ++c) proj[c] = a.proj[c];
+    bool ok = true;
+    for (int u = blockIdx.x; u < ru.nunits && ok; u += gridDim.x) {
+      const RowUnit w = row_unit(g, ru, u);
+      for (int y = w.ya; y < w.yb; ++y, ++tcount) {
+        const int buf = tcount & 1;
+        if (!(ok = mbar_wait(&acc_full[buf], (tcount >> 1) & 1, a.err, 14))) break;
+        tc_fence_after();
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 16), v);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[buf]);
+        conv_store<EPI>(a, row_tile_index(g, w, y), q * 32 + lane, v, bias, proj);
+      }
+    }
   }
   tc_fence_before();
   __syncthreads();
@@ -354,10 +430,11 @@ static int launch_one(const ConvArgs &a, int num_sms, cudaStream_t s) {
   static int per_sm = 0;
   if (!per_sm) {
     HPCCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    HPCCG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kConvThreads, smem));
-    if (per_sm < 1) per_sm = 1;
+    // resident CTAs per SM by shared memory (each CTA also reserves 1 KB)
+    per_sm = std::max(1, (227 * 1024) / (smem + 1024));
   }
-  const int grid = std::min(a.g.ntiles, num_sms * per_sm);
+  const int work = ROW ? row_units(a.g).nunits : a.g.ntiles;
+  const int grid = std::min(work, num_sms * per_sm);
   kern<<<grid, kConvThreads, smem, s>>>(a);
   HPCCG_CUDA(cudaGetLastError());
   return HPCCG_OK;

@@ -13,8 +13,9 @@
 // for each of the 27 taps and each 16-channel input group, one tcgen05.mma
 // (M=128, N=16, K=16) accumulates into a 16-column FP32 TMEM accumulator.
 //  * row tiles (nx a multiple of 128): a tile is one 128-voxel x-row; the
-//    3x3 neighbouring rows with a 1-voxel x halo (9 x 130 units per half) are
-//    fetched once and the 27 taps read them through shifted descriptors;
+//    3x3 neighbouring rows with a 1-voxel x halo are three "slabs" shared with
+//    the neighbouring tiles in y, and the 27 taps read them through shifted
+//    descriptors (one new slab fetched per tile);
 //  * brick tiles (smaller nx): a tile is a bx*by*bz brick and each tap's
 //    shifted brick is fetched separately (by*bz row spans per half).
 // Roles per CTA (192 threads): warp 0 fetches (its lanes issue the row spans
@@ -40,18 +41,23 @@ constexpr int kWTapBytes = 16 * 16 * 2;  // one tap of B: 16 x 16 BF16
 // Brick tiles: one stage per k-step (tap, input): 2 halves x 128 units.
 constexpr int kBrickStages = 24;
 constexpr int kBrickStageBytes = 2 * 128 * 16;
-// Row tiles: one stage per tile: inputs x 2 halves x (9 rows x 130 units), 128-B aligned planes.
+// Row tiles (nx a multiple of 128) walk y inside a work unit (b, z, 128-voxel
+// x block, chunk of up to kRowChunk rows of y).  A "slab" is grid row y of the
+// three z planes z-1, z, z+1 with a 1-voxel x halo: 3 rows x 130 units per
+// half.  Tile y reads slabs y-1, y, y+1, so each tile fetches one new slab and
+// a ring of kRowSlots slabs keeps several fetches in flight.
 constexpr int kRowVox = 130;
-constexpr int kRowPlaneBytes = ((9 * kRowVox * 16 + 127) / 128) * 128;
-constexpr int kRowStages = 2;
-__host__ __device__ constexpr int row_stage_bytes(int nin) { return nin * 2 * kRowPlaneBytes; }
+constexpr int kRowChunk = 32;
+constexpr int kSlabPlaneBytes = ((3 * kRowVox * 16 + 127) / 128) * 128;
+__host__ __device__ constexpr int slab_bytes(int nin) { return nin * 2 * kSlabPlaneBytes; }
+__host__ __device__ constexpr int row_slots(int nin) { return nin == 1 ? 8 : 6; }
 // mbarriers: full[S], empty[S], acc_full[2], acc_empty[2], drain, + TMEM slot.
 __host__ __device__ constexpr int bar_bytes(int stages) { return (2 * stages + 5) * 8 + 16; }
 __host__ __device__ constexpr int brick_smem_bytes(int nin) {
   return nin * 27 * kWTapBytes + kBrickStages * kBrickStageBytes + bar_bytes(kBrickStages);
 }
 __host__ __device__ constexpr int row_smem_bytes(int nin) {
-  return nin * 27 * kWTapBytes + kRowStages * row_stage_bytes(nin) + bar_bytes(kRowStages);
+  return nin * 27 * kWTapBytes + row_slots(nin) * slab_bytes(nin) + bar_bytes(row_slots(nin));
 }
 
 enum ConvEpi : int {

@@ -123,13 +123,13 @@ def test_gradients_match_oracle(env):
 def test_trained_network_reduces_fcg_iterations(env):
     """What the trained network gains: FCG iterations to FP64 rel-res 1e-8 on
     held-out Gaussian-random-field right-hand sides, against plain CG through
-    the same solver (net = None).  Trained briefly on 32^3 grids."""
+    the same solver (net = None).  Trained on 64^3 grids as the bench does."""
     torch, hp = env
     from hpccg_b200 import learned
 
-    net, hist = learned.train_preconditioner(32, seed=2, rhs=24, rounds=2, steps=150, batch=4)
+    net, hist = learned.train_preconditioner(64, seed=2, rhs=48, rounds=3, steps=300, batch=4)
     assert np.mean(hist[-20:]) < 0.5 * np.mean(hist[:5])
-    for n in (32, 64):
+    for n in (64, 96):
         M = hp.Matrix.generated(n, n, n)
         for sd in (77, 78):
             b = learned.gaussian_random_field(M, n, sd, torch)
