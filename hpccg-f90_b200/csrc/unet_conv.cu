@@ -236,6 +236,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_brick(ConvArgs a) {
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_bf16(128, 16);
+      const uint64_t ad0 = smem_desc(sA, kBrickStageBytes / 2, 128), wd = smem_desc(sW, 256, 128);
       uint32_t it = 0, tcount = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < g.ntiles && ok; t += gridDim.x, ++tcount) {
@@ -248,9 +249,8 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_brick(ConvArgs a) {
           const int s = it % S;
           if (!(ok = mbar_wait(&full[s], (it / S) & 1, a.err, 3))) break;
           tc_fence_after();
-          const int tap = ks / NIN, in = ks % NIN;
-          const uint64_t ad = smem_desc(sA + s * kBrickStageBytes, kBrickStageBytes / 2, 128);
-          const uint64_t bd = smem_desc(sW + (in * 27 + tap) * kWTapBytes, 256, 128);
+          const uint64_t ad = ad0 + (uint64_t)((s * kBrickStageBytes) >> 4);
+          const uint64_t bd = wd + (uint64_t)((ks % NIN * 27 + ks / NIN) * (kWTapBytes >> 4));
           mma_bf16(d, ad, bd, idesc, ks > 0 ? 1u : 0u);
           mma_commit(&empty[s]);
         }
@@ -352,6 +352,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_bf16(128, 16);
+      const uint64_t wd = smem_desc(sW, 256, 128);
       uint32_t sc0 = 0, tcount = 0;
       bool ok = true;
       for (int u = blockIdx.x; u < ru.nunits && ok; u += gridDim.x) {
@@ -367,14 +368,17 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
           if (!ok) break;
           tc_fence_after();
           const uint32_t d = tmem + (uint32_t)(buf * 16);
-#pragma unroll 1
+          // descriptors of the three slabs (y-1, y, y+1); a tap adds a constant
+          // offset (address field in 16-byte units, no carry: smem < 256 KB)
+          uint64_t sd[3];
+#pragma unroll
+          for (int j = 0; j < 3; ++j) sd[j] = smem_desc(sA + ((sc0 + i + j) % R) * kSlab, kSlabPlaneBytes, 128);
+#pragma unroll
           for (int ks = 0; ks < 27 * NIN; ++ks) {
             const int tap = ks / NIN, in = ks % NIN;
             const int dzp = tap / 9, dyp = (tap / 3) % 3, dxp = tap % 3;  // offsets + 1
-            const uint8_t *sl = sA + ((sc0 + i + dyp) % R) * kSlab;
-            const uint64_t ad =
-                smem_desc(sl + in * 2 * kSlabPlaneBytes + (dzp * kRowVox + dxp) * 16, kSlabPlaneBytes, 128);
-            const uint64_t bd = smem_desc(sW + (in * 27 + tap) * kWTapBytes, 256, 128);
+            const uint64_t ad = sd[dyp] + (uint64_t)((in * 2 * kSlabPlaneBytes + (dzp * kRowVox + dxp) * 16) >> 4);
+            const uint64_t bd = wd + (uint64_t)(((in * 27 + tap) * kWTapBytes) >> 4);
             mma_bf16(d, ad, bd, idesc, ks > 0 ? 1u : 0u);
           }
           mma_commit(&acc_full[buf]);
