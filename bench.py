@@ -12,7 +12,11 @@ Inputs (5.4 GB of matrix) are far larger than the 126 MB L2, so no flush is
 needed between steps.
 
 Solvers timed: plain FP64 CG (the reference's algorithm), and FP64 iterative
-refinement around an FP32 or BF16-value inner CG.  `value` is the device time
+refinement around an FP32 or BF16-value inner CG, each on the stored matrix
+(column-major ELL copy of the CSR, the reference's representation); then the
+same FP64 CG and the FP32 refinement with the matrix-free stencil SpMV (the
+operator checked equal to the CSR entry by entry; FP64 results bit-identical),
+and, unless --no-learned, the flexible PCG with the U-Net trained in-run.  `value` is the device time
 of one solve of the fastest solver whose FP64 true residual meets 1e-8 (CUDA
 events on the library stream, max over ranks); config.methods lists every
 solver.  `e2e` is the same solve through the host-array C-ABI call
@@ -45,7 +49,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "hpccg-f90_b200"))
 
-METRIC = "s to rel-res 1e-8 @256^3 (FP64 true residual), best of plain FP64 CG / mixed-precision IR"
+METRIC = ("s to rel-res 1e-8 @256^3 (FP64 true residual), best of FP64 CG / mixed-precision IR "
+          "(stored-matrix ELL or checked matrix-free stencil SpMV)")
 SEED_XSTAR = 1234
 REL_TOL = 1e-8
 
@@ -250,7 +255,8 @@ def run_ours(args):
     for prec in (hp.PREC_FP32, hp.PREC_BF16):
         M.set_mixed_rows_per_thread(prec, 4)
 
-    # Each solver maps to (device solve returning (info dict, kernel launches), host-array solve).
+    # Each solver: a device solve returning (info dict, kernel launches), run
+    # with the SpMV kind listed beside it.
     def fp64_cg():
         it, _, _, st = M.cg_device(d_b, d_x, max_iter, tol, history=False)
         assert st == hp.HPCCG_OK, st
@@ -264,9 +270,15 @@ def run_ours(args):
             return {"outer": info.outer_iters, "inner": info.inner_iters, "device_relres": info.relres}, launches
         return run
 
-    methods = [("fp64_cg", "plain FP64 CG (reference operation order), one CUDA graph", fp64_cg),
-               ("fp32_ir", "FP64 iterative refinement, FP32 inner CG", mixed(hp.PREC_FP32)),
-               ("bf16_ir", "FP64 iterative refinement, inner CG on BF16 values / FP32 vectors", mixed(hp.PREC_BF16))]
+    ELL, STENCIL = hp.SPMV_AUTO, hp.SPMV_STENCIL
+    methods = [("fp64_cg", "plain FP64 CG (reference operation order), one CUDA graph", fp64_cg, ELL),
+               ("fp32_ir", "FP64 iterative refinement, FP32 inner CG", mixed(hp.PREC_FP32), ELL),
+               ("bf16_ir", "FP64 iterative refinement, inner CG on BF16 values / FP32 vectors", mixed(hp.PREC_BF16),
+                ELL),
+               ("fp64_cg_stencil", "plain FP64 CG with the matrix-free stencil SpMV (bit-identical to fp64_cg)",
+                fp64_cg, STENCIL),
+               ("fp32_ir_stencil", "FP64 iterative refinement (FP64 stencil residual), FP32 matrix-free inner CG",
+                mixed(hp.PREC_FP32), STENCIL)]
     learned_info = None
     if not args.no_learned:
         from hpccg_b200 import learned
@@ -283,11 +295,12 @@ def run_ours(args):
             return ({"iterations": info.iters, "nn_applies": info.nn_applies, "fallback": info.fallback},
                     4 + 25 * info.iters)
 
-        methods.append(("learned_fcg", "flexible PCG (FP64) with the trained U-Net preconditioner (BF16 tensor cores)",
-                        learned_fcg))
+        methods.append(("learned_fcg", "flexible PCG (FP64, matrix-free stencil SpMV) with the trained U-Net "
+                        "preconditioner (BF16 tensor cores)", learned_fcg, STENCIL))
     results = {}
     clk_summary = None
-    for name, desc, fn in methods:
+    for name, desc, fn, kind in methods:
+        M.set_spmv(kind)
         for _ in range(args.warmup):
             d_x.zero_()
             fn()
@@ -308,10 +321,12 @@ def run_ours(args):
         relres = _fp64_relres(M, d_x, d_b, bnorm, scratch)
         err = float((d_x - xstar).abs().max().item())
         results[name] = {"ms": ms, "method": desc, "true_relres": relres, "max_abs_err_vs_xstar": err,
-                         "gpu_launches": launches, "clocks": clk.summary(), **info}
+                         "gpu_launches": launches, "clocks": clk.summary(), "spmv_kernel": list(M.get_spmv()),
+                         **info}
     if learned_info is not None:
         # the learned method on its own workload: Gaussian-random-field right-hand side
         grf = learned.gaussian_random_field(M, n, 4242, torch)
+        M.set_spmv(STENCIL)
         d_x.zero_()
         it_plain, _, _, _ = M.cg_device(grf, d_x, max_iter, REL_TOL * float(torch.linalg.vector_norm(grf)),
                                         history=False)
@@ -327,6 +342,7 @@ def run_ours(args):
     ok = {k: v for k, v in results.items() if v["true_relres"] <= REL_TOL}
     head = min(ok, key=lambda k: ok[k]["ms"])
     plain_ms = results["fp64_cg"]["ms"]
+    head_kind = STENCIL if head.endswith("_stencil") or head == "learned_fcg" else ELL
 
     # end to end through the host-array C-ABI call of the headline solver, pinned host buffers
     h_b = torch.empty(N, dtype=torch.float64, pin_memory=True)
@@ -334,13 +350,19 @@ def run_ours(args):
     h_x = torch.zeros(N, dtype=torch.float64, pin_memory=True)
     xb, bb = h_x.numpy(), h_b.numpy()
     e2e = []
+    M.set_spmv(head_kind)
     for s in range(args.warmup + args.steps):
         xb[:] = 0.0
         t0 = time.perf_counter()
-        if head == "fp64_cg":
+        if head.startswith("fp64_cg"):
             M.cg(bb, xb, max_iter, tol, history=False)
+        elif head == "learned_fcg":
+            h_bd = torch.from_numpy(bb).to(dev)
+            d_xe = torch.zeros_like(h_bd)
+            learned.solve_fcg(M, net, n, h_bd, d_xe, REL_TOL, max_iter)
+            xb[:] = d_xe.cpu().numpy()
         else:
-            M.solve_mixed(bb, xb, hp.PREC_FP32 if head == "fp32_ir" else hp.PREC_BF16, REL_TOL)
+            M.solve_mixed(bb, xb, hp.PREC_BF16 if head == "bf16_ir" else hp.PREC_FP32, REL_TOL)
         dt = time.perf_counter() - t0
         if s >= args.warmup:
             e2e.append(dt)
@@ -349,6 +371,7 @@ def run_ours(args):
     # rooflines (CUDA events on the library stream around back-to-back launches)
     hbm, _, peak_kind = _peaks()
     nnz = M.nnz
+    M.set_spmv(ELL)
     kms64 = M.time_cg_kernels(reps=20)
     alg64 = 12 * nnz + 20 * N + 4
     roof64 = {"bound": "hbm", "kernel": "k_cg_spmv_dot (FP64 SpMV + p.Ap)", "kernel_ms": kms64[1],
@@ -364,6 +387,23 @@ def run_ours(args):
                        "peak": hbm, "unit": "GB/s", "peak_source": peak_kind, "traffic": None,
                        "inner_iteration_ms": sum(km)}
         roofs[name]["frac"] = roofs[name]["achieved"] / hbm
+    M.set_spmv(STENCIL)
+    kst = M.time_cg_kernels(reps=20)
+    alg = 16 * N + 4  # x read once, y written; A is not stored
+    roofs["fp64_cg_stencil"] = {"bound": "hbm", "kernel": "k_cg_spmv_dot<StratStencil> (matrix-free FP64 SpMV + p.Ap)",
+                                "kernel_ms": kst[1], "alg_bytes_per_launch": alg,
+                                "achieved": alg / (kst[1] * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                                "peak_source": peak_kind, "traffic": None, "iteration_ms": sum(kst)}
+    roofs["fp64_cg_stencil"]["frac"] = roofs["fp64_cg_stencil"]["achieved"] / hbm
+    km = M.time_mixed_kernels(hp.PREC_FP32, 20)
+    alg = 8 * N + 4
+    roofs["fp32_ir_stencil"] = {"bound": "hbm",
+                                "kernel": "k_mp_spmv_dot<StratLpStencil> (matrix-free FP32 SpMV + p.Ap)",
+                                "kernel_ms": km[1], "alg_bytes_per_launch": alg,
+                                "achieved": alg / (km[1] * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                                "peak_source": peak_kind, "traffic": None, "inner_iteration_ms": sum(km)}
+    roofs["fp32_ir_stencil"]["frac"] = roofs["fp32_ir_stencil"]["achieved"] / hbm
+    roofs["learned_fcg"] = roofs["fp64_cg_stencil"]
 
     if rank != 0:
         if ws > 1:
@@ -381,19 +421,22 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": hr["ms"] / 1e3, "unit": "s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": hr["ms"], "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if head == "fp64_cg" else "f32/bf16 inner, f64 outer",
+        "vs_baseline": None, "dtype": "f64" if head.startswith("fp64") or head == "learned_fcg"
+        else "f32/bf16 inner, f64 outer",
         "data": "synthetic",
         "config": {"workload": f"{n}^3 27-point HPCCG matrix ({N} rows, {nnz} nonzeros), x* U[-1,1) seed 1234, "
                                f"b = A x*, x0 = 0, solved to FP64 ||b - A x|| <= 1e-8 ||b||",
                    "method": head, "speedup_vs_plain_gpu_cg": plain_ms / hr["ms"],
+                   "speedup_vs_plain_gpu_cg_stencil": results["fp64_cg_stencil"]["ms"] / hr["ms"],
                    "methods": results, "learned": learned_info,
                    "l2": "inputs (5.4 GB matrix) exceed the 126 MB L2; no flush",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
-                   "spmv_kernel": list(M.get_spmv())},
+                   "spmv_kernel": results[head]["spmv_kernel"]},
         "roofline": roofs[head], "roofline_all": roofs,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 16 * N, "d2h_bytes_per_step": 8 * N,
-                "call": "hpccg_gpu_cg" if head == "fp64_cg" else "hpccg_gpu_solve_mixed"},
+                "call": "hpccg_gpu_cg" if head.startswith("fp64_cg") else
+                ("hpccg_gpu_solve_fcg" if head == "learned_fcg" else "hpccg_gpu_solve_mixed")},
         "gpu_launches": hr["gpu_launches"],
         "clocks": hr["clocks"],
     }

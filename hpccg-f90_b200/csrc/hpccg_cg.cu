@@ -399,7 +399,8 @@ extern "C" int hpccg_gpu_cg_device(hpccg_ctx *c, const double *d_b, double *d_x,
 
 extern "C" int hpccg_gpu_set_spmv(hpccg_ctx *c, int32_t kind, int32_t param) {
   if (!c) return HPCCG_ERR_INVALID_ARG;
-  if (kind < HPCCG_SPMV_AUTO || kind > HPCCG_SPMV_CSR_VECTOR) return HPCCG_ERR_INVALID_ARG;
+  if (kind < HPCCG_SPMV_AUTO || kind > HPCCG_SPMV_STENCIL) return HPCCG_ERR_INVALID_ARG;
+  if (kind == HPCCG_SPMV_STENCIL && !c->gx) return HPCCG_ERR_UNSUPPORTED;
   if ((kind == HPCCG_SPMV_ELL || kind == HPCCG_SPMV_ELL2) && !c->d_ell_col) return HPCCG_ERR_UNSUPPORTED;
   if (kind == HPCCG_SPMV_ELL2 && c->ell_width != 27) return HPCCG_ERR_UNSUPPORTED;
   if (kind == HPCCG_SPMV_CSR_VECTOR && param != 4 && param != 8 && param != 16 && param != 32)
@@ -409,6 +410,7 @@ extern "C" int hpccg_gpu_set_spmv(hpccg_ctx *c, int32_t kind, int32_t param) {
     return HPCCG_ERR_INVALID_ARG;
   c->spmv_kind = kind;
   c->spmv_param = (kind != HPCCG_SPMV_CSR_VECTOR && param == 0) ? 4 : param;
+  if (kind == HPCCG_SPMV_STENCIL) c->spmv_param = 0;
   c->spmv_tuned = kind != HPCCG_SPMV_AUTO;
   return HPCCG_OK;
 }

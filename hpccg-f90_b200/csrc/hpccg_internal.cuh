@@ -67,6 +67,8 @@ struct hpccg_ctx {
   double *d_hist = nullptr;
   int32_t hist_cap = 0;
   int grid = 0;  // blocks for streaming kernels (multiple of the SM count)
+  // grid of generate_matrix the CSR was checked against (0: unknown)
+  int32_t gx = 0, gy = 0, gz = 0;
   // SpMV selection
   int spmv_kind = HPCCG_SPMV_AUTO;
   int spmv_param = 0;

@@ -324,6 +324,58 @@ fail:
   return rc ? rc : HPCCG_ERR_CUDA;
 }
 
+// Compares row i of the CSR with generate_matrix(nx,ny,nz): the kept
+// stencil columns in (sz, sy, sx) order, 27.0 on the diagonal and -1.0
+// elsewhere (MPI/src/SparseMatrix.F90:146-159).  Counts rows that differ.
+__global__ void check_stencil_kernel(int32_t n, int nx, int ny, int nz, const int32_t *rowptr,
+                                     const int32_t *col, const double *val, unsigned *bad) {
+  const int nxy = nx * ny;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int iz = i / nxy, rem = i - iz * nxy, iy = rem / nx, ix = rem - iy * nx;
+    const int32_t e = rowptr[i + 1];
+    int32_t k = rowptr[i];
+    bool ok = k >= 0 && e >= k;
+    for (int sz = -1; sz <= 1 && ok; ++sz)
+      for (int sy = -1; sy <= 1 && ok; ++sy)
+        for (int sx = -1; sx <= 1 && ok; ++sx) {
+          if ((unsigned)(iz + sz) >= (unsigned)nz || (unsigned)(iy + sy) >= (unsigned)ny ||
+              (unsigned)(ix + sx) >= (unsigned)nx)
+            continue;
+          const int j = i + sz * nxy + sy * nx + sx;
+          ok = k < e && col[k] == j && val[k] == (j == i ? 27.0 : -1.0);
+          ++k;
+        }
+    if (!ok || k != e) atomicAdd(bad, 1u);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && rowptr[0] != 0) atomicAdd(bad, 1u);
+}
+
+extern "C" int hpccg_gpu_set_geometry(hpccg_ctx *c, int32_t nx, int32_t ny, int32_t nz) {
+  if (!c || nx < 1 || ny < 1 || nz < 1 || (int64_t)nx * ny * nz != (int64_t)c->nrow) return HPCCG_ERR_INVALID_ARG;
+  c->gx = c->gy = c->gz = 0;
+  if (c->spmv_kind == HPCCG_SPMV_STENCIL) {
+    c->spmv_kind = HPCCG_SPMV_AUTO;
+    c->spmv_tuned = false;
+  }
+  unsigned *d_bad = nullptr, h_bad = 1;
+  HPCCG_CUDA(cudaMalloc(&d_bad, sizeof(unsigned)));
+  cudaError_t e = cudaMemsetAsync(d_bad, 0, sizeof(unsigned), c->stream);
+  if (e == cudaSuccess) {
+    check_stencil_kernel<<<grid_for(c, c->nrow), kBlock, 0, c->stream>>>(c->nrow, nx, ny, nz, c->d_rowptr,
+                                                                         c->d_col, c->d_val, d_bad);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, d_bad, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d_bad);
+  if (e != cudaSuccess) return set_cuda_error(e, "stencil check", __FILE__, __LINE__);
+  if (h_bad) return HPCCG_ERR_UNSUPPORTED;
+  c->gx = nx;
+  c->gy = ny;
+  c->gz = nz;
+  return HPCCG_OK;
+}
+
 // Longest row of generate_matrix: min(n,3) kept offsets per axis.
 static int generated_width(int nx, int ny, int nz) {
   return std::min(nx, 3) * std::min(ny, 3) * std::min(nz, 3);
@@ -351,6 +403,7 @@ extern "C" int hpccg_gpu_create_generated(int32_t nx, int32_t ny, int32_t nz, do
     rc = set_cuda_error(cudaGetLastError(), "generate matrix", __FILE__, __LINE__);
     goto fail;
   }
+  if ((rc = hpccg_gpu_set_geometry(c, nx, ny, nz))) goto fail;  // the matrix-free SpMV's precondition
   *out = c;
   return HPCCG_OK;
 fail:

@@ -37,6 +37,7 @@ struct MixedArgs {
   const void *val_lp;
   MixedState *st;
   Reduction red;
+  StencilGeom geom;  // matrix-free inner SpMV when the context uses the stencil
   cudaGraphConditionalHandle cond_outer, cond_inner;
   int use_cond;
 };
@@ -178,7 +179,7 @@ template <class S, typename VT>
 __global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_spmv_dot(MixedArgs g) {
   __shared__ double smem[32];
   EpiDot32 epi{g.p, g.Ap};
-  const double part = S::rows(g.n, g.npad, g.ell_col, reinterpret_cast<const VT *>(g.val_lp), g.p, epi);
+  const double part = S::rows(g.n, g.npad, g.ell_col, reinterpret_cast<const VT *>(g.val_lp), g.p, epi, g.geom);
   const double tot = block_sum<kBlock>(part, smem);
   if (arrive_last(g.red, tot)) {
     const double pAp = finish_sum<kBlock>(g.red, smem);
@@ -262,9 +263,10 @@ struct EpiStore32 {
 };
 template <class S, typename VT>
 __global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_spmv_lp(int n, int npad, const int32_t *col,
-                                                                   const VT *val, const float *x, float *y) {
+                                                                   const VT *val, const float *x, float *y,
+                                                                   StencilGeom geom) {
   EpiStore32 epi{y};
-  S::rows(n, npad, col, val, x, epi);
+  S::rows(n, npad, col, val, x, epi, geom);
 }
 
 __global__ void k_to_lp(const double *src, float *f32, __nv_bfloat16 *b16, size_t count) {
@@ -275,9 +277,11 @@ __global__ void k_to_lp(const double *src, float *f32, __nv_bfloat16 *b16, size_
   }
 }
 
-// Low-precision strategy dispatch: value type by precision, RPT and MINB by param.
+// Low-precision strategy dispatch: the matrix-free stencil when the context
+// uses it, else value type by precision, RPT and MINB by param.
 template <class F>
-inline int dispatch_lp(int precision, int rpt, F &&f) {
+inline int dispatch_lp(bool stencil, int precision, int rpt, F &&f) {
+  if (stencil) return f(StratLpStencil{}, (float *)nullptr);
   if (precision == 1) {
     switch (rpt) {
       case 1: return f(StratLp<float, 1, 4>{}, (float *)nullptr);
@@ -305,6 +309,7 @@ struct MixedRes {
   MixedState *st = nullptr;
   cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
   int exec_rpt[3] = {0, 0, 0};
+  bool exec_stencil[3] = {false, false, false};
   int rpt[3] = {0, 2, 4};  // rows per thread per precision (index 1 = FP32, 2 = BF16)
 };
 
@@ -338,8 +343,11 @@ __global__ void k_pad_vals27(const double *src, int W, int npad, double *dst) {
     for (int k = 0; k < 27; ++k) dst[(size_t)k * npad + i] = k < W ? src[(size_t)k * npad + i] : 0.0;
 }
 
+static bool uses_stencil(const hpccg_ctx *c) { return spmv_args(c).kind == HPCCG_SPMV_STENCIL; }
+
 static int mixed_res(hpccg_ctx *c, int precision, MixedRes **out) {
-  if (!c->d_ell_col || c->ell_width > 27) return HPCCG_ERR_UNSUPPORTED;
+  const bool stencil = uses_stencil(c);
+  if (!stencil && (!c->d_ell_col || c->ell_width > 27)) return HPCCG_ERR_UNSUPPORTED;
   std::lock_guard<std::mutex> lk(g_mixed_mu);
   MixedRes *&m = g_mixed[c];
   if (!m) {
@@ -355,7 +363,8 @@ static int mixed_res(hpccg_ctx *c, int precision, MixedRes **out) {
   const size_t slots = (size_t)27 * c->npad;
   const double *src = c->d_ell_val;
   double *tmp = nullptr;
-  if ((precision == 1 && !m->val32) || (precision == 2 && !m->val16) || (!m->col27 && c->ell_width != 27)) {
+  if (!stencil &&
+      ((precision == 1 && !m->val32) || (precision == 2 && !m->val16) || (!m->col27 && c->ell_width != 27))) {
     if (c->ell_width != 27) {
       HPCCG_CUDA(cudaMalloc(&tmp, sizeof(double) * slots));
       k_pad_vals27<<<c->num_sms * 8, kBlock, 0, c->stream>>>(c->d_ell_val, c->ell_width, c->npad, tmp);
@@ -396,12 +405,13 @@ static MixedArgs mixed_args(hpccg_ctx *c, MixedRes *m, int precision) {
   g.val_lp = precision == 1 ? (const void *)m->val32 : (const void *)m->val16;
   g.st = m->st;
   g.red = reduction_of(c);
+  g.geom = StencilGeom{c->gx, c->gy, c->gz};
   return g;
 }
 
 static int launch_inner_body(hpccg_ctx *c, MixedRes *m, int precision, const MixedArgs &g, cudaStream_t s) {
   k_mp_update_p<<<c->grid, kBlock, 0, s>>>(g);
-  int rc = dispatch_lp(precision, m->rpt[precision], [&](auto strat, auto *vt) {
+  int rc = dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
     using St = decltype(strat);
     using VT = std::remove_pointer_t<decltype(vt)>;
     k_mp_spmv_dot<St, VT><<<c->grid, kBlock, 0, s>>>(g);
@@ -504,6 +514,7 @@ static int build_mixed_graph(hpccg_ctx *c, MixedRes *m, int precision) {
     return set_cuda_error(e, "build mixed graph", __FILE__, __LINE__);
   }
   m->exec_rpt[precision] = m->rpt[precision];
+  m->exec_stencil[precision] = uses_stencil(c);
   return HPCCG_OK;
 }
 
@@ -562,7 +573,8 @@ static int solve_mixed_common(hpccg_ctx *c, int precision, double rel_tol, int32
   if (eager) {
     if ((rc = run_mixed_eager(c, m, precision))) return rc;
   } else {
-    if (!m->exec[precision] || m->exec_rpt[precision] != m->rpt[precision])
+    if (!m->exec[precision] || m->exec_rpt[precision] != m->rpt[precision] ||
+        m->exec_stencil[precision] != uses_stencil(c))
       if ((rc = build_mixed_graph(c, m, precision))) return rc;
     HPCCG_CUDA(cudaGraphLaunch(m->exec[precision], c->stream));
   }
@@ -622,10 +634,11 @@ extern "C" int hpccg_gpu_spmv_lowp(hpccg_ctx *c, int32_t precision, const float 
   if (rc) return rc;
   const int32_t *col = m->col27 ? m->col27 : c->d_ell_col;
   const void *val = precision == 1 ? (const void *)m->val32 : (const void *)m->val16;
-  rc = dispatch_lp(precision, m->rpt[precision], [&](auto strat, auto *vt) {
+  rc = dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
     using St = decltype(strat);
     using VT = std::remove_pointer_t<decltype(vt)>;
-    k_spmv_lp<St, VT><<<c->grid, kBlock, 0, c->stream>>>(c->nrow, c->npad, col, (const VT *)val, d_x, d_y);
+    k_spmv_lp<St, VT><<<c->grid, kBlock, 0, c->stream>>>(c->nrow, c->npad, col, (const VT *)val, d_x, d_y,
+                                                          StencilGeom{c->gx, c->gy, c->gz});
     return (int)cudaGetLastError();
   });
   if (rc) return set_cuda_error((cudaError_t)rc, "spmv_lowp", __FILE__, __LINE__);
@@ -660,7 +673,7 @@ extern "C" int hpccg_gpu_time_mixed_kernels(hpccg_ctx *c, int32_t precision, int
       if (which == 0) {
         k_mp_update_p<<<c->grid, kBlock, 0, c->stream>>>(g);
       } else if (which == 1) {
-        dispatch_lp(precision, m->rpt[precision], [&](auto strat, auto *vt) {
+        dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
           using St = decltype(strat);
           using VT = std::remove_pointer_t<decltype(vt)>;
           k_mp_spmv_dot<St, VT><<<c->grid, kBlock, 0, c->stream>>>(g);

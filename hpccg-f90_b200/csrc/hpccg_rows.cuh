@@ -14,8 +14,11 @@
 //    keeps x.
 //  * csr_vector_rows<LPR>: LPR lanes per CSR row (LPR = 32 is warp-per-row),
 //    lane-strided loads, butterfly shuffle reduction.  Reassociates the sum.
+//  * stencil_rows (hpccg_stencil.cuh): matrix-free, for a context whose CSR
+//    was checked equal to generate_matrix(nx,ny,nz); bit-identical to ELL.
 #pragma once
 #include "hpccg_internal.cuh"
+#include "hpccg_stencil.cuh"
 
 namespace hpccg {
 
@@ -148,11 +151,12 @@ struct EpiResidual {  // r = 1*b + (-1)*(A x), contribution r_i^2
 
 // Arguments every row strategy may need.
 struct SpmvArgs {
-  int kind;   // HPCCG_SPMV_ELL / ELL2 / CSR_VECTOR
+  int kind;   // HPCCG_SPMV_ELL / ELL2 / CSR_VECTOR / STENCIL
   int param;  // lanes per row for CSR_VECTOR
   int n, npad, W;
   const int32_t *rowptr, *col, *ell_col;
   const double *val, *ell_val;
+  StencilGeom geom;  // grid of generate_matrix (STENCIL only)
 };
 
 // Strategy tags: each kernel is compiled once per strategy and the host picks
@@ -193,6 +197,14 @@ struct StratCsr {
   }
 };
 
+struct StratStencil {
+  static constexpr int kMinBlocks = 4;
+  template <class Epi>
+  static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
+    return stencil_rows<double>(a.n, a.geom, x, e);
+  }
+};
+
 // Resident-block hints offered for the ELL strategies (the `param` of
 // hpccg_gpu_set_spmv for HPCCG_SPMV_ELL / HPCCG_SPMV_ELL2).
 constexpr int kEllMinBlocks[4] = {2, 3, 4, 8};
@@ -200,6 +212,7 @@ constexpr int kEllMinBlocks[4] = {2, 3, 4, 8};
 // Calls f(Strat{}) with the strategy the arguments select (host side).
 template <class F>
 inline int dispatch_strategy(const SpmvArgs &a, F &&f) {
+  if (a.kind == HPCCG_SPMV_STENCIL) return f(StratStencil{});
   if (a.kind == HPCCG_SPMV_CSR_VECTOR) {
     switch (a.param) {
       case 4: return f(StratCsr<4>{});
@@ -229,7 +242,8 @@ inline SpmvArgs spmv_args(const hpccg_ctx *c) {
   SpmvArgs a;
   a.kind = c->spmv_kind == HPCCG_SPMV_AUTO ? HPCCG_SPMV_ELL : c->spmv_kind;
   a.param = c->spmv_kind == HPCCG_SPMV_AUTO ? 4 : c->spmv_param;
-  if (!c->d_ell_col && a.kind != HPCCG_SPMV_CSR_VECTOR) {
+  if (a.kind == HPCCG_SPMV_STENCIL && !c->gx) a.kind = HPCCG_SPMV_ELL;
+  if (!c->d_ell_col && a.kind != HPCCG_SPMV_CSR_VECTOR && a.kind != HPCCG_SPMV_STENCIL) {
     a.kind = HPCCG_SPMV_CSR_VECTOR;
     a.param = 32;
   }
@@ -241,6 +255,7 @@ inline SpmvArgs spmv_args(const hpccg_ctx *c) {
   a.val = c->d_val;
   a.ell_col = c->d_ell_col;
   a.ell_val = c->d_ell_val;
+  a.geom = StencilGeom{c->gx, c->gy, c->gz};
   return a;
 }
 

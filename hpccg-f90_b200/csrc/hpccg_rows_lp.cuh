@@ -5,6 +5,7 @@
 // 32*RPT*sizeof(value) load plus a 32*RPT*4-byte column-index load.
 #pragma once
 #include "hpccg_internal.cuh"
+#include "hpccg_stencil.cuh"
 
 namespace hpccg {
 
@@ -112,8 +113,19 @@ struct StratLp {
   static constexpr int kMinBlocks = MINB;
   template <class Epi>
   static __device__ __forceinline__ double rows(int n, int npad, const int32_t *col, const VT *val,
-                                                const float *x, Epi &e) {
+                                                const float *x, Epi &e, const StencilGeom &) {
     return ell_rows_lp<VT, RPT, 27>(n, npad, col, val, x, e);
+  }
+};
+
+// Matrix-free FP32 rows of the generate_matrix operator (its values 27 and -1
+// are exact in FP32 and BF16 alike, so one kernel serves both precisions).
+struct StratLpStencil {
+  static constexpr int kMinBlocks = 4;
+  template <class Epi>
+  static __device__ __forceinline__ double rows(int n, int, const int32_t *, const float *, const float *x,
+                                                Epi &e, const StencilGeom &g) {
+    return stencil_rows<float>(n, g, x, e);
   }
 };
 

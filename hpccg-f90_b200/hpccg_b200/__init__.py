@@ -30,7 +30,7 @@ HPCCG_ERR_UNSUPPORTED = 7
 HPCCG_ERR_NO_DEVICE = 8
 HPCCG_ERR_TOO_LARGE = 9
 
-SPMV_AUTO, SPMV_ELL, SPMV_ELL2, SPMV_CSR_VECTOR = 0, 1, 2, 3
+SPMV_AUTO, SPMV_ELL, SPMV_ELL2, SPMV_CSR_VECTOR, SPMV_STENCIL = 0, 1, 2, 3, 4
 PREC_FP64, PREC_FP32, PREC_BF16 = 0, 1, 2
 
 
@@ -68,6 +68,7 @@ _SIGS = {
     "hpccg_gpu_info": (_c.c_int, [_vp, _c.POINTER(_i32), _c.POINTER(_i64), _c.POINTER(_i32)]),
     "hpccg_gpu_download_csr": (_c.c_int, [_vp, _i32p, _i32p, _f64p]),
     "hpccg_gpu_set_spmv": (_c.c_int, [_vp, _i32, _i32]),
+    "hpccg_gpu_set_geometry": (_c.c_int, [_vp, _i32, _i32, _i32]),
     "hpccg_gpu_get_spmv": (_c.c_int, [_vp, _c.POINTER(_i32), _c.POINTER(_i32)]),
     "hpccg_gpu_cg": (_c.c_int, [_vp, _f64p, _f64p, _i32, _f64, _c.POINTER(_i32), _c.POINTER(_f64), _vp]),
     "hpccg_gpu_cg_device": (_c.c_int, [_vp, _vp, _vp, _i32, _f64, _c.POINTER(_i32), _c.POINTER(_f64), _vp]),
@@ -225,6 +226,11 @@ class Matrix:
         return rowindex, colindex, values
 
     # -- kernel selection --
+    def set_geometry(self, nx: int, ny: int, nz: int):
+        """Check on the device that A is generate_matrix(nx,ny,nz); enables SPMV_STENCIL.
+        Raises HpccgError (HPCCG_ERR_UNSUPPORTED) when the matrix differs."""
+        _check(_lib.hpccg_gpu_set_geometry(self._h, nx, ny, nz), "set_geometry")
+
     def set_spmv(self, kind: int, param: int = 0):
         _check(_lib.hpccg_gpu_set_spmv(self._h, kind, param), "set_spmv")
 

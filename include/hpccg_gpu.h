@@ -76,12 +76,26 @@ int hpccg_gpu_download_csr(const hpccg_ctx *ctx, int32_t *rowindex, int32_t *col
                            double *values);
 
 /* SpMV kernel selection.  HPCCG_SPMV_AUTO picks the fastest bit-exact FP64
- * kernel on first use; the others force one kernel. */
+ * ELL kernel on first use (never the matrix-free stencil, which is opt-in);
+ * the others force one kernel. */
 #define HPCCG_SPMV_AUTO 0
 #define HPCCG_SPMV_ELL 1        /* thread per row, column-major ELL (param: resident blocks/SM hint 2,3,4,8) */
 #define HPCCG_SPMV_ELL2 2       /* two rows per thread, 16-byte loads (same param)  */
 #define HPCCG_SPMV_CSR_VECTOR 3 /* warp-per-row CSR (lanes per row = param)    */
+#define HPCCG_SPMV_STENCIL 4    /* matrix-free generate_matrix stencil (needs the geometry below) */
 int hpccg_gpu_set_spmv(hpccg_ctx *ctx, int32_t kind, int32_t param);
+
+/* Declares that the context's matrix is generate_matrix(nx,ny,nz)
+ * (MPI/src/SparseMatrix.F90:68-185) and checks that on the device, entry by
+ * entry: row pointers, column indices in order, and values (27.0 on the
+ * diagonal, -1.0 elsewhere).  On success the matrix-free SpMV
+ * HPCCG_SPMV_STENCIL may be selected: it forms every row sum from x alone, in
+ * the CSR's term order, so y, fused dots and CG histories are bit-identical
+ * to the ELL kernels' while A is never read.  Returns HPCCG_ERR_UNSUPPORTED
+ * when the matrix differs (the geometry is then cleared) and
+ * HPCCG_ERR_INVALID_ARG when nx*ny*nz is not the row count.  Contexts from
+ * hpccg_gpu_create_generated are checked and have the geometry already. */
+int hpccg_gpu_set_geometry(hpccg_ctx *ctx, int32_t nx, int32_t ny, int32_t nz);
 int hpccg_gpu_get_spmv(const hpccg_ctx *ctx, int32_t *kind, int32_t *param);
 
 /* ---- the CG entry point ------------------------------------------------- */

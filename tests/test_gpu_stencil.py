@@ -1,0 +1,146 @@
+"""Matrix-free SpMV (HPCCG_SPMV_STENCIL) against the CSR it replaces.
+
+Bars: the device check accepts exactly the generate_matrix CSR (any changed
+column, value or row length is rejected); the stencil SpMV is bit-identical
+to the ELL SpMV and to the oracle's spmv; a whole FP64 CG run (x, iteration
+count and residual history) is bit-identical to the ELL run; the FP32
+matrix-free inner solve of the iterative refinement meets the FP64 target.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(1, 1, 1), (2, 1, 1), (1, 2, 3), (2, 2, 2), (3, 5, 7), (7, 1, 3), (9, 2, 11), (33, 17, 5),
+         (16, 16, 16), (64, 64, 64), (128, 4, 2)]
+
+
+@pytest.fixture(scope="module")
+def hp():
+    import hpccg_b200
+    return hpccg_b200
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    assert t.cuda.is_available()
+    return t
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float64).view(np.int64)
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES)
+def test_stencil_spmv_bit_identical(hp, torch, nx, ny, nz):
+    A, x, b, xe = oracle.generate_matrix(nx, ny, nz)
+    n = nx * ny * nz
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    with pytest.raises(hp.HpccgError):
+        M.set_spmv(hp.SPMV_STENCIL)  # geometry not declared yet
+    M.set_geometry(nx, ny, nz)
+    rng = np.random.default_rng(nx * 10007 + ny * 101 + nz)
+    xv = rng.uniform(-1, 1, n) * np.exp2(rng.integers(-20, 20, n))
+    want = oracle.spmv(A, xv)
+    dx = torch.from_numpy(xv).cuda()
+    y_ell = torch.empty_like(dx)
+    y_st = torch.empty_like(dx)
+    M.set_spmv(hp.SPMV_ELL, 4)
+    M.spmv(dx, y_ell)
+    M.set_spmv(hp.SPMV_STENCIL)
+    assert M.get_spmv()[0] == hp.SPMV_STENCIL
+    M.spmv(dx, y_st)
+    assert np.array_equal(_bits(y_st.cpu().numpy()), _bits(y_ell.cpu().numpy()))
+    assert np.array_equal(_bits(y_st.cpu().numpy()), _bits(want))
+    G = hp.Matrix.generated(nx, ny, nz)  # generated contexts are checked at creation
+    G.set_spmv(hp.SPMV_STENCIL)
+    y_g = torch.empty_like(dx)
+    G.spmv(dx, y_g)
+    assert np.array_equal(_bits(y_g.cpu().numpy()), _bits(want))
+
+
+def test_stencil_check_rejects_other_matrices(hp):
+    nx, ny, nz = 6, 5, 4
+    A, x, b, xe = oracle.generate_matrix(nx, ny, nz)
+    with pytest.raises(hp.HpccgError) as e:
+        hp.Matrix.from_csr(A.rowindex, A.colindex, A.values).set_geometry(nx, ny, nz + 1)
+    assert e.value.code == hp.HPCCG_ERR_INVALID_ARG
+    with pytest.raises(hp.HpccgError) as e:  # same row count, other shape
+        hp.Matrix.from_csr(A.rowindex, A.colindex, A.values).set_geometry(nz, ny, nx)
+    assert e.value.code == hp.HPCCG_ERR_UNSUPPORTED
+    v = A.values.copy()
+    v[37] = -2.0
+    with pytest.raises(hp.HpccgError) as e:
+        hp.Matrix.from_csr(A.rowindex, A.colindex, v).set_geometry(nx, ny, nz)
+    assert e.value.code == hp.HPCCG_ERR_UNSUPPORTED
+    # a row with its last term dropped (row pointers shifted after it)
+    r = A.rowindex.copy()
+    c = np.delete(A.colindex, r[11] - 2)
+    vv = np.delete(A.values, r[11] - 2)
+    r[11:] -= 1
+    M = hp.Matrix.from_csr(r, c, vv)
+    with pytest.raises(hp.HpccgError) as e:
+        M.set_geometry(nx, ny, nz)
+    assert e.value.code == hp.HPCCG_ERR_UNSUPPORTED
+    with pytest.raises(hp.HpccgError):
+        M.set_spmv(hp.SPMV_STENCIL)
+
+
+@pytest.mark.parametrize("key", ["32x32x32", "3x5x7", "17x9x6"])
+def test_stencil_cg_bit_identical_to_ell(hp, key):
+    nx, ny, nz = map(int, key.split("x"))
+    A, x, b, xe = oracle.generate_matrix(nx, ny, nz)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    M.set_geometry(nx, ny, nz)
+    M.set_spmv(hp.SPMV_ELL, 4)
+    x1, it1, nr1, h1, s1 = M.cg(b, x.copy(), 150, 0.0)
+    M.set_spmv(hp.SPMV_STENCIL)
+    x2, it2, nr2, h2, s2 = M.cg(b, x.copy(), 150, 0.0)
+    assert (it1, s1) == (it2, s2)
+    assert np.array_equal(_bits(x1), _bits(x2)) and np.array_equal(_bits(h1), _bits(h2))
+    assert _bits(np.array([nr1]))[0] == _bits(np.array([nr2]))[0]
+    assert np.abs(x2 - 1.0).max() <= 1e-10
+
+
+def test_stencil_cg_128_matches_ell(hp, torch):
+    n = 128
+    dx = torch.zeros(n ** 3, dtype=torch.float64, device="cuda")
+    db = torch.zeros_like(dx)
+    M = hp.Matrix.generated(n, n, n, dx, db, None)
+    M.set_spmv(hp.SPMV_ELL, 4)
+    it1, nr1, h1, s1 = M.cg_device(db, dx, 120, 0.0)
+    x1 = dx.cpu().numpy()
+    dx.zero_()
+    M.set_spmv(hp.SPMV_STENCIL)
+    it2, nr2, h2, s2 = M.cg_device(db, dx, 120, 0.0)
+    assert (it1, s1) == (it2, s2) == (120, hp.HPCCG_OK)
+    assert np.array_equal(_bits(h1), _bits(h2)) and np.array_equal(_bits(x1), _bits(dx.cpu().numpy()))
+
+
+@pytest.mark.parametrize("precision", [1, 2])
+def test_stencil_mixed_refinement(hp, torch, precision):
+    n = 48
+    dx = torch.zeros(n ** 3, dtype=torch.float64, device="cuda")
+    db = torch.zeros_like(dx)
+    M = hp.Matrix.generated(n, n, n)
+    xs = torch.empty_like(dx)
+    M.uniform_pm1(1234, xs)
+    M.spmv(xs, db)
+    M.set_spmv(hp.SPMV_STENCIL)
+    info, rc = M.solve_mixed_device(db, dx, precision, rel_tol=1e-8)
+    assert rc == hp.HPCCG_OK and info.relres <= 1e-8
+    r = torch.empty_like(dx)
+    M.set_spmv(hp.SPMV_ELL, 4)
+    M.spmv(dx, r)
+    true_rel = float(torch.linalg.vector_norm(db - r) / torch.linalg.vector_norm(db))
+    assert true_rel <= 1e-8
+    assert float((dx - xs).abs().max()) <= 1e-6
+    y32 = torch.empty(n ** 3, dtype=torch.float32, device="cuda")
+    M.set_spmv(hp.SPMV_STENCIL)
+    M.spmv_lowp(precision, xs.float(), y32)
+    ref = torch.empty_like(dx)
+    M.spmv(xs.float().double(), ref)
+    assert float((y32.double() - ref).abs().max()) <= 1e-5 * float(ref.abs().max())
