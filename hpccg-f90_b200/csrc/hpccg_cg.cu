@@ -214,7 +214,7 @@ static CgArgs cg_args(hpccg_ctx *c, cudaGraphConditionalHandle h, int use_cond) 
 static int launch_prepare(hpccg_ctx *c, const SpmvArgs &a, const CgArgs &g, cudaStream_t s) {
   return dispatch_strategy(a, [&](auto strat) {
     using St = decltype(strat);
-    k_cg_residual<St><<<c->grid, kBlock, 0, s>>>(a, g);
+    k_cg_residual<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, g);
     return (int)cudaGetLastError();
   });
 }
@@ -223,7 +223,7 @@ static int launch_body(hpccg_ctx *c, const SpmvArgs &a, const CgArgs &g, cudaStr
   k_cg_update_p<<<c->grid, kBlock, 0, s>>>(g);
   int rc = dispatch_strategy(a, [&](auto strat) {
     using St = decltype(strat);
-    k_cg_spmv_dot<St><<<c->grid, kBlock, 0, s>>>(a, g);
+    k_cg_spmv_dot<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, g);
     return (int)cudaGetLastError();
   });
   if (rc) return rc;
@@ -235,7 +235,7 @@ int launch_spmv(hpccg_ctx *c, const double *x, double *y, cudaStream_t s) {
   const SpmvArgs a = spmv_args(c);
   return dispatch_strategy(a, [&](auto strat) {
     using St = decltype(strat);
-    k_spmv<St><<<c->grid, kBlock, 0, s>>>(a, x, y);
+    k_spmv<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, x, y);
     return (int)cudaGetLastError();
   });
 }
@@ -522,7 +522,7 @@ extern "C" int hpccg_gpu_time_cg_kernels(hpccg_ctx *c, int32_t reps, float *ms) 
       } else if (which == 1) {
         rc = dispatch_strategy(a, [&](auto strat) {
           using St = decltype(strat);
-          k_cg_spmv_dot<St><<<c->grid, kBlock, 0, c->stream>>>(a, g);
+          k_cg_spmv_dot<St><<<St::grid(a, c->grid), kBlock, 0, c->stream>>>(a, g);
           return 0;
         });
       } else {

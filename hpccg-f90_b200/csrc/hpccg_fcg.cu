@@ -198,7 +198,7 @@ extern "C" int hpccg_gpu_solve_fcg(hpccg_ctx *c, hpccg_unet *u, int32_t nx, int3
   auto residual = [&]() -> int {
     return dispatch_strategy(a, [&](auto strat) {
       using St = decltype(strat);
-      k_fcg_residual<St><<<c->grid, kBlock, 0, s>>>(a, g);
+      k_fcg_residual<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, g);
       return (int)cudaGetLastError();
     });
   };
@@ -253,7 +253,7 @@ extern "C" int hpccg_gpu_solve_fcg(hpccg_ctx *c, hpccg_unet *u, int32_t nx, int3
     restart = false;
     rc = dispatch_strategy(a, [&](auto strat) {
       using St = decltype(strat);
-      k_fcg_spmv_dot<St><<<c->grid, kBlock, 0, s>>>(a, g);
+      k_fcg_spmv_dot<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, g);
       return (int)cudaGetLastError();
     });
     if (rc) break;

@@ -38,6 +38,7 @@ struct MixedArgs {
   MixedState *st;
   Reduction red;
   StencilGeom geom;  // matrix-free inner SpMV when the context uses the stencil
+  PlaneMap pm;
   cudaGraphConditionalHandle cond_outer, cond_inner;
   int use_cond;
 };
@@ -172,6 +173,11 @@ struct EpiDot32 {
     y[i] = s;
     return (double)__ldg(p + i) * (double)s;
   }
+  // pi = p[i], already at hand in the matrix-free walk
+  __device__ __forceinline__ double operator()(int i, float s, float pi) const {
+    y[i] = s;
+    return (double)pi * (double)s;
+  }
 };
 
 // Ap = A p with low-precision values, alpha = rtrans / p.Ap.
@@ -179,7 +185,7 @@ template <class S, typename VT>
 __global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_spmv_dot(MixedArgs g) {
   __shared__ double smem[32];
   EpiDot32 epi{g.p, g.Ap};
-  const double part = S::rows(g.n, g.npad, g.ell_col, reinterpret_cast<const VT *>(g.val_lp), g.p, epi, g.geom);
+  const double part = S::rows(g.n, g.npad, g.ell_col, reinterpret_cast<const VT *>(g.val_lp), g.p, epi, g.geom, g.pm);
   const double tot = block_sum<kBlock>(part, smem);
   if (arrive_last(g.red, tot)) {
     const double pAp = finish_sum<kBlock>(g.red, smem);
@@ -256,7 +262,7 @@ __global__ void __launch_bounds__(kBlock) k_mp_end_inner(MixedArgs g) {
 // Plain low-precision y = A x for tests and timing.
 struct EpiStore32 {
   float *y;
-  __device__ __forceinline__ double operator()(int i, float s) const {
+  __device__ __forceinline__ double operator()(int i, float s, float = 0.f) const {
     y[i] = s;
     return 0.0;
   }
@@ -264,9 +270,9 @@ struct EpiStore32 {
 template <class S, typename VT>
 __global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_spmv_lp(int n, int npad, const int32_t *col,
                                                                    const VT *val, const float *x, float *y,
-                                                                   StencilGeom geom) {
+                                                                   StencilGeom geom, PlaneMap pm) {
   EpiStore32 epi{y};
-  S::rows(n, npad, col, val, x, epi, geom);
+  S::rows(n, npad, col, val, x, epi, geom, pm);
 }
 
 __global__ void k_to_lp(const double *src, float *f32, __nv_bfloat16 *b16, size_t count) {
@@ -406,6 +412,7 @@ static MixedArgs mixed_args(hpccg_ctx *c, MixedRes *m, int precision) {
   g.st = m->st;
   g.red = reduction_of(c);
   g.geom = StencilGeom{c->gx, c->gy, c->gz};
+  g.pm = spmv_args(c).pm;
   return g;
 }
 
@@ -414,7 +421,7 @@ static int launch_inner_body(hpccg_ctx *c, MixedRes *m, int precision, const Mix
   int rc = dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
     using St = decltype(strat);
     using VT = std::remove_pointer_t<decltype(vt)>;
-    k_mp_spmv_dot<St, VT><<<c->grid, kBlock, 0, s>>>(g);
+    k_mp_spmv_dot<St, VT><<<St::grid(g.pm, c->grid), kBlock, 0, s>>>(g);
     return (int)cudaGetLastError();
   });
   if (rc) return rc;
@@ -426,7 +433,7 @@ static int launch_residual64(hpccg_ctx *c, const MixedArgs &g, cudaStream_t s) {
   const SpmvArgs a = spmv_args(c);
   return dispatch_strategy(a, [&](auto strat) {
     using St = decltype(strat);
-    k_mp_residual64<St><<<c->grid, kBlock, 0, s>>>(a, g);
+    k_mp_residual64<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, g);
     return (int)cudaGetLastError();
   });
 }
@@ -637,8 +644,9 @@ extern "C" int hpccg_gpu_spmv_lowp(hpccg_ctx *c, int32_t precision, const float 
   rc = dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
     using St = decltype(strat);
     using VT = std::remove_pointer_t<decltype(vt)>;
-    k_spmv_lp<St, VT><<<c->grid, kBlock, 0, c->stream>>>(c->nrow, c->npad, col, (const VT *)val, d_x, d_y,
-                                                          StencilGeom{c->gx, c->gy, c->gz});
+    const PlaneMap pm = spmv_args(c).pm;
+    k_spmv_lp<St, VT><<<St::grid(pm, c->grid), kBlock, 0, c->stream>>>(c->nrow, c->npad, col, (const VT *)val, d_x,
+                                                                        d_y, StencilGeom{c->gx, c->gy, c->gz}, pm);
     return (int)cudaGetLastError();
   });
   if (rc) return set_cuda_error((cudaError_t)rc, "spmv_lowp", __FILE__, __LINE__);
@@ -676,7 +684,7 @@ extern "C" int hpccg_gpu_time_mixed_kernels(hpccg_ctx *c, int32_t precision, int
         dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
           using St = decltype(strat);
           using VT = std::remove_pointer_t<decltype(vt)>;
-          k_mp_spmv_dot<St, VT><<<c->grid, kBlock, 0, c->stream>>>(g);
+          k_mp_spmv_dot<St, VT><<<St::grid(g.pm, c->grid), kBlock, 0, c->stream>>>(g);
           return 0;
         });
       } else {

@@ -15,7 +15,8 @@
 //  * csr_vector_rows<LPR>: LPR lanes per CSR row (LPR = 32 is warp-per-row),
 //    lane-strided loads, butterfly shuffle reduction.  Reassociates the sum.
 //  * stencil_rows (hpccg_stencil.cuh): matrix-free, for a context whose CSR
-//    was checked equal to generate_matrix(nx,ny,nz); bit-identical to ELL.
+//    was checked equal to generate_matrix(nx,ny,nz); bit-identical to ELL
+//    (both follow the same plane map of rows to threads).
 #pragma once
 #include "hpccg_internal.cuh"
 #include "hpccg_stencil.cuh"
@@ -26,15 +27,27 @@ __device__ __forceinline__ double mul_add(double s, double v, double x) {
   return __dadd_rn(s, __dmul_rn(v, x));  // no contraction: reference rounding
 }
 
+// Calls body(i) for the calling thread's rows, in order: the plane map when
+// it is in use (hpccg_stencil.cuh), else grid-stride rows.
+template <class Body>
+__device__ __forceinline__ void thread_rows(int n, const PlaneMap &m, Body &&body) {
+  if (m.plane > 0) {
+    const PlaneSpan sp = plane_span(m, n / m.plane);
+    for (int z = sp.z0; z < sp.z1; ++z) body(sp.c + z * m.plane);
+    return;
+  }
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) body(i);
+}
+
 template <int W, int RPT, int U, class Epi>
 __device__ __forceinline__ double ell_rows(int n, int npad, const int32_t *__restrict__ col,
                                            const double *__restrict__ val,
-                                           const double *__restrict__ x, Epi &epi) {
+                                           const double *__restrict__ x, Epi &epi, const PlaneMap &m) {
   static_assert(W % U == 0, "slot chunk must divide the ELL width");
   double part = 0.0;
-  const int stride = gridDim.x * blockDim.x;
   if constexpr (RPT == 1) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    thread_rows(n, m, [&](int i) {
       double s = 0.0;
 #pragma unroll
       for (int k0 = 0; k0 < W; k0 += U) {
@@ -49,8 +62,9 @@ __device__ __forceinline__ double ell_rows(int n, int npad, const int32_t *__res
         for (int k = 0; k < U; ++k) s = mul_add(s, v[k], __ldg(x + c[k]));
       }
       part = __dadd_rn(part, epi(i, s));
-    }
+    });
   } else {
+    const int stride = gridDim.x * blockDim.x;
     const int half = npad >> 1;
     const int npairs = (n + 1) >> 1;
     const int2 *col2 = reinterpret_cast<const int2 *>(col);
@@ -85,16 +99,15 @@ template <class Epi>
 __device__ __forceinline__ double ell_rows_dyn(int n, int npad, int W,
                                                const int32_t *__restrict__ col,
                                                const double *__restrict__ val,
-                                               const double *__restrict__ x, Epi &epi) {
+                                               const double *__restrict__ x, Epi &epi, const PlaneMap &m) {
   double part = 0.0;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  thread_rows(n, m, [&](int i) {
     double s = 0.0;
 #pragma unroll 4
     for (int k = 0; k < W; ++k)
       s = mul_add(s, __ldcs(val + (size_t)k * npad + i), __ldg(x + __ldcs(col + (size_t)k * npad + i)));
     part = __dadd_rn(part, epi(i, s));
-  }
+  });
   return part;
 }
 
@@ -157,40 +170,50 @@ struct SpmvArgs {
   const int32_t *rowptr, *col, *ell_col;
   const double *val, *ell_val;
   StencilGeom geom;  // grid of generate_matrix (STENCIL only)
+  PlaneMap pm;       // row map of ELL (one row per thread) and STENCIL when the grid is known
 };
+
+// Launch grid of a strategy that follows the plane map when it is in use.
+inline int plane_or(const PlaneMap &m, int dflt) { return m.plane > 0 ? plane_grid(m) : dflt; }
 
 // Strategy tags: each kernel is compiled once per strategy and the host picks
 // the instantiation.  kMinBlocks feeds __launch_bounds__: with 2 resident
 // blocks per SM ptxas keeps all 27 slot loads of a row in flight (~120
 // registers); with 8 it interleaves loads and gathers at 32 registers and
 // relies on occupancy instead.  Strategies with the same RPT map rows to
-// threads identically, so they give bit-identical results (fused dots too).
+// threads identically, so they give bit-identical results (fused dots too);
+// one row per thread (ELL, STENCIL) follows the plane map when the grid of
+// the matrix is known.
 template <int MINB>
 struct StratEll1 {
   static constexpr int kMinBlocks = MINB;
+  static int grid(const SpmvArgs &a, int dflt) { return plane_or(a.pm, dflt); }
   template <class Epi>
   static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
-    return ell_rows<27, 1, 27>(a.n, a.npad, a.ell_col, a.ell_val, x, e);
+    return ell_rows<27, 1, 27>(a.n, a.npad, a.ell_col, a.ell_val, x, e, a.pm);
   }
 };
 template <int MINB>
 struct StratEll2 {
   static constexpr int kMinBlocks = MINB;
+  static int grid(const SpmvArgs &, int dflt) { return dflt; }
   template <class Epi>
   static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
-    return ell_rows<27, 2, 9>(a.n, a.npad, a.ell_col, a.ell_val, x, e);
+    return ell_rows<27, 2, 9>(a.n, a.npad, a.ell_col, a.ell_val, x, e, a.pm);
   }
 };
 struct StratEllDyn {
   static constexpr int kMinBlocks = 4;
+  static int grid(const SpmvArgs &a, int dflt) { return plane_or(a.pm, dflt); }
   template <class Epi>
   static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
-    return ell_rows_dyn(a.n, a.npad, a.W, a.ell_col, a.ell_val, x, e);
+    return ell_rows_dyn(a.n, a.npad, a.W, a.ell_col, a.ell_val, x, e, a.pm);
   }
 };
 template <int LPR>
 struct StratCsr {
   static constexpr int kMinBlocks = 4;
+  static int grid(const SpmvArgs &, int dflt) { return dflt; }
   template <class Epi>
   static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
     return csr_vector_rows<LPR>(a.n, a.rowptr, a.col, a.val, x, e);
@@ -198,10 +221,11 @@ struct StratCsr {
 };
 
 struct StratStencil {
-  static constexpr int kMinBlocks = 4;
+  static constexpr int kMinBlocks = 2;  // the FP64 3-plane window needs ~80 registers
+  static int grid(const SpmvArgs &a, int dflt) { return plane_or(a.pm, dflt); }
   template <class Epi>
   static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
-    return stencil_rows<double>(a.n, a.geom, x, e);
+    return stencil_rows<double>(a.n, a.geom, a.pm, x, e);
   }
 };
 
@@ -256,6 +280,7 @@ inline SpmvArgs spmv_args(const hpccg_ctx *c) {
   a.ell_col = c->d_ell_col;
   a.ell_val = c->d_ell_val;
   a.geom = StencilGeom{c->gx, c->gy, c->gz};
+  a.pm = c->gx ? plane_map(c->gx, c->gy, c->gz, kMaxPartials) : PlaneMap{0, 0, 0};
   return a;
 }
 

@@ -9,9 +9,16 @@
 // __dmul_rn(27, x(i)) for the diagonal.  A neighbour outside the grid
 // subtracts +0.0, which leaves the sum unchanged: the sum starts at +0.0 and
 // round-to-nearest never produces -0.0 from it.  So the FP64 row sums are
-// bit-identical to the CSR/ELL kernels'.  Rows map to threads exactly as in
-// ell_rows<..., RPT=1> (thread t: rows t, t+stride, ...), so fused dot
-// products, and with them whole CG runs, are bit-identical too.
+// bit-identical to the CSR/ELL kernels'.
+//
+// Row-to-thread map ("plane map", used when the grid is known): thread t
+// owns the grid column c = t mod nx*ny and walks z through one chunk of zc
+// planes, rows c + z*nx*ny for z in [q*zc, min(nz, (q+1)*zc)), q = t div
+// nx*ny.  Consecutive threads own consecutive rows (coalesced), and a thread
+// keeps the 3x3 neighbourhoods of planes z-1, z, z+1 in registers, so each row
+// takes 9 new values instead of 27.  The ELL kernel uses the same map for the
+// same context, so fused dot products -- and whole CG runs -- are
+// bit-identical between the two.
 #pragma once
 #include "hpccg_internal.cuh"
 
@@ -21,6 +28,51 @@ struct StencilGeom {
   int nx, ny, nz;
 };
 
+struct PlaneMap {
+  int plane;  // nx*ny rows per z plane; 0 = map not in use (grid-stride rows)
+  int zc;     // planes per thread
+  int nzc;    // z chunks
+};
+
+// Host: the plane map for a grid, with at most `max_blocks` blocks of kBlock
+// threads (the reduction scratch holds one partial per block).  Chunks of at
+// least 16 planes keep the per-thread start-up (two extra planes) small.
+inline PlaneMap plane_map(int nx, int ny, int nz, int max_blocks) {
+  PlaneMap m{0, 0, 0};
+  if (nx < 1 || ny < 1 || nz < 1) return m;
+  const int64_t plane = (int64_t)nx * ny;
+  for (int zc = 16;; zc *= 2) {
+    const int64_t nzc = (nz + zc - 1) / zc;
+    const int64_t blocks = (plane * nzc + kBlock - 1) / kBlock;
+    if (blocks <= max_blocks / 2 || (zc >= nz && blocks <= max_blocks)) {
+      m.plane = (int)plane;
+      m.zc = zc;
+      m.nzc = (int)nzc;
+      return m;
+    }
+    if (zc >= nz) return m;  // one plane alone needs too many threads
+  }
+}
+inline int plane_grid(const PlaneMap &m) {
+  return (int)(((int64_t)m.plane * m.nzc + kBlock - 1) / kBlock);
+}
+
+// The rows of the calling thread under the map: column c, planes [z0, z1).
+struct PlaneSpan {
+  int c, z0, z1;
+};
+__device__ __forceinline__ PlaneSpan plane_span(const PlaneMap &m, int nz) {
+  PlaneSpan s{0, 0, 0};
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)m.plane * m.nzc) return s;
+  const int q = (int)(t / m.plane);
+  s.c = (int)(t - (int64_t)q * m.plane);
+  s.z0 = q * m.zc;
+  s.z1 = min(nz, s.z0 + m.zc);
+  return s;
+}
+
+// Grid-stride form (any row order): one row from 27 loads.
 template <typename Real>
 __device__ __forceinline__ Real stencil_row(int i, const StencilGeom &g, const Real *__restrict__ x) {
   const int nxy = g.nx * g.ny;
@@ -51,11 +103,127 @@ __device__ __forceinline__ Real stencil_row(int i, const StencilGeom &g, const R
   return s;
 }
 
-// Grid-stride walk over the rows; epi(i, rowsum) stores and returns a dot term.
-template <typename Real, class Epi>
-__device__ __forceinline__ double stencil_rows(int n, const StencilGeom &g, const Real *__restrict__ x,
-                                               Epi &epi) {
+// Bit j = (sy+1)*3 + (sx+1) set when neighbour (sy, sx) of column (ix, iy)
+// lies inside the grid.
+__device__ __forceinline__ unsigned stencil_mask(const StencilGeom &g, int ix, int iy) {
+  unsigned mask = 0;
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    const int yy = iy + j / 3 - 1, xx = ix + j % 3 - 1;
+    if ((unsigned)yy < (unsigned)g.ny && (unsigned)xx < (unsigned)g.nx) mask |= 1u << j;
+  }
+  return mask;
+}
+
+// Loads the 3x3 neighbourhood (sy, sx order) of the thread's column in the
+// plane that `p` points into (p = &x[column + z*plane]); `mask` bit j clear
+// (or zin false) gives 0 for neighbour j, which lies outside the grid.
+template <typename Real>
+__device__ __forceinline__ void stencil_plane(const Real *__restrict__ p, int nx, unsigned mask, bool zin, Real *v) {
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    const int off = (j / 3 - 1) * nx + (j % 3 - 1);
+    v[j] = (zin && ((mask >> j) & 1u)) ? __ldg(p + off) : Real(0);
+  }
+}
+
+// Row sum from the three planes' neighbourhoods, in the reference's order.
+template <typename Real>
+__device__ __forceinline__ Real stencil_sum(const Real *a, const Real *b, const Real *c) {
+  Real s = Real(0);
+  if constexpr (sizeof(Real) == 8) {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s = __dsub_rn(s, a[j]);
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s = j == 4 ? __dadd_rn(s, __dmul_rn(27.0, b[j])) : __dsub_rn(s, b[j]);
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s = __dsub_rn(s, c[j]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s -= a[j];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s = j == 4 ? fmaf(27.f, b[j], s) : s - b[j];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s -= c[j];
+  }
+  return s;
+}
+
+// FP32 rows of the plane-map walk from 3x3 box sums: y_i = 28 x_i - (sum of
+// the 27 values of the 3x3x3 neighbourhood, self included), the box sum of
+// each plane formed once and used by the three rows that need it.  This
+// reassociates the row sum (for the low-precision inner solves only).  Loads
+// are unconditional from clamped addresses and weighted by 0/1 instead of
+// predicated (exact: 0*v = 0 for the finite vectors of a solve).
+template <class Epi>
+__device__ __forceinline__ double stencil_rows_box(const StencilGeom &g, const PlaneMap &m,
+                                                   const float *__restrict__ x, Epi &epi) {
   double part = 0.0;
+  const PlaneSpan sp = plane_span(m, g.nz);
+  if (sp.z0 >= sp.z1) return part;
+  const int iy = sp.c / g.nx, ix = sp.c - iy * g.nx;
+  const int dl = ix > 0 ? -1 : 0, dr = ix < g.nx - 1 ? 1 : 0;
+  const float wl = (float)(-dl), wr = (float)dr;
+  const int ylo = iy > 0 ? -g.nx : 0, yhi = iy < g.ny - 1 ? g.nx : 0;
+  const float wlo = iy > 0 ? 1.f : 0.f, whi = iy < g.ny - 1 ? 1.f : 0.f;
+  const float *pc = x + sp.c;
+  // box sum of plane z (zero outside [0, nz)); center = x of the column
+  auto box = [&](int z, float &center) {
+    const bool zin = (unsigned)z < (unsigned)g.nz;
+    const float *p = pc + (int64_t)(zin ? z : 0) * m.plane;
+    const float *q0 = p + ylo, *q2 = p + yhi;
+    const float c1 = __ldg(p);
+    float t1 = fmaf(wl, __ldg(p + dl), c1);
+    t1 = fmaf(wr, __ldg(p + dr), t1);
+    float t0 = fmaf(wl, __ldg(q0 + dl), __ldg(q0));
+    t0 = fmaf(wr, __ldg(q0 + dr), t0);
+    float t2 = fmaf(wl, __ldg(q2 + dl), __ldg(q2));
+    t2 = fmaf(wr, __ldg(q2 + dr), t2);
+    const float s = fmaf(wlo, t0, fmaf(whi, t2, t1));
+    center = c1;
+    return zin ? s : 0.f;
+  };
+  float xc, xn, unused;
+  float bm = box(sp.z0 - 1, unused), b0 = box(sp.z0, xc);
+  for (int z = sp.z0; z < sp.z1; ++z) {
+    const float bp = box(z + 1, xn);
+    part += epi(sp.c + z * m.plane, fmaf(28.f, xc, -((bm + b0) + bp)), xc);
+    bm = b0;
+    b0 = bp;
+    xc = xn;
+  }
+  return part;
+}
+
+// All rows of the calling thread; epi(i, rowsum) stores and returns a dot term.
+template <typename Real, class Epi>
+__device__ __forceinline__ double stencil_rows(int n, const StencilGeom &g, const PlaneMap &m,
+                                               const Real *__restrict__ x, Epi &epi) {
+  double part = 0.0;
+  if (m.plane > 0) {
+    const PlaneSpan sp = plane_span(m, g.nz);
+    if (sp.z0 >= sp.z1) return part;
+    const int iy = sp.c / g.nx, ix = sp.c - iy * g.nx;
+    const unsigned mask = stencil_mask(g, ix, iy);
+    const Real *pc = x + sp.c;
+    Real a[9], b[9], c[9];  // planes z-1, z, z+1
+    stencil_plane<Real>(pc + (int64_t)(sp.z0 - 1) * m.plane, g.nx, mask, sp.z0 > 0, a);
+    stencil_plane<Real>(pc + (int64_t)sp.z0 * m.plane, g.nx, mask, true, b);
+    for (int z = sp.z0; z < sp.z1; ++z) {
+      stencil_plane<Real>(pc + (int64_t)(z + 1) * m.plane, g.nx, mask, z + 1 < g.nz, c);
+      const Real s = stencil_sum<Real>(a, b, c);
+      if constexpr (sizeof(Real) == 8)
+        part = __dadd_rn(part, epi(sp.c + z * m.plane, s));
+      else
+        part += epi(sp.c + z * m.plane, s);
+#pragma unroll
+      for (int j = 0; j < 9; ++j) {
+        a[j] = b[j];
+        b[j] = c[j];
+      }
+    }
+    return part;
+  }
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const Real s = stencil_row<Real>(i, g, x);
