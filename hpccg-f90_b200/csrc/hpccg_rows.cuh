@@ -221,7 +221,7 @@ struct StratCsr {
 };
 
 struct StratStencil {
-  static constexpr int kMinBlocks = 2;  // the FP64 3-plane window needs ~80 registers
+  static constexpr int kMinBlocks = 4;
   static int grid(const SpmvArgs &a, int dflt) { return plane_or(a.pm, dflt); }
   template <class Epi>
   static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {

@@ -123,7 +123,7 @@ struct StratLp {
 // are exact in FP32 and BF16 alike, so one kernel serves both precisions);
 // 3x3 box sums along the plane map (stencil_rows_box) when it is in use.
 struct StratLpStencil {
-  static constexpr int kMinBlocks = 4;
+  static constexpr int kMinBlocks = 5;
   static int grid(const PlaneMap &m, int dflt) { return m.plane > 0 ? plane_grid(m) : dflt; }
   template <class Epi>
   static __device__ __forceinline__ double rows(int n, int, const int32_t *, const float *, const float *x,

@@ -15,8 +15,8 @@
 // owns the grid column c = t mod nx*ny and walks z through one chunk of zc
 // planes, rows c + z*nx*ny for z in [q*zc, min(nz, (q+1)*zc)), q = t div
 // nx*ny.  Consecutive threads own consecutive rows (coalesced), and a thread
-// keeps the 3x3 neighbourhoods of planes z-1, z, z+1 in registers, so each row
-// takes 9 new values instead of 27.  The ELL kernel uses the same map for the
+// keeps what it needs of planes z-1, z, z+1 in registers, so each row takes
+// 9 new values instead of 27.  The ELL kernel uses the same map for the
 // same context, so fused dot products -- and whole CG runs -- are
 // bit-identical between the two.
 #pragma once
@@ -127,20 +127,28 @@ __device__ __forceinline__ void stencil_plane(const Real *__restrict__ p, int nx
   }
 }
 
-// Row sum from the three planes' neighbourhoods, in the reference's order.
+// The same sum split at plane boundaries: lead = the first 9 terms (plane
+// z-1) from 0, tail = lead followed by planes z and z+1.
 template <typename Real>
-__device__ __forceinline__ Real stencil_sum(const Real *a, const Real *b, const Real *c) {
+__device__ __forceinline__ Real stencil_lead(const Real *a) {
   Real s = Real(0);
-  if constexpr (sizeof(Real) == 8) {
 #pragma unroll
-    for (int j = 0; j < 9; ++j) s = __dsub_rn(s, a[j]);
+  for (int j = 0; j < 9; ++j) {
+    if constexpr (sizeof(Real) == 8)
+      s = __dsub_rn(s, a[j]);
+    else
+      s -= a[j];
+  }
+  return s;
+}
+template <typename Real>
+__device__ __forceinline__ Real stencil_tail(Real s, const Real *b, const Real *c) {
+  if constexpr (sizeof(Real) == 8) {
 #pragma unroll
     for (int j = 0; j < 9; ++j) s = j == 4 ? __dadd_rn(s, __dmul_rn(27.0, b[j])) : __dsub_rn(s, b[j]);
 #pragma unroll
     for (int j = 0; j < 9; ++j) s = __dsub_rn(s, c[j]);
   } else {
-#pragma unroll
-    for (int j = 0; j < 9; ++j) s -= a[j];
 #pragma unroll
     for (int j = 0; j < 9; ++j) s = j == 4 ? fmaf(27.f, b[j], s) : s - b[j];
 #pragma unroll
@@ -206,21 +214,23 @@ __device__ __forceinline__ double stencil_rows(int n, const StencilGeom &g, cons
     const int iy = sp.c / g.nx, ix = sp.c - iy * g.nx;
     const unsigned mask = stencil_mask(g, ix, iy);
     const Real *pc = x + sp.c;
-    Real a[9], b[9], c[9];  // planes z-1, z, z+1
-    stencil_plane<Real>(pc + (int64_t)(sp.z0 - 1) * m.plane, g.nx, mask, sp.z0 > 0, a);
+    // The row sum starts with the 9 terms of plane z-1 added to 0 in order:
+    // that prefix depends on plane z-1 alone, so it is formed once per plane
+    // (lead) and the window keeps only planes z and z+1 in full.
+    Real b[9], c[9];
+    stencil_plane<Real>(pc + (int64_t)(sp.z0 - 1) * m.plane, g.nx, mask, sp.z0 > 0, c);
+    Real lead = stencil_lead<Real>(c);
     stencil_plane<Real>(pc + (int64_t)sp.z0 * m.plane, g.nx, mask, true, b);
     for (int z = sp.z0; z < sp.z1; ++z) {
       stencil_plane<Real>(pc + (int64_t)(z + 1) * m.plane, g.nx, mask, z + 1 < g.nz, c);
-      const Real s = stencil_sum<Real>(a, b, c);
+      const Real s = stencil_tail<Real>(lead, b, c);
       if constexpr (sizeof(Real) == 8)
         part = __dadd_rn(part, epi(sp.c + z * m.plane, s));
       else
         part += epi(sp.c + z * m.plane, s);
+      lead = stencil_lead<Real>(b);
 #pragma unroll
-      for (int j = 0; j < 9; ++j) {
-        a[j] = b[j];
-        b[j] = c[j];
-      }
+      for (int j = 0; j < 9; ++j) b[j] = c[j];
     }
     return part;
   }
