@@ -142,13 +142,13 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def _traffic_from_profile():
-    """DRAM bytes per launch of the fused SpMV kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "spmv_dot_fp64_256.txt")
+def _traffic_from_profile(name="spmv_dot_fp64_256.txt", key="dram_bytes_per_launch_full_size"):
+    """DRAM bytes per launch of a kernel at full size, from a committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.startswith("dram_bytes_per_launch_full_size:"):
+        if line.startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].split()[0])
             except ValueError:
@@ -299,6 +299,9 @@ def run_ours(args):
                         "preconditioner (BF16 tensor cores)", learned_fcg, STENCIL))
     results = {}
     clk_summary = None
+    if args.methods:
+        keep = set(args.methods.split(",")) | {"fp64_cg", "fp64_cg_stencil"}  # the speed-up baselines
+        methods = [m for m in methods if m[0] in keep]
     for name, desc, fn, kind in methods:
         M.set_spmv(kind)
         for _ in range(args.warmup):
@@ -376,7 +379,8 @@ def run_ours(args):
     alg64 = 12 * nnz + 20 * N + 4
     roof64 = {"bound": "hbm", "kernel": "k_cg_spmv_dot (FP64 SpMV + p.Ap)", "kernel_ms": kms64[1],
               "alg_bytes_per_launch": alg64, "achieved": alg64 / (kms64[1] * 1e-3) / 1e9, "peak": hbm,
-              "unit": "GB/s", "peak_source": peak_kind, "traffic": _traffic_from_profile()}
+              "unit": "GB/s", "peak_source": peak_kind,
+              "traffic": _traffic_from_profile() if n == 256 else None}
     roof64["frac"] = roof64["achieved"] / hbm
     roofs = {"fp64_cg": roof64}
     for name, prec, vb in (("fp32_ir", hp.PREC_FP32, 4), ("bf16_ir", hp.PREC_BF16, 2)):
@@ -393,7 +397,9 @@ def run_ours(args):
     roofs["fp64_cg_stencil"] = {"bound": "hbm", "kernel": "k_cg_spmv_dot<StratStencil> (matrix-free FP64 SpMV + p.Ap)",
                                 "kernel_ms": kst[1], "alg_bytes_per_launch": alg,
                                 "achieved": alg / (kst[1] * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
-                                "peak_source": peak_kind, "traffic": None, "iteration_ms": sum(kst)}
+                                "peak_source": peak_kind,
+                                "traffic": _traffic_from_profile("stencil_spmv_256.txt") if n == 256 else None,
+                                "iteration_ms": sum(kst)}
     roofs["fp64_cg_stencil"]["frac"] = roofs["fp64_cg_stencil"]["achieved"] / hbm
     km = M.time_mixed_kernels(hp.PREC_FP32, 20)
     alg = 8 * N + 4
@@ -401,7 +407,11 @@ def run_ours(args):
                                 "kernel": "k_mp_spmv_dot<StratLpStencil> (matrix-free FP32 SpMV + p.Ap)",
                                 "kernel_ms": km[1], "alg_bytes_per_launch": alg,
                                 "achieved": alg / (km[1] * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
-                                "peak_source": peak_kind, "traffic": None, "inner_iteration_ms": sum(km)}
+                                "peak_source": peak_kind,
+                                "traffic": _traffic_from_profile("stencil_spmv_256.txt",
+                                                                 "fp32_dram_bytes_per_launch_full_size")
+                                if n == 256 else None,
+                                "inner_iteration_ms": sum(km)}
     roofs["fp32_ir_stencil"]["frac"] = roofs["fp32_ir_stencil"]["achieved"] / hbm
     roofs["learned_fcg"] = roofs["fp64_cg_stencil"]
 
@@ -457,6 +467,7 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip training/timing the learned preconditioner")
     ap.add_argument("--train-steps", type=int, default=400)
+    ap.add_argument("--methods", default="", help="comma-separated subset of solvers to time (default: all)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3

@@ -166,3 +166,48 @@ def solve_fcg(M: Matrix, net: Unet | None, n: int, d_b, d_x, rel_tol: float = 1e
                                   rel_tol, max_iter, ctypes.byref(info))
     _check(rc, "solve_fcg", allow=(HPCCG_OK, HPCCG_ERR_NOT_CONVERGED))
     return info, rc
+
+
+def _main(argv=None):
+    """Command line: time the U-Net forward pass (random weights) on an n^3 grid,
+    or train the preconditioner and report its FCG iteration gain.
+
+        python -m hpccg_b200.learned forward --n 128 --reps 5
+        python -m hpccg_b200.learned train --n 64 --steps 400
+    """
+    import argparse
+    import json
+
+    import torch
+
+    ap = argparse.ArgumentParser(prog="python -m hpccg_b200.learned")
+    ap.add_argument("cmd", choices=["forward", "train"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--seed", type=int, default=1)
+    a = ap.parse_args(argv)
+    if a.cmd == "forward":
+        net = Unet(a.seed)
+        d_in = torch.randn(a.n ** 3, dtype=torch.float32, device="cuda")
+        d_out = torch.empty_like(d_in)
+        net.forward(d_in, d_out, a.n, a.n, a.n)  # first call sizes the workspace
+        ms = net.time_forward(d_in, d_out, a.n, a.n, a.n, a.reps)
+        print(json.dumps({"unet_forward_ms": ms, "n": a.n, "params": net.nparams}))
+        return 0
+    net, hist = train_preconditioner(a.n, seed=a.seed, steps=a.steps)
+    M = Matrix.generated(a.n, a.n, a.n)
+    b = gaussian_random_field(M, a.n, 4242, torch)
+    x = torch.zeros_like(b)
+    plain, _ = solve_fcg(M, None, a.n, b, x)
+    x.zero_()
+    lrn, _ = solve_fcg(M, net, a.n, b, x)
+    print(json.dumps({"loss_first": float(np.mean(hist[:5])), "loss_last": float(np.mean(hist[-20:])),
+                      "plain_iters": plain.iters, "learned_iters": lrn.iters, "relres": lrn.relres}))
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+
+    sys.exit(_main())
