@@ -228,6 +228,48 @@ def _fp64_relres(M, d_x, d_b, bnorm, scratch):
     return float(np.sqrt(M.ddot1(scratch))) / bnorm
 
 
+def batch_workload(hp, torch, args):
+    """The batched-solve workload: 64 systems with (nx, ny, nz) uniform in [16, 96] (seed 7),
+    x*_s U[-1,1) (seed 7+s), b_s = A_s x*_s, every system to FP64 rel-res 1e-8.  Times the
+    stacked persistent solve (FP64 CG and FP32 refinement) against the same systems solved one
+    after another with the single-system FP64 CG graph."""
+    sizes = hp.batch_sizes(7, 64, 16, 96)
+    B = hp.Batch.generated(sizes)
+    xs = B.stack([hp.uniform_pm1_host(7 + s, int(B.nrows[s])) for s in range(B.nsys)])
+    d_xs = torch.from_numpy(xs).cuda()
+    d_b = torch.empty_like(d_xs)
+    B.spmv(d_xs, d_b)
+    d_x = torch.zeros_like(d_b)
+    out = {"systems": int(B.nsys), "rows": int(B.nrows.sum()), "stacked_rows": int(B.stacked_rows),
+           "sizes": "nx,ny,nz uniform in [16,96], seed 7"}
+    for name, prec in (("fp64", hp.PREC_FP64), ("fp32_ir", hp.PREC_FP32)):
+        times = []
+        for rep in range(args.warmup + args.steps):
+            d_x.zero_()
+            iters, relres, outer, rc = B.solve(d_b, d_x, prec, REL_TOL)
+            if rep >= args.warmup:
+                times.append(B.last_solve_ms())
+        err = max(float((d_x[B.offsets[s]:B.offsets[s] + B.nrows[s]] - d_xs[B.offsets[s]:B.offsets[s] + B.nrows[s]])
+                        .abs().max()) for s in range(B.nsys))
+        out[name] = {"ms": float(np.median(times)), "status": int(rc), "max_relres": float(relres.max()),
+                     "iters_min_max": [int(iters.min()), int(iters.max())], "max_abs_err_vs_xstar": err}
+    out["schedule"] = list(B.get_schedule())
+    seq = 0.0
+    for s, (nx, ny, nz) in enumerate(sizes):
+        M = hp.Matrix.generated(int(nx), int(ny), int(nz))
+        bs = d_b[B.offsets[s]:B.offsets[s] + B.nrows[s]]
+        xsol = torch.zeros_like(bs)
+        M.cg_device(bs, xsol, 1000, REL_TOL * float(torch.linalg.vector_norm(bs)), history=False)
+        xsol.zero_()
+        M.cg_device(bs, xsol, 1000, REL_TOL * float(torch.linalg.vector_norm(bs)), history=False)
+        seq += M.last_solve_ms()
+        M.close()
+    out["sequential_fp64_cg_ms"] = seq
+    out["speedup_fp64_vs_sequential"] = seq / out["fp64"]["ms"]
+    B.close()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -342,6 +384,7 @@ def run_ours(args):
         d_in = torch.randn(N, dtype=torch.float32, device=dev)
         d_out = torch.empty_like(d_in)
         learned_info["unet_forward_ms"] = net.time_forward(d_in, d_out, n, n, n, 3)
+    batch_info = batch_workload(hp, torch, args) if not args.no_batch else None
     ok = {k: v for k, v in results.items() if v["true_relres"] <= REL_TOL}
     head = min(ok, key=lambda k: ok[k]["ms"])
     plain_ms = results["fp64_cg"]["ms"]
@@ -438,7 +481,7 @@ def run_ours(args):
                                f"b = A x*, x0 = 0, solved to FP64 ||b - A x|| <= 1e-8 ||b||",
                    "method": head, "speedup_vs_plain_gpu_cg": plain_ms / hr["ms"],
                    "speedup_vs_plain_gpu_cg_stencil": results["fp64_cg_stencil"]["ms"] / hr["ms"],
-                   "methods": results, "learned": learned_info,
+                   "methods": results, "learned": learned_info, "batch": batch_info,
                    "l2": "inputs (5.4 GB matrix) exceed the 126 MB L2; no flush",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
                    "spmv_kernel": results[head]["spmv_kernel"]},
@@ -468,6 +511,7 @@ def main(argv=None):
     ap.add_argument("--no-learned", action="store_true", help="skip training/timing the learned preconditioner")
     ap.add_argument("--train-steps", type=int, default=400)
     ap.add_argument("--methods", default="", help="comma-separated subset of solvers to time (default: all)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-system batched-solve workload")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3

@@ -131,6 +131,29 @@ def exported_symbols() -> list[str]:
     return sorted(_SIGS)
 
 
+def splitmix64_at(seed: int, i) -> np.ndarray:
+    """The project's counter-based generator (splitmix64 finaliser of seed + (i+1)*golden),
+    the same sequence hpccg_gpu_uniform_pm1 draws on the device; i is an index array."""
+    i = np.asarray(i, np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + (i + np.uint64(1)) * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def uniform_pm1_host(seed: int, n: int, offset: int = 0) -> np.ndarray:
+    """n doubles in [-1, 1) from the generator (host copy of hpccg_gpu_uniform_pm1)."""
+    u = (splitmix64_at(seed, np.arange(offset, offset + n, dtype=np.uint64)) >> np.uint64(11)).astype(np.float64)
+    return 2.0 * (u * 2.0 ** -53) - 1.0
+
+
+def batch_sizes(seed: int, nsys: int, lo: int, hi: int) -> np.ndarray:
+    """Grid sizes of a batch workload: (nx, ny, nz) per system, each uniform in [lo, hi]."""
+    z = splitmix64_at(seed, np.arange(3 * nsys, dtype=np.uint64)) % np.uint64(hi - lo + 1)
+    return (lo + z.astype(np.int64)).astype(np.int32).reshape(nsys, 3)
+
+
 def _dptr(t) -> int:
     """Device pointer of a torch CUDA tensor (contiguous float64 expected)."""
     if not t.is_cuda or not t.is_contiguous():

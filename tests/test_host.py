@@ -77,3 +77,14 @@ def test_driver_built_and_prints_usage():
         subprocess.run(["make", "-s", "-C", PKG], check=True)
     out = subprocess.run([exe], capture_output=True, text=True, timeout=60)
     assert out.returncode == 0 and "USAGE" in out.stdout
+
+
+def test_host_generator_matches_oracle():
+    """The package's host copy of the generator (workload synthesis in bench.py)
+    draws the same numbers as the oracle's restatement."""
+    import hpccg_b200 as hp
+    import oracle
+
+    assert np.array_equal(hp.uniform_pm1_host(1234, 1000), oracle.uniform_pm1(1234, 1000))
+    assert np.array_equal(hp.uniform_pm1_host(9, 50, offset=0), oracle.uniform_pm1(9, 50))
+    assert np.array_equal(hp.batch_sizes(7, 64, 16, 96).reshape(-1), np.asarray(oracle.batch_sizes(7, 64, 16, 96)).reshape(-1))
