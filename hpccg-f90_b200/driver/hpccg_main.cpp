@@ -7,7 +7,15 @@
 // (numerics.F90:103,125,150).  Extra options keep the reference defaults.
 //
 //   HPCCG-B200 nx ny nz [--max-iter N] [--tol T] [--device-generate]
-//                       [--spmv KIND[,PARAM]] [--quiet]
+//                       [--spmv KIND[,PARAM]] [--timing-level L] [--quiet]
+//
+// --timing-level follows the reference's TIMINGLEV (MPI/config.mk TIMER_LEVEL,
+// default 1; numerics.F90:100-156): 1 prints "TIMER: Total"; 2 adds one
+// "TIMER: Iteration" line per iteration; 3 adds "MFLOPS SPARSEMV" with the
+// reference's operation count niters * 2 * total_nnz (total_nnz = 27 N).  The
+// whole CG runs as one graph launch, so the per-iteration figure is the device
+// solve time divided by the iteration count, and the SpMV time is the fused
+// SpMV kernel's measured time per launch times the iteration count.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -62,12 +70,14 @@ int main(int argc, char **argv) {
   int max_iter = 150;    // main.F90:127
   double tolerance = 0;  // main.F90:128
   bool device_generate = false, quiet = false;
+  int timing_level = 1;  // MPI/config.mk TIMER_LEVEL
   int spmv_kind = HPCCG_SPMV_AUTO, spmv_param = 0;
   for (int i = 4; i < argc; ++i) {
     if (!strcmp(argv[i], "--max-iter") && i + 1 < argc) max_iter = atoi(argv[++i]);
     else if (!strcmp(argv[i], "--tol") && i + 1 < argc) tolerance = atof(argv[++i]);
     else if (!strcmp(argv[i], "--device-generate")) device_generate = true;
     else if (!strcmp(argv[i], "--quiet")) quiet = true;
+    else if (!strcmp(argv[i], "--timing-level") && i + 1 < argc) timing_level = atoi(argv[++i]);
     else if (!strcmp(argv[i], "--spmv") && i + 1 < argc) {
       spmv_kind = atoi(argv[++i]);
       const char *comma = strchr(argv[i], ',');
@@ -106,6 +116,8 @@ int main(int argc, char **argv) {
     check(hpccg_gpu_create((int32_t)n, nnz, rowindex.data(), colindex.data(), values.data(), &ctx),
           "create");
   }
+  if (spmv_kind == HPCCG_SPMV_STENCIL && !device_generate)
+    check(hpccg_gpu_set_geometry(ctx, nx, ny, nz), "set_geometry");  // device check of the CSR
   if (spmv_kind != HPCCG_SPMV_AUTO) check(hpccg_gpu_set_spmv(ctx, spmv_kind, spmv_param), "set_spmv");
 
   // printInfo, main.F90:33-75 (total_nnz is the reference's 27*N count)
@@ -137,7 +149,18 @@ int main(int argc, char **argv) {
   }
   if (rc == HPCCG_ERR_BREAKDOWN) printf(" CG breakdown after %d iterations\n", niters);
   const double secs = std::chrono::duration<double>(t1 - t0).count();
-  printf(" TIMER: Total %15.7g sec\n", secs);
+  float solve_ms = 0.f;
+  check(hpccg_gpu_last_solve_ms(ctx, &solve_ms), "last_solve_ms");
+  if (timing_level > 1 && niters > 0)
+    for (int k = 1; k <= niters; ++k) printf(" TIMER: Iteration %15.7g sec\n", 1e-3 * solve_ms / niters);
+  if (timing_level > 0) printf(" TIMER: Total %15.7g sec\n", secs);
+  if (timing_level > 2 && niters > 0) {
+    float kms[3] = {0.f, 0.f, 0.f};
+    check(hpccg_gpu_time_cg_kernels(ctx, 10, kms), "time_cg_kernels");
+    const double total_time_spmv = 1e-3 * kms[1] * niters;
+    const double fnops_sparsemv = niters * 2.0 * (double)(27 * n);
+    printf(" MFLOPS SPARSEMV %15.7g\n", fnops_sparsemv / total_time_spmv / 1.0e6);
+  }
   double err = 0.0;
   for (int64_t i = 0; i < n; ++i) err = std::fmax(err, std::fabs(x[i] - xexact[i]));
   printf(" Iterations: %d  final normr: %.17g  max|x - xexact|: %.3e\n", niters, normr, err);
