@@ -178,6 +178,11 @@ struct EpiDot32 {
     y[i] = s;
     return (double)pi * (double)s;
   }
+  // rows i .. i+3 (i a multiple of 4)
+  __device__ __forceinline__ double store4(int i, float4 s, float4 pi) const {
+    *reinterpret_cast<float4 *>(y + i) = s;
+    return ((double)pi.x * s.x + (double)pi.y * s.y) + ((double)pi.z * s.z + (double)pi.w * s.w);
+  }
 };
 
 // Ap = A p with low-precision values, alpha = rtrans / p.Ap.
@@ -264,6 +269,10 @@ struct EpiStore32 {
   float *y;
   __device__ __forceinline__ double operator()(int i, float s, float = 0.f) const {
     y[i] = s;
+    return 0.0;
+  }
+  __device__ __forceinline__ double store4(int i, float4 s, float4) const {
+    *reinterpret_cast<float4 *>(y + i) = s;
     return 0.0;
   }
 };
@@ -421,7 +430,7 @@ static int launch_inner_body(hpccg_ctx *c, MixedRes *m, int precision, const Mix
   int rc = dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
     using St = decltype(strat);
     using VT = std::remove_pointer_t<decltype(vt)>;
-    k_mp_spmv_dot<St, VT><<<St::grid(g.pm, c->grid), kBlock, 0, s>>>(g);
+    k_mp_spmv_dot<St, VT><<<St::grid(g.pm, g.geom, c->grid), kBlock, 0, s>>>(g);
     return (int)cudaGetLastError();
   });
   if (rc) return rc;
@@ -645,7 +654,7 @@ extern "C" int hpccg_gpu_spmv_lowp(hpccg_ctx *c, int32_t precision, const float 
     using St = decltype(strat);
     using VT = std::remove_pointer_t<decltype(vt)>;
     const PlaneMap pm = spmv_args(c).pm;
-    k_spmv_lp<St, VT><<<St::grid(pm, c->grid), kBlock, 0, c->stream>>>(c->nrow, c->npad, col, (const VT *)val, d_x,
+    k_spmv_lp<St, VT><<<St::grid(pm, StencilGeom{c->gx, c->gy, c->gz}, c->grid), kBlock, 0, c->stream>>>(c->nrow, c->npad, col, (const VT *)val, d_x,
                                                                         d_y, StencilGeom{c->gx, c->gy, c->gz}, pm);
     return (int)cudaGetLastError();
   });
@@ -684,7 +693,7 @@ extern "C" int hpccg_gpu_time_mixed_kernels(hpccg_ctx *c, int32_t precision, int
         dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
           using St = decltype(strat);
           using VT = std::remove_pointer_t<decltype(vt)>;
-          k_mp_spmv_dot<St, VT><<<St::grid(g.pm, c->grid), kBlock, 0, c->stream>>>(g);
+          k_mp_spmv_dot<St, VT><<<St::grid(g.pm, g.geom, c->grid), kBlock, 0, c->stream>>>(g);
           return 0;
         });
       } else {

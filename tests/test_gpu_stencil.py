@@ -144,3 +144,22 @@ def test_stencil_mixed_refinement(hp, torch, precision):
     ref = torch.empty_like(dx)
     M.spmv(xs.float().double(), ref)
     assert float((y32.double() - ref).abs().max()) <= 1e-5 * float(ref.abs().max())
+
+
+@pytest.mark.parametrize("nx,ny,nz", [(3, 5, 7), (9, 2, 11), (4, 4, 4), (16, 16, 16), (33, 17, 5), (128, 4, 2),
+                                      (12, 20, 7), (1, 1, 1)])
+def test_stencil_fp32_spmv(hp, torch, nx, ny, nz):
+    """The FP32 matrix-free SpMV of the inner solves (box sums; four columns per
+    thread when nx is a multiple of 4) against the FP64 SpMV of the same
+    FP32-rounded input, within FP32 accumulation error."""
+    n = nx * ny * nz
+    M = hp.Matrix.generated(nx, ny, nz)
+    M.set_spmv(hp.SPMV_STENCIL)
+    rng = np.random.default_rng(n + 3)
+    x32 = torch.from_numpy(rng.uniform(-1, 1, n).astype(np.float32)).cuda()
+    y32 = torch.empty_like(x32)
+    M.spmv_lowp(hp.PREC_FP32, x32, y32)
+    ref = torch.empty(n, dtype=torch.float64, device="cuda")
+    M.spmv(x32.double(), ref)
+    err = float((y32.double() - ref).abs().max())
+    assert err <= 2e-5 * max(1.0, float(ref.abs().max())), err
