@@ -203,14 +203,15 @@ __device__ __forceinline__ double stencil_rows_box(const StencilGeom &g, const P
   return part;
 }
 
-// FP32 box walk with four consecutive columns per thread (nx a multiple of 4):
-// per plane and grid line one aligned 16-byte load of the four columns plus
-// the two x neighbours, so a row costs ~2 loads and ~8 adds.  Its own map:
-// thread t owns columns 4*(t mod nx*ny/4) .. +3 of one z chunk of zc planes.
-__host__ __device__ inline PlaneMap box4_map(const PlaneMap &m, int nx, int nz) {
+// FP32 box walk with W = 4 or 8 consecutive columns per thread (nx a multiple
+// of W): per plane and grid line W/4 aligned 16-byte loads of the columns plus
+// the two x neighbours, so a row costs well under 2 loads and ~8 adds.  Its own
+// map: thread t owns columns W*(t mod nx*ny/W) .. +W-1 of one z chunk.
+template <int W>
+__host__ __device__ inline PlaneMap boxw_map(const PlaneMap &m, int nx, int nz) {
   PlaneMap q{0, 0, 0};
-  if (m.plane <= 0 || nx % 4) return q;
-  q.plane = m.plane / 4;
+  if (m.plane <= 0 || nx % W) return q;
+  q.plane = m.plane / W;
   q.zc = m.zc / 2 < 4 ? 4 : m.zc / 2;
   q.nzc = (nz + q.zc - 1) / q.zc;
   if ((int64_t)q.plane * q.nzc > (int64_t)kMaxPartials * kBlock) {  // keep the reduction scratch
@@ -220,62 +221,70 @@ __host__ __device__ inline PlaneMap box4_map(const PlaneMap &m, int nx, int nz) 
   return q;
 }
 
-template <class Epi>
-__device__ __forceinline__ double stencil_rows_box4(const StencilGeom &g, const PlaneMap &q,
+template <int W, class Epi>
+__device__ __forceinline__ double stencil_rows_boxw(const StencilGeom &g, const PlaneMap &q,
                                                     const float *__restrict__ x, Epi &epi) {
+  static_assert(W % 4 == 0, "whole 16-byte loads");
   double part = 0.0;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (int64_t)q.plane * q.nzc) return part;
   const int qz = (int)(t / q.plane);
-  const int c0 = 4 * (int)(t - (int64_t)qz * q.plane);  // first of the 4 columns
+  const int c0 = W * (int)(t - (int64_t)qz * q.plane);  // first of the W columns
   const int z0 = qz * q.zc, z1 = min(g.nz, z0 + q.zc);
   const int iy = c0 / g.nx, ix0 = c0 - iy * g.nx;
-  const int plane = 4 * q.plane;
-  const int dl = ix0 > 0 ? -1 : 0, dr = ix0 + 4 < g.nx ? 4 : 3;
-  const float wl = ix0 > 0 ? 1.f : 0.f, wr = ix0 + 4 < g.nx ? 1.f : 0.f;
+  const int plane = W * q.plane;
+  const int dl = ix0 > 0 ? -1 : 0, dr = ix0 + W < g.nx ? W : W - 1;
+  const float wl = ix0 > 0 ? 1.f : 0.f, wr = ix0 + W < g.nx ? 1.f : 0.f;
   const int ylo = iy > 0 ? -g.nx : 0, yhi = iy < g.ny - 1 ? g.nx : 0;
   const float wlo = iy > 0 ? 1.f : 0.f, whi = iy < g.ny - 1 ? 1.f : 0.f;
   const float *pc = x + c0;
-  // 3-point line sums of the 4 columns of one grid line
-  auto line = [&](const float *p, float4 &v, float *s) {
-    v = __ldg(reinterpret_cast<const float4 *>(p));
+  // 3-point line sums of the W columns of one grid line; v = the line's values
+  auto line = [&](const float *p, float *v, float *s) {
+#pragma unroll
+    for (int k = 0; k < W / 4; ++k) {
+      const float4 u = __ldg(reinterpret_cast<const float4 *>(p) + k);
+      v[4 * k] = u.x;
+      v[4 * k + 1] = u.y;
+      v[4 * k + 2] = u.z;
+      v[4 * k + 3] = u.w;
+    }
     const float l = wl * __ldg(p + dl), r = wr * __ldg(p + dr);
-    s[0] = (l + v.x) + v.y;
-    s[1] = (v.x + v.y) + v.z;
-    s[2] = (v.y + v.z) + v.w;
-    s[3] = (v.z + v.w) + r;
+#pragma unroll
+    for (int j = 0; j < W; ++j) s[j] = ((j > 0 ? v[j - 1] : l) + v[j]) + (j < W - 1 ? v[j + 1] : r);
   };
-  // 3x3 box sums of plane z for the 4 columns (zero outside [0, nz)); v = the columns' x
-  auto box = [&](int z, float *b, float4 &v) {
+  // 3x3 box sums of plane z for the W columns (zero outside [0, nz)); v = the columns' x
+  auto box = [&](int z, float *b, float *v) {
     const bool zin = (unsigned)z < (unsigned)g.nz;
     const float *p = pc + (int64_t)(zin ? z : 0) * plane;
-    float s0[4], s1[4], s2[4];
-    float4 u;
+    float s0[W], s1[W], s2[W], u[W];
     line(p + ylo, u, s0);
     line(p, v, s1);
     line(p + yhi, u, s2);
     const float wz = zin ? 1.f : 0.f;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) b[j] = wz * fmaf(wlo, s0[j], fmaf(whi, s2[j], s1[j]));
+    for (int j = 0; j < W; ++j) b[j] = wz * fmaf(wlo, s0[j], fmaf(whi, s2[j], s1[j]));
   };
-  float bm[4], b0[4], bp[4];
-  float4 vm, v0, vp;
+  float bm[W], b0[W], bp[W], vm[W], v0[W], vp[W];
   box(z0 - 1, bm, vm);
   box(z0, b0, v0);
   for (int z = z0; z < z1; ++z) {
     box(z + 1, bp, vp);
-    float4 y;
-    y.x = fmaf(28.f, v0.x, -((bm[0] + b0[0]) + bp[0]));
-    y.y = fmaf(28.f, v0.y, -((bm[1] + b0[1]) + bp[1]));
-    y.z = fmaf(28.f, v0.z, -((bm[2] + b0[2]) + bp[2]));
-    y.w = fmaf(28.f, v0.w, -((bm[3] + b0[3]) + bp[3]));
-    part += epi.store4(c0 + z * plane, y, v0);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int k = 0; k < W / 4; ++k) {
+      float4 y, xv;
+      y.x = fmaf(28.f, v0[4 * k], -((bm[4 * k] + b0[4 * k]) + bp[4 * k]));
+      y.y = fmaf(28.f, v0[4 * k + 1], -((bm[4 * k + 1] + b0[4 * k + 1]) + bp[4 * k + 1]));
+      y.z = fmaf(28.f, v0[4 * k + 2], -((bm[4 * k + 2] + b0[4 * k + 2]) + bp[4 * k + 2]));
+      y.w = fmaf(28.f, v0[4 * k + 3], -((bm[4 * k + 3] + b0[4 * k + 3]) + bp[4 * k + 3]));
+      xv = make_float4(v0[4 * k], v0[4 * k + 1], v0[4 * k + 2], v0[4 * k + 3]);
+      part += epi.store4(c0 + 4 * k + z * plane, y, xv);
+    }
+#pragma unroll
+    for (int j = 0; j < W; ++j) {
       bm[j] = b0[j];
       b0[j] = bp[j];
+      v0[j] = vp[j];
     }
-    v0 = vp;
   }
   return part;
 }
