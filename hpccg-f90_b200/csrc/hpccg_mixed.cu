@@ -360,6 +360,16 @@ __global__ void k_pad_vals27(const double *src, int W, int npad, double *dst) {
 
 static bool uses_stencil(const hpccg_ctx *c) { return spmv_args(c).kind == HPCCG_SPMV_STENCIL; }
 
+// Row map of the low-precision matrix-free SpMV: four columns per thread in one
+// wave of resident threads (StratLpStencil: 256 threads x 4 blocks per SM) when
+// nx allows it, else the context's plane map.
+static PlaneMap lp_map(const hpccg_ctx *c) {
+  const PlaneMap pm = spmv_args(c).pm;
+  if (!uses_stencil(c) || pm.plane <= 0) return pm;
+  const PlaneMap q = boxw_map(4, c->gx, c->gy, c->gz, (int64_t)c->num_sms * StratLpStencil::kMinBlocks * kBlock);
+  return q.plane > 0 ? q : pm;
+}
+
 static int mixed_res(hpccg_ctx *c, int precision, MixedRes **out) {
   const bool stencil = uses_stencil(c);
   if (!stencil && (!c->d_ell_col || c->ell_width > 27)) return HPCCG_ERR_UNSUPPORTED;
@@ -421,7 +431,7 @@ static MixedArgs mixed_args(hpccg_ctx *c, MixedRes *m, int precision) {
   g.st = m->st;
   g.red = reduction_of(c);
   g.geom = StencilGeom{c->gx, c->gy, c->gz};
-  g.pm = spmv_args(c).pm;
+  g.pm = lp_map(c);
   return g;
 }
 
@@ -653,7 +663,7 @@ extern "C" int hpccg_gpu_spmv_lowp(hpccg_ctx *c, int32_t precision, const float 
   rc = dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
     using St = decltype(strat);
     using VT = std::remove_pointer_t<decltype(vt)>;
-    const PlaneMap pm = spmv_args(c).pm;
+    const PlaneMap pm = lp_map(c);
     k_spmv_lp<St, VT><<<St::grid(pm, StencilGeom{c->gx, c->gy, c->gz}, c->grid), kBlock, 0, c->stream>>>(c->nrow, c->npad, col, (const VT *)val, d_x,
                                                                         d_y, StencilGeom{c->gx, c->gy, c->gz}, pm);
     return (int)cudaGetLastError();

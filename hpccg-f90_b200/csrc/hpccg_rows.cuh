@@ -280,7 +280,7 @@ inline SpmvArgs spmv_args(const hpccg_ctx *c) {
   a.ell_col = c->d_ell_col;
   a.ell_val = c->d_ell_val;
   a.geom = StencilGeom{c->gx, c->gy, c->gz};
-  a.pm = c->gx ? plane_map(c->gx, c->gy, c->gz, kMaxPartials) : PlaneMap{0, 0, 0};
+  a.pm = c->gx ? plane_map(c->gx, c->gy, c->gz, kMaxPartials) : PlaneMap{0, 0, 0, 1};
   return a;
 }
 

@@ -121,19 +121,16 @@ struct StratLp {
 
 // Matrix-free FP32 rows of the generate_matrix operator (its values 27 and -1
 // are exact in FP32 and BF16 alike, so one kernel serves both precisions);
-// 3x3 box sums along the plane map (stencil_rows_boxw<4>: four columns per
-// thread when nx is a multiple of 4; eight measured slower) when it is in use.
+// 3x3 box sums along the plane map, or along the four-column map of
+// stencil_rows_boxw<4> (nx a multiple of 4; eight columns measured slower).
+// The map comes with the arguments (lp_map on the host).
 struct StratLpStencil {
   static constexpr int kMinBlocks = 4;
-  static int grid(const PlaneMap &m, const StencilGeom &g, int dflt) {
-    const PlaneMap q4 = boxw_map<4>(m, g.nx, g.nz);
-    return q4.plane > 0 ? plane_grid(q4) : (m.plane > 0 ? plane_grid(m) : dflt);
-  }
+  static int grid(const PlaneMap &m, const StencilGeom &, int dflt) { return m.plane > 0 ? plane_grid(m) : dflt; }
   template <class Epi>
   static __device__ __forceinline__ double rows(int n, int, const int32_t *, const float *, const float *x,
                                                 Epi &e, const StencilGeom &g, const PlaneMap &m) {
-    const PlaneMap q4 = boxw_map<4>(m, g.nx, g.nz);
-    if (q4.plane > 0) return stencil_rows_boxw<4>(g, q4, x, e);
+    if (m.cols == 4) return stencil_rows_boxw<4>(g, m, x, e);
     return m.plane > 0 ? stencil_rows_box(g, m, x, e) : stencil_rows<float>(n, g, m, x, e);
   }
 };

@@ -20,6 +20,8 @@
 // same context, so fused dot products -- and whole CG runs -- are
 // bit-identical between the two.
 #pragma once
+#include <algorithm>
+
 #include "hpccg_internal.cuh"
 
 namespace hpccg {
@@ -29,16 +31,17 @@ struct StencilGeom {
 };
 
 struct PlaneMap {
-  int plane;  // nx*ny rows per z plane; 0 = map not in use (grid-stride rows)
+  int plane;  // nx*ny rows per z plane (divided by cols); 0 = map not in use (grid-stride rows)
   int zc;     // planes per thread
   int nzc;    // z chunks
+  int cols;   // consecutive grid columns per thread (0 or 1: one; 4: the FP32 box walk)
 };
 
 // Host: the plane map for a grid, with at most `max_blocks` blocks of kBlock
 // threads (the reduction scratch holds one partial per block).  Chunks of at
 // least 16 planes keep the per-thread start-up (two extra planes) small.
 inline PlaneMap plane_map(int nx, int ny, int nz, int max_blocks) {
-  PlaneMap m{0, 0, 0};
+  PlaneMap m{0, 0, 0, 1};
   if (nx < 1 || ny < 1 || nz < 1) return m;
   const int64_t plane = (int64_t)nx * ny;
   for (int zc = 16;; zc *= 2) {
@@ -207,17 +210,20 @@ __device__ __forceinline__ double stencil_rows_box(const StencilGeom &g, const P
 // of W): per plane and grid line W/4 aligned 16-byte loads of the columns plus
 // the two x neighbours, so a row costs well under 2 loads and ~8 adds.  Its own
 // map: thread t owns columns W*(t mod nx*ny/W) .. +W-1 of one z chunk.
-template <int W>
-__host__ __device__ inline PlaneMap boxw_map(const PlaneMap &m, int nx, int nz) {
-  PlaneMap q{0, 0, 0};
-  if (m.plane <= 0 || nx % W) return q;
-  q.plane = m.plane / W;
-  q.zc = m.zc / 2 < 4 ? 4 : m.zc / 2;
-  q.nzc = (nz + q.zc - 1) / q.zc;
-  if ((int64_t)q.plane * q.nzc > (int64_t)kMaxPartials * kBlock) {  // keep the reduction scratch
-    q.zc = m.zc;
-    q.nzc = m.nzc;
-  }
+// Host: the map of the W-column walk.  The z range of each column is split so
+// that all threads are resident at once (one wave): a thread's chunk is then
+// as long as possible, which keeps the two extra planes of its start small.
+inline PlaneMap boxw_map(int W, int nx, int ny, int nz, int64_t resident_threads) {
+  PlaneMap q{0, 0, 0, W};
+  if (nx < 1 || ny < 1 || nz < 1 || nx % W) return q;
+  const int64_t cols = (int64_t)nx * ny / W;
+  const int64_t k = std::max<int64_t>(1, std::min<int64_t>(nz, resident_threads / cols));
+  const int zc = (int)((nz + k - 1) / k);
+  const int nzc = (nz + zc - 1) / zc;
+  if (cols * nzc > (int64_t)kMaxPartials * kBlock) return q;  // keep the reduction scratch
+  q.plane = (int)cols;
+  q.zc = zc;
+  q.nzc = nzc;
   return q;
 }
 
