@@ -16,8 +16,13 @@
 #include <algorithm>
 #include <type_traits>
 
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
 #include "hpccg_rows.cuh"
 #include "hpccg_rows_lp.cuh"
+#include "hpccg_stencil_tma.cuh"
 
 namespace hpccg {
 
@@ -208,6 +213,29 @@ __global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_spmv_dot(MixedArgs
   }
 }
 
+// The same with the matrix-free SpMV fed by TMA (hpccg_stencil_tma.cuh).
+__global__ void __launch_bounds__(kBlock) k_mp_spmv_dot_tma(MixedArgs g, TmaTile t,
+                                                            const __grid_constant__ CUtensorMap map) {
+  __shared__ double smem[32];
+  EpiDot32 epi{g.p, g.Ap};
+  const double part = stencil_rows_tma(t, &map, epi, &g.st->status);
+  const double tot = block_sum<kBlock>(part, smem);
+  if (arrive_last(g.red, tot)) {
+    const double pAp = finish_sum<kBlock>(g.red, smem);
+    if (threadIdx.x == 0) {
+      MixedState &st = *g.st;
+      st.pending = 0;
+      const double alpha = st.rtrans / pAp;
+      if (!(pAp > 0.0) || !isfinite(alpha)) {
+        st.inner_break = 1;
+        st.alpha = 0.0;
+      } else {
+        st.alpha = alpha;
+      }
+    }
+  }
+}
+
 // r -= alpha Ap, rr, inner stop test.
 __global__ void __launch_bounds__(kBlock) k_mp_update_r(MixedArgs g) {
   __shared__ double smem[32];
@@ -284,6 +312,50 @@ __global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_spmv_lp(int n, int np
   S::rows(n, npad, col, val, x, epi, geom, pm);
 }
 
+__global__ void __launch_bounds__(kBlock) k_spmv_lp_tma(TmaTile t, const __grid_constant__ CUtensorMap map, float *y,
+                                                        int *status) {
+  EpiStore32 epi{y};
+  stencil_rows_tma(t, &map, epi, status);
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+static std::mutex g_encode_mu;
+
+int make_stencil_tmap(CUtensorMap *map, const float *base, int nx, int ny, int nz) {
+  {
+    std::lock_guard<std::mutex> lk(g_encode_mu);
+    if (!g_encode) {
+      void *fn = nullptr;
+      cudaDriverEntryPointQueryResult q;
+      const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+      if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+        return set_cuda_error(e == cudaSuccess ? cudaErrorNotSupported : e, "cuTensorMapEncodeTiled", __FILE__,
+                              __LINE__);
+      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+  }
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || nx % 4) return HPCCG_ERR_UNSUPPORTED;
+  const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4};
+  const cuuint32_t box[3] = {kTmaBoxX, kTmaBoxY, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims, strides, box,
+                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? HPCCG_OK : HPCCG_ERR_UNSUPPORTED;
+}
+
+// Plan of the TMA SpMV for a context (nzc = 0: not usable).
+static TmaTile tma_plan(const hpccg_ctx *c) {
+  static int per_sm = 0;
+  if (!per_sm) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_spmv_dot_tma, kBlock, 0) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+  }
+  return tma_tile_plan(c->gx, c->gy, c->gz, c->num_sms * per_sm);
+}
+
 __global__ void k_to_lp(const double *src, float *f32, __nv_bfloat16 *b16, size_t count) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
     const double v = src[i];
@@ -326,6 +398,11 @@ struct MixedRes {
   int exec_rpt[3] = {0, 0, 0};
   bool exec_stencil[3] = {false, false, false};
   int rpt[3] = {0, 2, 4};  // rows per thread per precision (index 1 = FP32, 2 = BF16)
+  // matrix-free SpMV on p by TMA (when the context uses the stencil and nx % 4 == 0)
+  CUtensorMap pmap;
+  TmaTile tile{};
+  bool tma = false;
+  int tma_gx = 0;  // grid the map was made for
 };
 
 #include <map>
@@ -411,9 +488,16 @@ static int mixed_res(hpccg_ctx *c, int precision, MixedRes **out) {
     if (tmp) cudaFree(tmp);
     HPCCG_CUDA(cudaGetLastError());
   }
+  if (stencil && m->tma_gx != c->gx) {
+    m->tile = tma_plan(c);
+    m->tma = m->tile.nzc > 0 && make_stencil_tmap(&m->pmap, m->p, c->gx, c->gy, c->gz) == HPCCG_OK;
+    m->tma_gx = c->gx;
+  }
   *out = m;
   return HPCCG_OK;
 }
+
+static bool use_tma(const hpccg_ctx *c, const MixedRes *m) { return uses_stencil(c) && m->tma; }
 
 static MixedArgs mixed_args(hpccg_ctx *c, MixedRes *m, int precision) {
   MixedArgs g{};
@@ -437,6 +521,11 @@ static MixedArgs mixed_args(hpccg_ctx *c, MixedRes *m, int precision) {
 
 static int launch_inner_body(hpccg_ctx *c, MixedRes *m, int precision, const MixedArgs &g, cudaStream_t s) {
   k_mp_update_p<<<c->grid, kBlock, 0, s>>>(g);
+  if (use_tma(c, m)) {
+    k_mp_spmv_dot_tma<<<tma_tile_grid(m->tile), kBlock, 0, s>>>(g, m->tile, m->pmap);
+    k_mp_update_r<<<c->grid, kBlock, 0, s>>>(g);
+    return (int)cudaGetLastError();
+  }
   int rc = dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
     using St = decltype(strat);
     using VT = std::remove_pointer_t<decltype(vt)>;
@@ -658,6 +747,18 @@ extern "C" int hpccg_gpu_spmv_lowp(hpccg_ctx *c, int32_t precision, const float 
   MixedRes *m = nullptr;
   int rc = mixed_res(c, precision, &m);
   if (rc) return rc;
+  if (use_tma(c, m)) {
+    CUtensorMap xmap;
+    if (make_stencil_tmap(&xmap, d_x, c->gx, c->gy, c->gz) == HPCCG_OK) {
+      HPCCG_CUDA(cudaMemsetAsync(&m->st->status, 0, sizeof(int), c->stream));
+      k_spmv_lp_tma<<<tma_tile_grid(m->tile), kBlock, 0, c->stream>>>(m->tile, xmap, d_y, &m->st->status);
+      HPCCG_CUDA(cudaGetLastError());
+      int status = 0;
+      HPCCG_CUDA(cudaMemcpyAsync(&status, &m->st->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+      return status ? status : HPCCG_OK;
+    }
+  }
   const int32_t *col = m->col27 ? m->col27 : c->d_ell_col;
   const void *val = precision == 1 ? (const void *)m->val32 : (const void *)m->val16;
   rc = dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
@@ -699,6 +800,8 @@ extern "C" int hpccg_gpu_time_mixed_kernels(hpccg_ctx *c, int32_t precision, int
       HPCCG_CUDA(cudaMemsetAsync(&m->st->inner_break, 0, sizeof(int), c->stream));
       if (which == 0) {
         k_mp_update_p<<<c->grid, kBlock, 0, c->stream>>>(g);
+      } else if (which == 1 && use_tma(c, m)) {
+        k_mp_spmv_dot_tma<<<tma_tile_grid(m->tile), kBlock, 0, c->stream>>>(g, m->tile, m->pmap);
       } else if (which == 1) {
         dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
           using St = decltype(strat);
