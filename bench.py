@@ -447,12 +447,13 @@ def run_ours(args):
     km = M.time_mixed_kernels(hp.PREC_FP32, 20)
     alg = 8 * N + 4
     roofs["fp32_ir_stencil"] = {"bound": "hbm",
-                                "kernel": "k_mp_spmv_dot<StratLpStencil> (matrix-free FP32 SpMV + p.Ap)",
+                                "kernel": "k_mp_spmv_dot_tma (matrix-free FP32 SpMV, TMA-fed, + p.Ap)"
+                                if n % 4 == 0 else "k_mp_spmv_dot<StratLpStencil> (matrix-free FP32 SpMV + p.Ap)",
                                 "kernel_ms": km[1], "alg_bytes_per_launch": alg,
                                 "achieved": alg / (km[1] * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                                 "peak_source": peak_kind,
                                 "traffic": _traffic_from_profile("stencil_spmv_256.txt",
-                                                                 "fp32_dram_bytes_per_launch_full_size")
+                                                                 "fp32_tma_dram_bytes_per_launch_full_size")
                                 if n == 256 else None,
                                 "inner_iteration_ms": sum(km)}
     roofs["fp32_ir_stencil"]["frac"] = roofs["fp32_ir_stencil"]["achieved"] / hbm
