@@ -254,6 +254,17 @@ def batch_workload(hp, torch, args):
         out[name] = {"ms": float(np.median(times)), "status": int(rc), "max_relres": float(relres.max()),
                      "iters_min_max": [int(iters.min()), int(iters.max())], "max_abs_err_vs_xstar": err}
     out["schedule"] = list(B.get_schedule())
+    B.set_spmv(hp.SPMV_STENCIL)  # matrix-free rows, same iterates in FP64
+    for name, prec in (("fp64_stencil", hp.PREC_FP64), ("fp32_ir_stencil", hp.PREC_FP32)):
+        times = []
+        for rep in range(args.warmup + args.steps):
+            d_x.zero_()
+            iters, relres, outer, rc = B.solve(d_b, d_x, prec, REL_TOL)
+            if rep >= args.warmup:
+                times.append(B.last_solve_ms())
+        out[name] = {"ms": float(np.median(times)), "status": int(rc), "max_relres": float(relres.max()),
+                     "iters_min_max": [int(iters.min()), int(iters.max())]}
+    out["schedule_stencil"] = list(B.get_schedule())
     seq = 0.0
     for s, (nx, ny, nz) in enumerate(sizes):
         M = hp.Matrix.generated(int(nx), int(ny), int(nz))

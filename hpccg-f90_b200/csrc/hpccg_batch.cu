@@ -15,6 +15,10 @@
 //   FP32 / BF16: per-system FP64 iterative refinement around an inner CG in
 //         FP32 vectors and FP32 / BF16 values (as hpccg_mixed.cu), with the
 //         FP64 true residual as the judge of every system.
+// Batches built by hpccg_batch_create_generated may switch to matrix-free
+// rows (hpccg_batch_set_spmv, HPCCG_SPMV_STENCIL): each row is formed from the
+// system's own grid with the reference's term order (hpccg_stencil.cuh), so
+// the FP64 iterates are bit-identical to the ELL rows'.
 #include <stdlib.h>
 
 #include <algorithm>
@@ -23,6 +27,7 @@
 
 #include "hpccg_internal.cuh"
 #include "hpccg_rows_lp.cuh"
+#include "hpccg_stencil.cuh"
 
 namespace hpccg {
 
@@ -46,6 +51,7 @@ struct BatchArgs {
   double *part;             // one partial per chunk
   unsigned *counter;
   BatchSys *sys;
+  const int4 *dims;         // (nx, ny, nz, first row) per system: matrix-free rows; null = ELL
   double rel_tol, inner_rtol;
   int max_iter, max_outer, max_inner;
   cudaGraphConditionalHandle c_outer, c_inner;
@@ -53,7 +59,11 @@ struct BatchArgs {
 };
 
 // ---- per-row operations ------------------------------------------------------
-__device__ __forceinline__ double row_fp64(const BatchArgs &g, int i, const double *x) {
+__device__ __forceinline__ double row_fp64(const BatchArgs &g, int i, int sys, const double *x) {
+  if (g.dims) {
+    const int4 d = g.dims[sys];
+    return stencil_row<double>(i - d.w, StencilGeom{d.x, d.y, d.z}, x + d.w);
+  }
   double s = 0.0;
 #pragma unroll
   for (int k = 0; k < 27; ++k) {
@@ -64,7 +74,11 @@ __device__ __forceinline__ double row_fp64(const BatchArgs &g, int i, const doub
 }
 
 template <typename VT>
-__device__ __forceinline__ float row_lp(const BatchArgs &g, int i, const float *x) {
+__device__ __forceinline__ float row_lp(const BatchArgs &g, int i, int sys, const float *x) {
+  if (g.dims) {
+    const int4 d = g.dims[sys];
+    return stencil_row<float>(i - d.w, StencilGeom{d.x, d.y, d.z}, x + d.w);
+  }
   float s = 0.f;
   const VT *val = reinterpret_cast<const VT *>(g.val_lp);
 #pragma unroll
@@ -100,7 +114,7 @@ struct PhBnorm {  // bb = b.b
 struct PhInit64 {  // r = b - A x, p = r, rtrans = r.r
   static __device__ bool active(const BatchArgs &g, int s) { return true; }
   static __device__ double row(const BatchArgs &g, int i, int s) {
-    const double ri = __dsub_rn(g.b[i], row_fp64(g, i, g.x));
+    const double ri = __dsub_rn(g.b[i], row_fp64(g, i, s, g.x));
     g.r[i] = ri;
     return __dmul_rn(ri, ri);
   }
@@ -118,7 +132,7 @@ struct PhInit64 {  // r = b - A x, p = r, rtrans = r.r
 struct PhSpmvDot64 {  // Ap = A p, alpha = rtrans / p.Ap
   static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].active; }
   static __device__ double row(const BatchArgs &g, int i, int s) {
-    const double ai = row_fp64(g, i, g.p);
+    const double ai = row_fp64(g, i, s, g.p);
     g.Ap[i] = ai;
     return __dmul_rn(g.p[i], ai);
   }
@@ -164,7 +178,7 @@ struct PhUpdate64 {  // x += alpha p, r -= alpha Ap, beta, per-system stop test
 struct PhResidual64 {  // final r = b - A x, relres (all systems)
   static __device__ bool active(const BatchArgs &g, int s) { return true; }
   static __device__ double row(const BatchArgs &g, int i, int s) {
-    const double ri = __dsub_rn(g.b[i], row_fp64(g, i, g.x));
+    const double ri = __dsub_rn(g.b[i], row_fp64(g, i, s, g.x));
     return __dmul_rn(ri, ri);
   }
   static __device__ void finalize(const BatchArgs &g, int s, double t) {
@@ -179,7 +193,7 @@ struct PhResidual64 {  // final r = b - A x, relres (all systems)
 struct PhOuter64 {  // r64 = b - A x, relres, outer decision (systems still refining)
   static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].active; }
   static __device__ double row(const BatchArgs &g, int i, int s) {
-    const double ri = __dsub_rn(g.b[i], row_fp64(g, i, g.x));
+    const double ri = __dsub_rn(g.b[i], row_fp64(g, i, s, g.x));
     g.r[i] = ri;
     return __dmul_rn(ri, ri);
   }
@@ -224,7 +238,7 @@ template <typename VT>
 struct PhSpmvDotLp {
   static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].inner_active; }
   static __device__ double row(const BatchArgs &g, int i, int s) {
-    const float ai = row_lp<VT>(g, i, g.p32);
+    const float ai = row_lp<VT>(g, i, s, g.p32);
     g.Ap32[i] = ai;
     return (double)g.p32[i] * ai;
   }
@@ -356,7 +370,7 @@ __global__ void __launch_bounds__(256) k_batch_end_inner(BatchArgs g) {
 __global__ void k_batch_spmv(BatchArgs g, const double *x, double *y) {
   for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
     const int4 tile = g.tiles[t];
-    for (int i = tile.y + threadIdx.x; i < tile.z; i += 256) y[i] = row_fp64(g, i, x);
+    for (int i = tile.y + threadIdx.x; i < tile.z; i += 256) y[i] = row_fp64(g, i, tile.x, x);
   }
 }
 
@@ -438,11 +452,13 @@ struct hpccg_batch {
   BatchSys *sys = nullptr;
   int *d_sys_chunk0 = nullptr;
   int4 *d_tiles = nullptr;
+  int4 *d_dims = nullptr;  // generated batches: (nx, ny, nz, first row) per system
+  int spmv_kind = HPCCG_SPMV_ELL;
   int ntiles = 0;
   int tile_chunks = 0, blocks_per_sm = 0;  // schedule; 0 = not tuned yet
   bool tuned = false;
   cudaGraphExec_t exec[3] = {nullptr, nullptr, nullptr};
-  int exec_tile[3] = {0, 0, 0}, exec_bps[3] = {0, 0, 0}, exec_maxit[3] = {-1, -1, -1};
+  int exec_tile[3] = {0, 0, 0}, exec_bps[3] = {0, 0, 0}, exec_maxit[3] = {-1, -1, -1}, exec_kind[3] = {0, 0, 0};
   double exec_tol[3] = {-1.0, -1.0, -1.0};
   float last_ms = 0.f;
 };
@@ -451,7 +467,7 @@ static void batch_free(hpccg_batch *B) {
   for (auto &e : B->exec)
     if (e) cudaGraphExecDestroy(e);
   void *bufs[] = {B->col, B->val, B->val32, B->val16, B->x, B->b, B->r, B->p, B->Ap, B->r32, B->p32,
-                  B->Ap32, B->d32, B->part, B->counter, B->sys, B->d_sys_chunk0, B->d_tiles};
+                  B->Ap32, B->d32, B->part, B->counter, B->sys, B->d_sys_chunk0, B->d_tiles, B->d_dims};
   for (void *q : bufs)
     if (q) cudaFree(q);
   if (B->ev0) cudaEventDestroy(B->ev0);
@@ -562,6 +578,18 @@ extern "C" int hpccg_batch_create_generated(int32_t nsys, const int32_t *sizes, 
   for (int s = 0; s < nsys; ++s)
     k_batch_generate<<<B->num_sms * 8, 256, 0, B->stream>>>(sizes[3 * s], sizes[3 * s + 1], sizes[3 * s + 2],
                                                              B->off[s], B->npad, B->col, B->val);
+  {
+    std::vector<int4> dims(nsys);
+    for (int s = 0; s < nsys; ++s) dims[s] = make_int4(sizes[3 * s], sizes[3 * s + 1], sizes[3 * s + 2], B->off[s]);
+    cudaError_t e = cudaMalloc(&B->d_dims, sizeof(int4) * nsys);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(B->d_dims, dims.data(), sizeof(int4) * nsys, cudaMemcpyHostToDevice, B->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
+    if (e != cudaSuccess) {
+      batch_free(B);
+      return set_cuda_error(e, "batch dims", __FILE__, __LINE__);
+    }
+  }
   if ((rc = batch_pad_rows(B))) {
     batch_free(B);
     return rc;
@@ -668,6 +696,7 @@ static BatchArgs batch_args(hpccg_batch *B, int precision) {
   g.part = B->part;
   g.counter = B->counter;
   g.sys = B->sys;
+  g.dims = B->spmv_kind == HPCCG_SPMV_STENCIL ? B->d_dims : nullptr;
   return g;
 }
 
@@ -795,7 +824,8 @@ static int run_batch(hpccg_batch *B, int precision, bool eager, double rel_tol, 
     return HPCCG_OK;
   }
   if (!B->exec[precision] || B->exec_tile[precision] != B->tile_chunks || B->exec_bps[precision] != B->blocks_per_sm ||
-      B->exec_tol[precision] != rel_tol || B->exec_maxit[precision] != max_iter) {
+      B->exec_tol[precision] != rel_tol || B->exec_maxit[precision] != max_iter ||
+      B->exec_kind[precision] != B->spmv_kind) {
     if (B->exec[precision]) cudaGraphExecDestroy(B->exec[precision]);
     B->exec[precision] = nullptr;
     cudaStreamCaptureStatus cs;
@@ -849,6 +879,7 @@ static int run_batch(hpccg_batch *B, int precision, bool eager, double rel_tol, 
       return set_cuda_error(e, "build batch graph", __FILE__, __LINE__);
     }
     B->exec_tile[precision] = B->tile_chunks;
+    B->exec_kind[precision] = B->spmv_kind;
     B->exec_bps[precision] = B->blocks_per_sm;
     B->exec_tol[precision] = rel_tol;
     B->exec_maxit[precision] = max_iter;
@@ -930,6 +961,18 @@ extern "C" int hpccg_batch_set_schedule(hpccg_batch *B, int32_t tile_chunks, int
   return build_tiles(B, tile_chunks);
 }
 
+extern "C" int hpccg_batch_set_spmv(hpccg_batch *B, int32_t kind) {
+  if (!B) return HPCCG_ERR_INVALID_ARG;
+  if (kind == HPCCG_SPMV_AUTO) kind = HPCCG_SPMV_ELL;
+  if (kind != HPCCG_SPMV_ELL && kind != HPCCG_SPMV_STENCIL) return HPCCG_ERR_INVALID_ARG;
+  if (kind == HPCCG_SPMV_STENCIL && !B->d_dims) return HPCCG_ERR_UNSUPPORTED;
+  if (kind != B->spmv_kind) {
+    B->spmv_kind = kind;
+    B->tuned = false;  // the schedule is re-timed with the new rows
+  }
+  return HPCCG_OK;
+}
+
 extern "C" int hpccg_batch_get_schedule(const hpccg_batch *B, int32_t *tile_chunks, int32_t *blocks_per_sm) {
   if (!B) return HPCCG_ERR_INVALID_ARG;
   if (tile_chunks) *tile_chunks = B->tile_chunks;
@@ -954,7 +997,8 @@ extern "C" int hpccg_batch_solve(hpccg_batch *B, const double *d_b, double *d_x,
     return HPCCG_ERR_INVALID_ARG;
   int rc = autotune(B);
   if (rc) return rc;
-  if (precision != HPCCG_PREC_FP64 && (rc = ensure_lp(B, precision))) return rc;
+  if (precision != HPCCG_PREC_FP64 && B->spmv_kind != HPCCG_SPMV_STENCIL && (rc = ensure_lp(B, precision)))
+    return rc;
   const size_t bytes = sizeof(double) * B->npad;
   HPCCG_CUDA(cudaMemcpyAsync(B->b, d_b, bytes, cudaMemcpyDeviceToDevice, B->stream));
   HPCCG_CUDA(cudaMemcpyAsync(B->x, d_x, bytes, cudaMemcpyDeviceToDevice, B->stream));

@@ -89,6 +89,7 @@ _SIGS = {
     "hpccg_batch_destroy": (None, [_vp]),
     "hpccg_batch_info": (_c.c_int, [_vp, _c.POINTER(_i32), _c.POINTER(_i64), _vp]),
     "hpccg_batch_set_schedule": (_c.c_int, [_vp, _i32, _i32]),
+    "hpccg_batch_set_spmv": (_c.c_int, [_vp, _i32]),
     "hpccg_batch_get_schedule": (_c.c_int, [_vp, _c.POINTER(_i32), _c.POINTER(_i32)]),
     "hpccg_batch_spmv": (_c.c_int, [_vp, _vp, _vp]),
     "hpccg_batch_solve": (_c.c_int, [_vp, _vp, _vp, _i32, _f64, _i32, _vp, _vp, _vp]),
@@ -434,6 +435,10 @@ class Batch:
 
     def set_schedule(self, tile_chunks: int, blocks_per_sm: int):
         _check(_lib.hpccg_batch_set_schedule(self._h, tile_chunks, blocks_per_sm), "batch_set_schedule")
+
+    def set_spmv(self, kind: int):
+        """SPMV_ELL (stacked matrix) or SPMV_STENCIL (matrix-free; generated batches only)."""
+        _check(_lib.hpccg_batch_set_spmv(self._h, kind), "batch_set_spmv")
 
     def get_schedule(self):
         t, b = _i32(0), _i32(0)

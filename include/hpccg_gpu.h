@@ -186,6 +186,12 @@ int hpccg_batch_info(const hpccg_batch *batch, int32_t *nsys, int64_t *stacked_r
 /* Tile size in 512-row chunks and resident blocks per SM of the phase
  * kernels; (0, 0) re-enables the autotuner (run on the next solve). */
 int hpccg_batch_set_schedule(hpccg_batch *batch, int32_t tile_chunks, int32_t blocks_per_sm);
+/* Row kernel of the batch: HPCCG_SPMV_ELL (default; the stacked matrix) or
+ * HPCCG_SPMV_STENCIL (matrix-free rows from each system's grid, reference term
+ * order, so FP64 iterates are bit-identical; only for batches from
+ * hpccg_batch_create_generated, else HPCCG_ERR_UNSUPPORTED).  A change of kind
+ * re-runs the schedule autotuner on the next solve. */
+int hpccg_batch_set_spmv(hpccg_batch *batch, int32_t kind);
 int hpccg_batch_get_schedule(const hpccg_batch *batch, int32_t *tile_chunks, int32_t *blocks_per_sm);
 /* y = A x over all systems (stacked device vectors). */
 int hpccg_batch_spmv(hpccg_batch *batch, const double *d_x, double *d_y);

@@ -141,3 +141,44 @@ def test_batch_eager_equals_graph(hp, torch, monkeypatch):
             B.solve(db, dx, prec, 1e-8, 1000)
             res.append(dx.cpu().numpy())
     assert np.array_equal(res[0], res[2]) and np.array_equal(res[1], res[3])
+
+
+def test_batch_stencil_bit_identical_to_ell(hp, torch):
+    """Matrix-free rows (generated batches) give the ELL batch's FP64 iterates
+    bit for bit; the FP32 refinement meets the FP64 target per system; a batch
+    built from CSR refuses the stencil."""
+    sizes = [(3, 5, 7), (16, 16, 16), (1, 1, 1), (20, 9, 13), (2, 2, 2), (31, 17, 5)]
+    B = hp.Batch.generated(sizes)
+    xs = B.stack([oracle.uniform_pm1(11 + s, int(B.nrows[s])) for s in range(B.nsys)])
+    d_xs = torch.from_numpy(xs).cuda()
+    y_ell, y_st = torch.empty_like(d_xs), torch.empty_like(d_xs)
+    B.spmv(d_xs, y_ell)
+    B.set_spmv(hp.SPMV_STENCIL)
+    B.spmv(d_xs, y_st)
+    for u, v in zip(B.unstack(y_ell.cpu().numpy()), B.unstack(y_st.cpu().numpy())):  # real rows only
+        assert np.array_equal(u.view(np.int64), v.view(np.int64))
+    d_b = torch.from_numpy(B.stack(B.unstack(y_ell.cpu().numpy()))).cuda()  # zero gaps
+    runs = {}
+    for kind in (hp.SPMV_ELL, hp.SPMV_STENCIL):
+        B.set_spmv(kind)
+        d_x = torch.zeros_like(d_b)
+        iters, relres, outer, rc = B.solve(d_b, d_x, FP64, 1e-10)
+        assert rc == hp.HPCCG_OK
+        runs[kind] = (iters.copy(), relres.copy(), d_x.cpu().numpy())
+    assert np.array_equal(runs[hp.SPMV_ELL][0], runs[hp.SPMV_STENCIL][0])
+    for u, v in zip(B.unstack(runs[hp.SPMV_ELL][2]), B.unstack(runs[hp.SPMV_STENCIL][2])):
+        assert np.array_equal(u.view(np.int64), v.view(np.int64))
+    B.set_spmv(hp.SPMV_STENCIL)
+    d_x = torch.zeros_like(d_b)
+    iters, relres, outer, rc = B.solve(d_b, d_x, FP32, 1e-8)
+    assert rc == hp.HPCCG_OK and np.all(relres <= 1e-8)
+    for s in range(B.nsys):
+        A, _, _, _ = oracle.generate_matrix(*sizes[s])
+        xs_s = d_x.cpu().numpy()[B.offsets[s]:B.offsets[s] + B.nrows[s]]
+        bs = d_b.cpu().numpy()[B.offsets[s]:B.offsets[s] + B.nrows[s]]
+        assert np.linalg.norm(bs - oracle.spmv(A, xs_s)) <= 1e-8 * np.linalg.norm(bs) * (1 + 1e-6)
+    A4 = oracle.generate_matrix(4, 4, 4)[0]
+    Bc = hp.Batch.from_csr([(A4.rowindex, A4.colindex, A4.values)])
+    with pytest.raises(hp.HpccgError) as e:
+        Bc.set_spmv(hp.SPMV_STENCIL)
+    assert e.value.code == hp.HPCCG_ERR_UNSUPPORTED
