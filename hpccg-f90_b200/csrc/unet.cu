@@ -169,8 +169,12 @@ static int conv(hpccg_unet *u, int layer, int level, const __nv_bfloat16 *in0, c
     return launch_conv3_tc(nin, epi, a, u->num_sms, u->stream);
   }
   if (in_f32 && (epi == kEpiBiasRelu || epi == kEpiBias)) {  // the 1-channel input layer
-    k_conv3_in1<<<grid1d(u, Lv.nvox), 256, 0, u->stream>>>(in_f32, W, bias, static_cast<__nv_bfloat16 *>(out),
-                                                          Lv.nx, Lv.ny, Lv.nz, u->nb, epi == kEpiBiasRelu);
+    if (Lv.nx % 4 == 0)
+      k_conv3_in1x4<<<grid1d(u, Lv.nvox / 4), 256, 0, u->stream>>>(
+          in_f32, W, bias, static_cast<__nv_bfloat16 *>(out), Lv.nx, Lv.ny, Lv.nz, u->nb, epi == kEpiBiasRelu);
+    else
+      k_conv3_in1<<<grid1d(u, Lv.nvox), 256, 0, u->stream>>>(
+          in_f32, W, bias, static_cast<__nv_bfloat16 *>(out), Lv.nx, Lv.ny, Lv.nz, u->nb, epi == kEpiBiasRelu);
     HPCCG_CUDA(cudaGetLastError());
     return HPCCG_OK;
   }

@@ -90,43 +90,82 @@ __global__ void k_conv3_cc(CcConvArgs a) {
   }
 }
 
-// The 1-channel input layer: out[v][co] = act(sum_tap in[v+off] W[tap][co] + b[co]),
-// weights and bias staged in shared memory, two 16-byte BF16 stores per voxel.
-__global__ void __launch_bounds__(256) k_conv3_in1(const float *in, const float *W, const float *bias,
-                                                   __nv_bfloat16 *out, int nx, int ny, int nz, int nb, int relu) {
-  __shared__ float sw[27 * 16 + 16];
+// The 1-channel input layer: out[v][co] = act(sum_tap in[v+off] W[tap][co] + b[co]).
+// A thread forms V voxels consecutive in x (nx a multiple of V): per (dz, dy)
+// line it loads the V+2 inputs once, and each tap's 16 weights (shared memory)
+// once for all V voxels; two 16-byte BF16 stores per voxel.
+template <int V>
+__device__ __forceinline__ void conv3_in1_body(const float *in, const float *W, const float *bias,
+                                               __nv_bfloat16 *out, int nx, int ny, int nz, int nb, int relu) {
+  __shared__ __align__(16) float sw[27 * 16 + 16];
   for (int e = threadIdx.x; e < 27 * 16 + 16; e += blockDim.x) sw[e] = e < 27 * 16 ? W[e] : bias[e - 27 * 16];
   __syncthreads();
-  const int64_t nvox = (int64_t)nx * ny * nz * nb;
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvox; v += (int64_t)gridDim.x * blockDim.x) {
-    const int x = (int)(v % nx), y = (int)((v / nx) % ny), z = (int)((v / ((int64_t)nx * ny)) % nz);
-    float acc[16];
+  const int64_t ngroups = (int64_t)nx * ny * nz * nb / V;
+  for (int64_t gi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gi < ngroups;
+       gi += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v0 = gi * V;
+    const int64_t row = v0 / nx;  // (b, z, y)
+    const int x0 = (int)(v0 - row * nx), y = (int)(row % ny), z = (int)((row / ny) % nz);
+    float acc[V][16];
 #pragma unroll
-    for (int c = 0; c < 16; ++c) acc[c] = sw[27 * 16 + c];
+    for (int j = 0; j < V; ++j)
 #pragma unroll
-    for (int tap = 0; tap < 27; ++tap) {
-      const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
-      const bool inside = (unsigned)(x + dx) < (unsigned)nx && (unsigned)(y + dy) < (unsigned)ny &&
-                          (unsigned)(z + dz) < (unsigned)nz;
-      const float s = inside ? __ldg(in + v + dx + (int64_t)dy * nx + (int64_t)dz * nx * ny) : 0.f;
+      for (int c = 0; c < 16; ++c) acc[j][c] = sw[27 * 16 + c];
 #pragma unroll
-      for (int c = 0; c < 16; ++c) acc[c] = fmaf(s, sw[tap * 16 + c], acc[c]);
-    }
-    uint32_t w[8];
+    for (int dz = -1; dz <= 1; ++dz) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      float lo = acc[2 * c], hi = acc[2 * c + 1];
-      if (relu) {
-        lo = fmaxf(lo, 0.f);
-        hi = fmaxf(hi, 0.f);
+      for (int dy = -1; dy <= 1; ++dy) {
+        const bool line = (unsigned)(y + dy) < (unsigned)ny && (unsigned)(z + dz) < (unsigned)nz;
+        const float *p = in + v0 + (int64_t)dy * nx + (int64_t)dz * nx * ny;
+        float s[V + 2];
+#pragma unroll
+        for (int k = 0; k < V + 2; ++k) {
+          const int xx = x0 + k - 1;
+          s[k] = (line && (unsigned)xx < (unsigned)nx) ? __ldg(p + k - 1) : 0.f;
+        }
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+          const float4 *w4 = reinterpret_cast<const float4 *>(sw + ((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)) * 16);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const float4 w = w4[q];
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+              const float a = s[j + dx + 1];
+              acc[j][4 * q] = fmaf(a, w.x, acc[j][4 * q]);
+              acc[j][4 * q + 1] = fmaf(a, w.y, acc[j][4 * q + 1]);
+              acc[j][4 * q + 2] = fmaf(a, w.z, acc[j][4 * q + 2]);
+              acc[j][4 * q + 3] = fmaf(a, w.w, acc[j][4 * q + 3]);
+            }
+          }
+        }
       }
-      const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
-      w[c] = *reinterpret_cast<const uint32_t *>(&h);
     }
-    const int64_t row = v / nx;
-    *reinterpret_cast<uint4 *>(out + act_unit(row, 0, x, nx) * 8) = make_uint4(w[0], w[1], w[2], w[3]);
-    *reinterpret_cast<uint4 *>(out + act_unit(row, 1, x, nx) * 8) = make_uint4(w[4], w[5], w[6], w[7]);
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      uint32_t w[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        float lo = acc[j][2 * c], hi = acc[j][2 * c + 1];
+        if (relu) {
+          lo = fmaxf(lo, 0.f);
+          hi = fmaxf(hi, 0.f);
+        }
+        const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+        w[c] = *reinterpret_cast<const uint32_t *>(&h);
+      }
+      *reinterpret_cast<uint4 *>(out + act_unit(row, 0, x0 + j, nx) * 8) = make_uint4(w[0], w[1], w[2], w[3]);
+      *reinterpret_cast<uint4 *>(out + act_unit(row, 1, x0 + j, nx) * 8) = make_uint4(w[4], w[5], w[6], w[7]);
+    }
   }
+}
+__global__ void __launch_bounds__(256) k_conv3_in1(const float *in, const float *W, const float *bias,
+                                                   __nv_bfloat16 *out, int nx, int ny, int nz, int nb, int relu) {
+  conv3_in1_body<1>(in, W, bias, out, nx, ny, nz, nb, relu);
+}
+__global__ void __launch_bounds__(256, 2) k_conv3_in1x4(const float *in, const float *W, const float *bias,
+                                                     __nv_bfloat16 *out, int nx, int ny, int nz, int nb, int relu) {
+  conv3_in1_body<4>(in, W, bias, out, nx, ny, nz, nb, relu);
 }
 
 // ---- resampling (row-planar 16-channel tensors; fine dims nx, ny, nz even) -------------------

@@ -30,6 +30,8 @@ __global__ void k_flip_fp32(const float *W, int cin, int g, float *Wf);
 __global__ void k_conv3_cc(CcConvArgs a);
 __global__ void k_conv3_in1(const float *in, const float *W, const float *bias, __nv_bfloat16 *out, int nx, int ny,
                             int nz, int nb, int relu);
+__global__ void k_conv3_in1x4(const float *in, const float *W, const float *bias, __nv_bfloat16 *out, int nx, int ny,
+                              int nz, int nb, int relu);  // nx a multiple of 4
 __global__ void k_pool(const __nv_bfloat16 *in, __nv_bfloat16 *out, int nx, int ny, int nz, int nb);
 __global__ void k_upsample(const __nv_bfloat16 *in, __nv_bfloat16 *out, int nx, int ny, int nz, int nb);
 __global__ void k_pool_bwd(const float *dc, float *df, int nx, int ny, int nz, int nb);
