@@ -275,39 +275,47 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_brick(ConvArgs a) {
 struct RowUnits {
   int nxb, nchunks, nunits;
 };
+template <int RX>
 __host__ __device__ __forceinline__ RowUnits row_units(const ConvGeom &g) {
   RowUnits r;
-  r.nxb = g.nx / 128;
-  r.nchunks = (g.ny + kRowChunk - 1) / kRowChunk;
+  r.nxb = g.nx / RX;
+  r.nchunks = (g.ny + row_chunk(RX) - 1) / row_chunk(RX);
   r.nunits = r.nxb * g.nz * g.nb * r.nchunks;
   return r;
 }
 struct RowUnit {
   int b, z, x0, ya, yb;
 };
+template <int RX>
 __device__ __forceinline__ RowUnit row_unit(const ConvGeom &g, const RowUnits &ru, int u) {
   RowUnit w;
   const int c = u % ru.nchunks;
   int r = u / ru.nchunks;
-  w.x0 = (r % ru.nxb) * 128;
+  w.x0 = (r % ru.nxb) * RX;
   r /= ru.nxb;
   w.z = r % g.nz;
   w.b = r / g.nz;
-  w.ya = c * kRowChunk;
-  w.yb = min(g.ny, w.ya + kRowChunk);
+  w.ya = c * row_chunk(RX);
+  w.yb = min(g.ny, w.ya + row_chunk(RX));
   return w;
 }
-// Tile index (as tile_origin decodes it) of row y of a unit.
+// Tile index (as tile_origin decodes it, g.bx = RX) of row y of a unit.
+template <int RX>
 __device__ __forceinline__ int row_tile_index(const ConvGeom &g, const RowUnit &w, int y) {
-  return ((w.b * g.nz + w.z) * g.ny + y) * g.tx + w.x0 / 128;
+  return ((w.b * g.nz + w.z) * g.ny + y) * g.tx + w.x0 / RX;
 }
 
-template <int NIN, int EPI>
+// RX = 128: one TMEM lane per voxel.  RX = 64 (MMA M = 64): voxel row m of the
+// tile sits in TMEM lane (m / 16) * 32 + m % 16, i.e. lanes 0-15 of each
+// warp's quarter (checked on the GPU by dumping an M = 64 accumulator).
+template <int NIN, int EPI, int RX>
 __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];
   constexpr int kWBytes = NIN * 27 * kWTapBytes;
-  constexpr int kSlab = slab_bytes(NIN);
-  constexpr int R = row_slots(NIN);
+  constexpr int kSlab = slab_bytes(NIN, RX);
+  constexpr int R = row_slots(NIN, RX);
+  constexpr int kRowVox = row_vox(RX), kSlabPlaneBytes = slab_plane_bytes(RX);
+  static_assert(RX == 128 || RX == 64, "MMA M is 128 or 64");
   uint8_t *sW = smem;
   uint8_t *sA = smem + kWBytes;
   uint64_t *full = reinterpret_cast<uint64_t *>(sA + R * kSlab);
@@ -321,14 +329,14 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t tmem = conv_setup<NIN, R>(a, sW, full, slot, warp);
   const ConvGeom &g = a.g;
-  const RowUnits ru = row_units(g);
+  const RowUnits ru = row_units<RX>(g);
 
   if (warp == 0) {
     // fetch slabs ya-1 .. yb of every unit: NIN x 2 halves x 3 z-rows spans
     uint32_t sc = 0;
     bool ok = true;
     for (int u = blockIdx.x; u < ru.nunits && ok; u += gridDim.x) {
-      const RowUnit w = row_unit(g, ru, u);
+      const RowUnit w = row_unit<RX>(g, ru, u);
       for (int ys = w.ya - 1; ys <= w.yb; ++ys, ++sc) {
         const int s = sc % R;
         const uint32_t n = sc / R;
@@ -351,12 +359,12 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t idesc = idesc_bf16(128, 16);
+      constexpr uint32_t idesc = idesc_bf16(RX, 16);
       const uint64_t wd = smem_desc(sW, 256, 128);
       uint32_t sc0 = 0, tcount = 0;
       bool ok = true;
       for (int u = blockIdx.x; u < ru.nunits && ok; u += gridDim.x) {
-        const RowUnit w = row_unit(g, ru, u);
+        const RowUnit w = row_unit<RX>(g, ru, u);
         const int ntile = w.yb - w.ya;
         uint32_t ready = sc0;  // slabs [sc0, ready) have been waited for
         for (int i = 0; i < ntile; ++i, ++tcount) {
@@ -404,7 +412,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
       for (int c = 0; c < 17; ++c) proj[c] = a.proj[c];
     bool ok = true;
     for (int u = blockIdx.x; u < ru.nunits && ok; u += gridDim.x) {
-      const RowUnit w = row_unit(g, ru, u);
+      const RowUnit w = row_unit<RX>(g, ru, u);
       for (int y = w.ya; y < w.yb; ++y, ++tcount) {
         const int buf = tcount & 1;
         if (!(ok = mbar_wait(&acc_full[buf], (tcount >> 1) & 1, a.err, 14))) break;
@@ -414,7 +422,10 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&acc_empty[buf]);
-        conv_store<EPI>(a, row_tile_index(g, w, y), q * 32 + lane, v, bias, proj);
+        if (RX == 128)
+          conv_store<EPI>(a, row_tile_index<RX>(g, w, y), q * 32 + lane, v, bias, proj);
+        else if (lane < 16)
+          conv_store<EPI>(a, row_tile_index<RX>(g, w, y), q * 16 + lane, v, bias, proj);
       }
     }
   }
@@ -426,18 +437,20 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
   }
 }
 
-template <int NIN, int EPI, bool ROW>
+// RX = 0: brick tiles; 128 / 64: row tiles of that many voxels.
+template <int NIN, int EPI, int RX>
 static int launch_one(const ConvArgs &a, int num_sms, cudaStream_t s) {
-  constexpr int smem = ROW ? row_smem_bytes(NIN) : brick_smem_bytes(NIN);
+  constexpr bool ROW = RX != 0;
+  constexpr int smem = ROW ? row_smem_bytes(NIN, RX == 0 ? 128 : RX) : brick_smem_bytes(NIN);
   static_assert(smem <= 227 * 1024, "conv CTA exceeds the shared-memory limit");
-  auto kern = ROW ? k_conv3_row<NIN, EPI> : k_conv3_brick<NIN, EPI>;
+  auto kern = ROW ? k_conv3_row<NIN, EPI, RX == 0 ? 128 : RX> : k_conv3_brick<NIN, EPI>;
   static int per_sm = 0;
   if (!per_sm) {
     HPCCG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     // resident CTAs per SM by shared memory (each CTA also reserves 1 KB)
     per_sm = std::max(1, (227 * 1024) / (smem + 1024));
   }
-  const int work = ROW ? row_units(a.g).nunits : a.g.ntiles;
+  const int work = ROW ? row_units<RX == 0 ? 128 : RX>(a.g).nunits : a.g.ntiles;
   const int grid = std::min(work, num_sms * per_sm);
   kern<<<grid, kConvThreads, smem, s>>>(a);
   HPCCG_CUDA(cudaGetLastError());
@@ -445,12 +458,24 @@ static int launch_one(const ConvArgs &a, int num_sms, cudaStream_t s) {
 }
 
 template <int NIN, int EPI>
-static int launch_mode(const ConvArgs &a, int num_sms, cudaStream_t s, bool row) {
-  return row ? launch_one<NIN, EPI, true>(a, num_sms, s) : launch_one<NIN, EPI, false>(a, num_sms, s);
+static int launch_mode(const ConvArgs &a, int num_sms, cudaStream_t s, int rx) {
+  if (rx == 128) return launch_one<NIN, EPI, 128>(a, num_sms, s);
+  if (rx == 64) return launch_one<NIN, EPI, 64>(a, num_sms, s);
+  return launch_one<NIN, EPI, 0>(a, num_sms, s);
 }
 
-int launch_conv3_tc(int nin, int epi, const ConvArgs &a, int num_sms, cudaStream_t s, bool force_brick) {
-  const bool row = conv_row_ok(a.g) && !force_brick;
+int launch_conv3_tc(int nin, int epi, const ConvArgs &a_in, int num_sms, cudaStream_t s, bool force_brick) {
+  ConvArgs a = a_in;
+  int row = 0;
+  if (!force_brick) {
+    ConvGeom g64;
+    if (conv_row_ok(a.g)) {
+      row = 128;
+    } else if (conv_row64_geom(a.g, &g64)) {
+      a.g = g64;
+      row = 64;
+    }
+  }
   if (nin == 1) {
     switch (epi) {
       case kEpiBiasRelu: return launch_mode<1, kEpiBiasRelu>(a, num_sms, s, row);

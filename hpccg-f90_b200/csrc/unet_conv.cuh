@@ -41,23 +41,24 @@ constexpr int kWTapBytes = 16 * 16 * 2;  // one tap of B: 16 x 16 BF16
 // Brick tiles: one stage per k-step (tap, input): 2 halves x 128 units.
 constexpr int kBrickStages = 24;
 constexpr int kBrickStageBytes = 2 * 128 * 16;
-// Row tiles (nx a multiple of 128) walk y inside a work unit (b, z, 128-voxel
-// x block, chunk of up to kRowChunk rows of y).  A "slab" is grid row y of the
-// three z planes z-1, z, z+1 with a 1-voxel x halo: 3 rows x 130 units per
-// half.  Tile y reads slabs y-1, y, y+1, so each tile fetches one new slab and
-// a ring of kRowSlots slabs keeps several fetches in flight.
-constexpr int kRowVox = 130;
-constexpr int kRowChunk = 32;
-constexpr int kSlabPlaneBytes = ((3 * kRowVox * 16 + 127) / 128) * 128;
-__host__ __device__ constexpr int slab_bytes(int nin) { return nin * 2 * kSlabPlaneBytes; }
-__host__ __device__ constexpr int row_slots(int nin) { return nin == 1 ? 8 : 6; }
+// Row tiles of RX = 128 voxels (nx a multiple of 128; MMA M = 128) or RX = 64
+// (nx = 64; M = 64) walk y inside a work unit (b, z, RX-voxel x block, chunk of
+// up to row_chunk(RX) rows of y).  A "slab" is grid row y of the three z planes
+// z-1, z, z+1 with a 1-voxel x halo: 3 rows x (RX + 2) units per half.  Tile y
+// reads slabs y-1, y, y+1, so each tile fetches one new slab and a ring of
+// row_slots slabs keeps several fetches in flight.
+__host__ __device__ constexpr int row_vox(int rx) { return rx + 2; }
+__host__ __device__ constexpr int row_chunk(int rx) { return rx == 128 ? 32 : 8; }
+__host__ __device__ constexpr int slab_plane_bytes(int rx) { return ((3 * row_vox(rx) * 16 + 127) / 128) * 128; }
+__host__ __device__ constexpr int slab_bytes(int nin, int rx) { return nin * 2 * slab_plane_bytes(rx); }
+__host__ __device__ constexpr int row_slots(int nin, int rx) { return (rx == 128 && nin == 1) ? 8 : 6; }
 // mbarriers: full[S], empty[S], acc_full[2], acc_empty[2], drain, + TMEM slot.
 __host__ __device__ constexpr int bar_bytes(int stages) { return (2 * stages + 5) * 8 + 16; }
 __host__ __device__ constexpr int brick_smem_bytes(int nin) {
   return nin * 27 * kWTapBytes + kBrickStages * kBrickStageBytes + bar_bytes(kBrickStages);
 }
-__host__ __device__ constexpr int row_smem_bytes(int nin) {
-  return nin * 27 * kWTapBytes + row_slots(nin) * slab_bytes(nin) + bar_bytes(row_slots(nin));
+__host__ __device__ constexpr int row_smem_bytes(int nin, int rx) {
+  return nin * 27 * kWTapBytes + row_slots(nin, rx) * slab_bytes(nin, rx) + bar_bytes(row_slots(nin, rx));
 }
 
 enum ConvEpi : int {
@@ -106,6 +107,19 @@ inline bool conv_geom(int nx, int ny, int nz, int nb, ConvGeom *g) {
   return true;
 }
 inline bool conv_row_ok(const ConvGeom &g) { return g.bx == 128 && g.by == 1 && g.bz == 1; }
+// Geometry of 64-voxel row tiles for nx = 64 (tile = one grid row).
+inline bool conv_row64_geom(const ConvGeom &g, ConvGeom *r) {
+  if (g.nx != 64) return false;
+  *r = g;
+  r->bx = 64;
+  r->by = 1;
+  r->bz = 1;
+  r->tx = 1;
+  r->ty = g.ny;
+  r->tz = g.nz;
+  r->ntiles = g.ny * g.nz * g.nb;
+  return true;
+}
 
 // Launches the tensor-core conv (row tiles when possible unless force_brick).
 int launch_conv3_tc(int nin, int epi, const ConvArgs &a, int num_sms, cudaStream_t s, bool force_brick = false);
