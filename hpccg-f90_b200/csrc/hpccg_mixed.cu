@@ -538,7 +538,15 @@ static int launch_inner_body(hpccg_ctx *c, MixedRes *m, int precision, const Mix
 }
 
 static int launch_residual64(hpccg_ctx *c, const MixedArgs &g, cudaStream_t s) {
-  const SpmvArgs a = spmv_args(c);
+  SpmvArgs a = spmv_args(c);
+  if (a.kind == HPCCG_SPMV_STENCIL) {  // the FP64 box walk, four columns per thread
+    const PlaneMap q = boxw_map(4, c->gx, c->gy, c->gz, (int64_t)c->num_sms * StratStencilBox64::kMinBlocks * kBlock);
+    if (q.plane > 0) {
+      a.pm = q;
+      k_mp_residual64<StratStencilBox64><<<StratStencilBox64::grid(a, c->grid), kBlock, 0, s>>>(a, g);
+      return (int)cudaGetLastError();
+    }
+  }
   return dispatch_strategy(a, [&](auto strat) {
     using St = decltype(strat);
     k_mp_residual64<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, g);

@@ -229,6 +229,17 @@ struct StratStencil {
   }
 };
 
+// FP64 box walk with four columns per thread (the outer residual of the
+// refinement; a.pm must be a boxw_map(4, ...) map).
+struct StratStencilBox64 {
+  static constexpr int kMinBlocks = 2;
+  static int grid(const SpmvArgs &a, int dflt) { return plane_or(a.pm, dflt); }
+  template <class Epi>
+  static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
+    return stencil_rows_box64x4(a.geom, a.pm, x, e);
+  }
+};
+
 // Resident-block hints offered for the ELL strategies (the `param` of
 // hpccg_gpu_set_spmv for HPCCG_SPMV_ELL / HPCCG_SPMV_ELL2).
 constexpr int kEllMinBlocks[4] = {2, 3, 4, 8};

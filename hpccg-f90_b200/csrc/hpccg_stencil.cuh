@@ -295,6 +295,65 @@ __device__ __forceinline__ double stencil_rows_boxw(const StencilGeom &g, const 
   return part;
 }
 
+// FP64 box walk, four columns per thread (map from boxw_map(4, ...)), for the
+// outer residual of the refinement: the same reassociated sum as the FP32 box
+// walk in double precision (not the reference's term order).
+template <class Epi>
+__device__ __forceinline__ double stencil_rows_box64x4(const StencilGeom &g, const PlaneMap &q,
+                                                       const double *__restrict__ x, Epi &epi) {
+  double part = 0.0;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)q.plane * q.nzc) return part;
+  const int qz = (int)(t / q.plane);
+  const int c0 = 4 * (int)(t - (int64_t)qz * q.plane);
+  const int z0 = qz * q.zc, z1 = min(g.nz, z0 + q.zc);
+  const int iy = c0 / g.nx, ix0 = c0 - iy * g.nx;
+  const int plane = 4 * q.plane;
+  const int dl = ix0 > 0 ? -1 : 0, dr = ix0 + 4 < g.nx ? 4 : 3;
+  const double wl = ix0 > 0 ? 1.0 : 0.0, wr = ix0 + 4 < g.nx ? 1.0 : 0.0;
+  const int ylo = iy > 0 ? -g.nx : 0, yhi = iy < g.ny - 1 ? g.nx : 0;
+  const double wlo = iy > 0 ? 1.0 : 0.0, whi = iy < g.ny - 1 ? 1.0 : 0.0;
+  const double *pc = x + c0;
+  auto line = [&](const double *p, double *v, double *s) {
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(p));
+    const double2 b = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = b.x;
+    v[3] = b.y;
+    const double l = wl * __ldg(p + dl), r = wr * __ldg(p + dr);
+    s[0] = (l + v[0]) + v[1];
+    s[1] = (v[0] + v[1]) + v[2];
+    s[2] = (v[1] + v[2]) + v[3];
+    s[3] = (v[2] + v[3]) + r;
+  };
+  auto box = [&](int z, double *bx, double *v) {
+    const bool zin = (unsigned)z < (unsigned)g.nz;
+    const double *p = pc + (int64_t)(zin ? z : 0) * plane;
+    double s0[4], s1[4], s2[4], u[4];
+    line(p + ylo, u, s0);
+    line(p, v, s1);
+    line(p + yhi, u, s2);
+    const double wz = zin ? 1.0 : 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) bx[j] = wz * fma(wlo, s0[j], fma(whi, s2[j], s1[j]));
+  };
+  double bm[4], b0[4], bp[4], vm[4], v0[4], vp[4];
+  box(z0 - 1, bm, vm);
+  box(z0, b0, v0);
+  for (int z = z0; z < z1; ++z) {
+    box(z + 1, bp, vp);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      part += epi(c0 + j + z * plane, fma(28.0, v0[j], -((bm[j] + b0[j]) + bp[j])));
+      bm[j] = b0[j];
+      b0[j] = bp[j];
+      v0[j] = vp[j];
+    }
+  }
+  return part;
+}
+
 // All rows of the calling thread; epi(i, rowsum) stores and returns a dot term.
 template <typename Real, class Epi>
 __device__ __forceinline__ double stencil_rows(int n, const StencilGeom &g, const PlaneMap &m,
