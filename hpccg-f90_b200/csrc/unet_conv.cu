@@ -157,6 +157,39 @@ __device__ __forceinline__ uint32_t conv_setup(const ConvArgs &a, uint8_t *sW, u
   return *slot;
 }
 
+// Set-up of the row kernel: weights, the barriers of each of the P pipelines
+// (pipeline p starts at rings + p*pipe_bytes; its 2R+5 barriers follow its ring
+// of ring_bytes), and
+// 32*P TMEM columns allocated by warp 1; the TMEM base lands in *slot.
+template <int NIN, int R, int P>
+__device__ __forceinline__ uint32_t conv_setup_row(const ConvArgs &a, uint8_t *sW, uint8_t *rings, int ring_bytes,
+                                                   int pipe_bytes, uint32_t *slot, int warp) {
+  constexpr int kWBytes = NIN * 27 * kWTapBytes;
+  for (int i = threadIdx.x; i < kWBytes / 16; i += blockDim.x)
+    reinterpret_cast<uint4 *>(sW)[i] = reinterpret_cast<const uint4 *>(a.wpack)[i];
+  if (threadIdx.x == 0) {
+    for (int p = 0; p < P; ++p) {
+      uint64_t *bars = reinterpret_cast<uint64_t *>(rings + p * pipe_bytes + ring_bytes);
+      for (int s = 0; s < 2 * R; ++s) mbar_init(&bars[s], 1);
+      mbar_init(&bars[2 * R + 0], 1);
+      mbar_init(&bars[2 * R + 1], 1);
+      mbar_init(&bars[2 * R + 2], 4);
+      mbar_init(&bars[2 * R + 3], 4);
+      mbar_init(&bars[2 * R + 4], 1);
+    }
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    tmem_alloc(slot, 32 * P);
+    tmem_relinquish();
+  }
+  fence_proxy_async_smem();  // weights -> tensor-core proxy
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  return *slot;
+}
+
 // Epilogue role (warps 2-5): drain each tile's accumulator and store it.
 template <int EPI>
 __device__ __forceinline__ void conv_epilogue(const ConvArgs &a, uint64_t *acc_full, uint64_t *acc_empty,
@@ -309,33 +342,41 @@ __device__ __forceinline__ int row_tile_index(const ConvGeom &g, const RowUnit &
 // tile sits in TMEM lane (m / 16) * 32 + m % 16, i.e. lanes 0-15 of each
 // warp's quarter (checked on the GPU by dumping an M = 64 accumulator).
 template <int NIN, int EPI, int RX>
-__global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
+__global__ void __launch_bounds__(kConvThreads * row_pipes(NIN, RX), 1) k_conv3_row(ConvArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];
+  constexpr int P = row_pipes(NIN, RX);
   constexpr int kWBytes = NIN * 27 * kWTapBytes;
   constexpr int kSlab = slab_bytes(NIN, RX);
-  constexpr int R = row_slots(NIN, RX);
+  constexpr int R = row_slots(NIN, RX, P);
   constexpr int kRowVox = row_vox(RX), kSlabPlaneBytes = slab_plane_bytes(RX);
   static_assert(RX == 128 || RX == 64, "MMA M is 128 or 64");
+  static_assert((2 * R + 5) * 8 + 4 <= bar_bytes(R), "barrier area");
+  static_assert(R >= 4, "the window needs the three slabs of a tile plus one in flight");
+  constexpr int kPipeBytes = row_pipe_bytes(NIN, RX);
+  static_assert(R * kSlab + bar_bytes(R) <= kPipeBytes && kPipeBytes % 128 == 0, "shared memory plan");
+  // pipeline `pipe` = warps 6*pipe .. 6*pipe+5 in the roles producer, MMA, 4 x epilogue;
+  // it owns units blockIdx.x + (k*P + pipe)*gridDim.x, its slab ring, its barriers
+  // and TMEM columns 32*pipe .. +31
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pipe = warp / 6, role = warp % 6;
   uint8_t *sW = smem;
-  uint8_t *sA = smem + kWBytes;
+  uint8_t *sA = smem + kWBytes + pipe * kPipeBytes;
   uint64_t *full = reinterpret_cast<uint64_t *>(sA + R * kSlab);
   uint64_t *empty = full + R;
   uint64_t *acc_full = empty + R;
   uint64_t *acc_empty = acc_full + 2;
   uint64_t *drain = acc_empty + 2;
-  uint32_t *slot = reinterpret_cast<uint32_t *>(drain + 1);
-  static_assert((2 * R + 5) * 8 + 4 <= bar_bytes(R), "barrier area");
-  static_assert(R >= 4, "the window needs the three slabs of a tile plus one in flight");
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t tmem = conv_setup<NIN, R>(a, sW, full, slot, warp);
+  uint32_t *slot = reinterpret_cast<uint32_t *>(smem + kWBytes + R * kSlab + 2 * R * 8 + 5 * 8);  // pipeline 0's
+  const uint32_t tmem = conv_setup_row<NIN, R, P>(a, sW, smem + kWBytes, R * kSlab, kPipeBytes, slot, warp) + 32 * pipe;
   const ConvGeom &g = a.g;
   const RowUnits ru = row_units<RX>(g);
+  const int u0 = blockIdx.x + pipe * gridDim.x, ustep = P * gridDim.x;
 
-  if (warp == 0) {
+  if (role == 0) {
     // fetch slabs ya-1 .. yb of every unit: NIN x 2 halves x 3 z-rows spans
     uint32_t sc = 0;
     bool ok = true;
-    for (int u = blockIdx.x; u < ru.nunits && ok; u += gridDim.x) {
+    for (int u = u0; u < ru.nunits && ok; u += ustep) {
       const RowUnit w = row_unit<RX>(g, ru, u);
       for (int ys = w.ya - 1; ys <= w.yb; ++ys, ++sc) {
         const int s = sc % R;
@@ -357,13 +398,13 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
       const uint32_t first = sc > (uint32_t)R ? sc - R : 0;
       for (uint32_t j = first; j < sc; ++j) mbar_wait(&full[j % R], (j / R) & 1, a.err, 15);
     }
-  } else if (warp == 1) {
+  } else if (role == 1) {
     if (lane == 0) {
       constexpr uint32_t idesc = idesc_bf16(RX, 16);
       const uint64_t wd = smem_desc(sW, 256, 128);
       uint32_t sc0 = 0, tcount = 0;
       bool ok = true;
-      for (int u = blockIdx.x; u < ru.nunits && ok; u += gridDim.x) {
+      for (int u = u0; u < ru.nunits && ok; u += ustep) {
         const RowUnit w = row_unit<RX>(g, ru, u);
         const int ntile = w.yb - w.ya;
         uint32_t ready = sc0;  // slabs [sc0, ready) have been waited for
@@ -411,7 +452,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
 #pragma unroll
       for (int c = 0; c < 17; ++c) proj[c] = a.proj[c];
     bool ok = true;
-    for (int u = blockIdx.x; u < ru.nunits && ok; u += gridDim.x) {
+    for (int u = u0; u < ru.nunits && ok; u += ustep) {
       const RowUnit w = row_unit<RX>(g, ru, u);
       for (int y = w.ya; y < w.yb; ++y, ++tcount) {
         const int buf = tcount & 1;
@@ -433,7 +474,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv3_row(ConvArgs a) {
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem, 32);
+    tmem_dealloc(tmem - 32 * pipe, 32 * P);
   }
 }
 
@@ -450,9 +491,10 @@ static int launch_one(const ConvArgs &a, int num_sms, cudaStream_t s) {
     // resident CTAs per SM by shared memory (each CTA also reserves 1 KB)
     per_sm = std::max(1, (227 * 1024) / (smem + 1024));
   }
+  constexpr int pipes = ROW ? row_pipes(NIN, RX == 0 ? 128 : RX) : 1;
   const int work = ROW ? row_units<RX == 0 ? 128 : RX>(a.g).nunits : a.g.ntiles;
-  const int grid = std::min(work, num_sms * per_sm);
-  kern<<<grid, kConvThreads, smem, s>>>(a);
+  const int grid = std::min((work + pipes - 1) / pipes, num_sms * per_sm);
+  kern<<<grid, kConvThreads * pipes, smem, s>>>(a);
   HPCCG_CUDA(cudaGetLastError());
   return HPCCG_OK;
 }

@@ -51,14 +51,27 @@ __host__ __device__ constexpr int row_vox(int rx) { return rx + 2; }
 __host__ __device__ constexpr int row_chunk(int rx) { return rx == 128 ? 32 : 8; }
 __host__ __device__ constexpr int slab_plane_bytes(int rx) { return ((3 * row_vox(rx) * 16 + 127) / 128) * 128; }
 __host__ __device__ constexpr int slab_bytes(int nin, int rx) { return nin * 2 * slab_plane_bytes(rx); }
-__host__ __device__ constexpr int row_slots(int nin, int rx) { return (rx == 128 && nin == 1) ? 8 : 6; }
+__host__ __device__ constexpr int row_slots(int nin, int rx, int pipes = 1) {
+  return pipes == 2 ? 4 : ((rx == 128 && nin == 1) ? 8 : 6);
+}
+// Row kernels may run two independent pipelines (producer, MMA issuer and
+// epilogue warps each, own slab ring and accumulators) in one CTA that shares
+// the weights: two MMA-issuing threads per SM where the shared memory of one
+// pipeline per CTA leaves room for only one CTA.
+__host__ __device__ constexpr int row_pipes(int nin, int rx) { return (nin == 2 && rx == 128) ? 2 : 1; }
 // mbarriers: full[S], empty[S], acc_full[2], acc_empty[2], drain, + TMEM slot.
 __host__ __device__ constexpr int bar_bytes(int stages) { return (2 * stages + 5) * 8 + 16; }
 __host__ __device__ constexpr int brick_smem_bytes(int nin) {
   return nin * 27 * kWTapBytes + kBrickStages * kBrickStageBytes + bar_bytes(kBrickStages);
 }
+// One pipeline's ring and barriers, rounded up so that the next ring starts on
+// a 128-byte boundary (bulk copies and MMA operands need 16-byte alignment).
+__host__ __device__ constexpr int row_pipe_bytes(int nin, int rx) {
+  return ((row_slots(nin, rx, row_pipes(nin, rx)) * slab_bytes(nin, rx) +
+           bar_bytes(row_slots(nin, rx, row_pipes(nin, rx))) + 127) / 128) * 128;
+}
 __host__ __device__ constexpr int row_smem_bytes(int nin, int rx) {
-  return nin * 27 * kWTapBytes + row_slots(nin, rx) * slab_bytes(nin, rx) + bar_bytes(row_slots(nin, rx));
+  return nin * 27 * kWTapBytes + row_pipes(nin, rx) * row_pipe_bytes(nin, rx);
 }
 
 enum ConvEpi : int {
