@@ -9,18 +9,19 @@
 // are the two K chunks).  So every operand tile arrives by 1D bulk copies
 // (cp.async.bulk) of whole row spans, with zero fill at the grid faces.
 //
-// A conv is an implicit GEMM per tile of 128 voxels (one TMEM lane each):
-// for each of the 27 taps and each 16-channel input group, one tcgen05.mma
-// (M=128, N=16, K=16) accumulates into a 16-column FP32 TMEM accumulator.
-//  * row tiles (nx a multiple of 128): a tile is one 128-voxel x-row; the
-//    3x3 neighbouring rows with a 1-voxel x halo are three "slabs" shared with
-//    the neighbouring tiles in y, and the 27 taps read them through shifted
-//    descriptors (one new slab fetched per tile);
-//  * brick tiles (smaller nx): a tile is a bx*by*bz brick and each tap's
-//    shifted brick is fetched separately (by*bz row spans per half).
-// Roles per CTA (192 threads): warp 0 fetches (its lanes issue the row spans
-// in parallel), warp 1 allocates TMEM and lane 0 issues the MMAs, warps 2-5
-// (one per TMEM lane quarter) run the epilogue.
+// A conv is an implicit GEMM per tile of 128 (or 64) voxels: for each of the
+// 27 taps and each 16-channel input group, one tcgen05.mma (M=128 or 64,
+// N=16, K=16) accumulates into a 16-column FP32 TMEM accumulator.
+//  * row tiles (nx a multiple of 128, or nx = 64 with M = 64): a tile is one
+//    x-row; the 3x3 neighbouring rows with a 1-voxel x halo are three "slabs"
+//    shared with the neighbouring tiles in y, and the 27 taps read them through
+//    shifted descriptors (one new slab fetched per tile);
+//  * brick tiles (other narrow grids): a tile is a bx*by*bz brick of 128
+//    voxels and each tap's shifted brick is fetched separately.
+// Roles per pipeline (192 threads): warp 0 fetches (its lanes issue the row
+// spans in parallel), warp 1 allocates TMEM and lane 0 issues the MMAs, warps
+// 2-5 (one per TMEM lane quarter) run the epilogue.  Row kernels of 32-channel
+// layers run two such pipelines per CTA (384 threads) that share the weights.
 #pragma once
 #include "hpccg_internal.cuh"
 #include "unet_tc.cuh"
