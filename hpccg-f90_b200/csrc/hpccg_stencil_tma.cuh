@@ -1,11 +1,11 @@
 // hpccg_stencil_tma.cuh -- the FP32 matrix-free SpMV of the inner solves with
-// its input streamed by TMA: a CTA owns a 32 x 32 tile of grid columns and a
+// its input streamed by TMA: a CTA owns a 32 x 64 tile of grid columns and a
 // chunk of z planes; one thread issues 3D tensor loads of the tile with its
-// halo (40 x 34 floats, the x start rounded down to a 16-byte boundary) into a
+// halo (40 x 66 floats, the x start rounded down to a 16-byte boundary) into a
 // ring of kTmaStages shared-memory slots, kTmaStages planes ahead of the row
 // being summed.  Planes and rows outside the grid arrive as zeros (tensor-map
 // out-of-bounds fill), so the sums need no masks.  Each thread forms the 3x3
-// box sums of its 4 columns from shared memory, keeps three planes of box sums
+// box sums of its 4 x 2 columns from shared memory (4 grid lines serve both rows), keeps three planes of box sums
 // in registers and writes y_i = 28 x_i - (box(z-1) + box(z) + box(z+1)), the
 // same reassociated FP32 sum as stencil_rows_boxw.
 //
@@ -20,13 +20,14 @@
 
 namespace hpccg {
 
-constexpr int kTmaTileX = 32, kTmaTileY = 32;           // columns per CTA
+constexpr int kTmaRows = 2;                             // grid rows (y) per thread
+constexpr int kTmaTileX = 32, kTmaTileY = 32 * kTmaRows;  // columns per CTA
 constexpr int kTmaBoxX = kTmaTileX + 8;                 // x0-4 .. x0+35 (16-byte aligned start)
-constexpr int kTmaBoxY = kTmaTileY + 2;                 // y0-1 .. y0+32
+constexpr int kTmaBoxY = kTmaTileY + 2;                 // y0-1 .. y0+TY
 constexpr int kTmaSlotFloats = ((kTmaBoxX * kTmaBoxY * 4 + 127) / 128) * 128 / 4;
-constexpr int kTmaStages = 8;
+constexpr int kTmaStages = 4;
 constexpr uint32_t kTmaBoxBytes = kTmaBoxX * kTmaBoxY * 4;
-static_assert(kBlock == (kTmaTileX / 4) * kTmaTileY, "one thread per 4 columns of the tile");
+static_assert(kBlock == (kTmaTileX / 4) * (kTmaTileY / kTmaRows), "one thread per 4 x kTmaRows columns");
 
 struct TmaTile {
   int nx, ny, nz;
@@ -77,8 +78,7 @@ __device__ __forceinline__ double stencil_rows_tma(const TmaTile &t, const CUten
   const int q = blockIdx.x / per_plane, tile = blockIdx.x - q * per_plane;
   const int x0 = (tile % t.tiles_x) * kTmaTileX, y0 = (tile / t.tiles_x) * kTmaTileY;
   const int z0 = q * t.zc, z1 = min(t.nz, z0 + t.zc);
-  const int xc = x0 + 4 * tx, yc = y0 + ty;
-  const bool active = xc < t.nx && yc < t.ny;
+  const int xc = x0 + 4 * tx, yc = y0 + kTmaRows * ty;  // rows yc .. yc + kTmaRows - 1
   const int64_t plane = (int64_t)t.nx * t.ny;
   if (tid == 0) {
     for (int s = 0; s < kTmaStages; ++s) tc::mbar_init(&full[s], 1);
@@ -96,8 +96,8 @@ __device__ __forceinline__ double stencil_rows_tma(const TmaTile &t, const CUten
   int next = z0 - 1;  // next plane to load (thread 0's view)
   if (tid == 0)
     for (; next <= z1 && next < z0 - 1 + kTmaStages; ++next) issue(next);
-  // box sums (and centres) of plane p for this thread's 4 columns
-  auto consume = [&](int p, float *b, float4 &v) -> bool {
+  // box sums (and centres) of plane p for this thread's 4 x kTmaRows columns
+  auto consume = [&](int p, float (*b)[4], float4 *v) -> bool {
     const int s = slot_of(p);
     const uint32_t parity = (uint32_t)((p - z0 + 1) / kTmaStages) & 1u;
     bool ok = true;
@@ -113,21 +113,24 @@ __device__ __forceinline__ double stencil_rows_tma(const TmaTile &t, const CUten
       if (status) atomicCAS(status, 0, HPCCG_ERR_TIMEOUT);
       return false;
     }
-    const float *c = ring + s * kTmaSlotFloats + (ty + 1) * kTmaBoxX + 4 + 4 * tx;
-    float sum[4] = {0.f, 0.f, 0.f, 0.f};
+    // 3-point line sums of the kTmaRows + 2 grid lines yc-1 .. yc+kTmaRows (box rows kTmaRows*ty ..)
+    const float *c = ring + s * kTmaSlotFloats + (kTmaRows * ty) * kTmaBoxX + 4 + 4 * tx;
+    float ls[kTmaRows + 2][4];
 #pragma unroll
-    for (int dy = -1; dy <= 1; ++dy) {
-      const float *r = c + dy * kTmaBoxX;
+    for (int k = 0; k < kTmaRows + 2; ++k) {
+      const float *r = c + k * kTmaBoxX;
       const float4 m = *reinterpret_cast<const float4 *>(r);
       const float l = r[-1], rr = r[4];
-      if (dy == 0) v = m;
-      sum[0] += (l + m.x) + m.y;
-      sum[1] += (m.x + m.y) + m.z;
-      sum[2] += (m.y + m.z) + m.w;
-      sum[3] += (m.z + m.w) + rr;
+      if (k >= 1 && k <= kTmaRows) v[k - 1] = m;
+      ls[k][0] = (l + m.x) + m.y;
+      ls[k][1] = (m.x + m.y) + m.z;
+      ls[k][2] = (m.y + m.z) + m.w;
+      ls[k][3] = (m.z + m.w) + rr;
     }
 #pragma unroll
-    for (int j = 0; j < 4; ++j) b[j] = sum[j];
+    for (int j = 0; j < kTmaRows; ++j)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) b[j][i] = (ls[j][i] + ls[j + 1][i]) + ls[j + 2][i];
     return true;
   };
   // after every thread has read plane p its slot takes plane p + S
@@ -140,8 +143,8 @@ __device__ __forceinline__ double stencil_rows_tma(const TmaTile &t, const CUten
     }
     return !failed;
   };
-  float bm[4], b0[4], bp[4];
-  float4 vm, v0, vp;
+  float bm[kTmaRows][4], b0[kTmaRows][4], bp[kTmaRows][4];
+  float4 vm[kTmaRows], v0[kTmaRows], vp[kTmaRows];
   int consumed = z0 - 2;  // last plane consumed by every thread
   bool ok = consume(z0 - 1, bm, vm);
   if (release() && ok) {
@@ -153,20 +156,23 @@ __device__ __forceinline__ double stencil_rows_tma(const TmaTile &t, const CUten
         ok = consume(z + 1, bp, vp);
         if (!release() || !ok) break;
         consumed = z + 1;
-        if (active) {
-          float4 y;
-          y.x = fmaf(28.f, v0.x, -((bm[0] + b0[0]) + bp[0]));
-          y.y = fmaf(28.f, v0.y, -((bm[1] + b0[1]) + bp[1]));
-          y.z = fmaf(28.f, v0.z, -((bm[2] + b0[2]) + bp[2]));
-          y.w = fmaf(28.f, v0.w, -((bm[3] + b0[3]) + bp[3]));
-          part += epi.store4((int)(z * plane + (int64_t)yc * t.nx + xc), y, v0);
-        }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          bm[j] = b0[j];
-          b0[j] = bp[j];
+        for (int j = 0; j < kTmaRows; ++j) {
+          if (xc < t.nx && yc + j < t.ny) {
+            float4 y;
+            y.x = fmaf(28.f, v0[j].x, -((bm[j][0] + b0[j][0]) + bp[j][0]));
+            y.y = fmaf(28.f, v0[j].y, -((bm[j][1] + b0[j][1]) + bp[j][1]));
+            y.z = fmaf(28.f, v0[j].z, -((bm[j][2] + b0[j][2]) + bp[j][2]));
+            y.w = fmaf(28.f, v0[j].w, -((bm[j][3] + b0[j][3]) + bp[j][3]));
+            part += epi.store4((int)(z * plane + (int64_t)(yc + j) * t.nx + xc), y, v0[j]);
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            bm[j][i] = b0[j][i];
+            b0[j][i] = bp[j][i];
+          }
+          v0[j] = vp[j];
         }
-        v0 = vp;
       }
     }
   }
