@@ -349,7 +349,10 @@ int make_stencil_tmap(CUtensorMap *map, const float *base, int nx, int ny, int n
 static TmaTile tma_plan(const hpccg_ctx *c) {
   static int per_sm = 0;
   if (!per_sm) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_spmv_dot_tma, kBlock, 0) != cudaSuccess ||
+    cudaFuncSetAttribute(k_mp_spmv_dot_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaRingBytes);
+    cudaFuncSetAttribute(k_spmv_lp_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaRingBytes);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_spmv_dot_tma, kBlock, kTmaRingBytes) !=
+            cudaSuccess ||
         per_sm < 1)
       per_sm = 1;
   }
@@ -522,7 +525,7 @@ static MixedArgs mixed_args(hpccg_ctx *c, MixedRes *m, int precision) {
 static int launch_inner_body(hpccg_ctx *c, MixedRes *m, int precision, const MixedArgs &g, cudaStream_t s) {
   k_mp_update_p<<<c->grid, kBlock, 0, s>>>(g);
   if (use_tma(c, m)) {
-    k_mp_spmv_dot_tma<<<tma_tile_grid(m->tile), kBlock, 0, s>>>(g, m->tile, m->pmap);
+    k_mp_spmv_dot_tma<<<tma_tile_grid(m->tile), kBlock, kTmaRingBytes, s>>>(g, m->tile, m->pmap);
     k_mp_update_r<<<c->grid, kBlock, 0, s>>>(g);
     return (int)cudaGetLastError();
   }
@@ -759,7 +762,7 @@ extern "C" int hpccg_gpu_spmv_lowp(hpccg_ctx *c, int32_t precision, const float 
     CUtensorMap xmap;
     if (make_stencil_tmap(&xmap, d_x, c->gx, c->gy, c->gz) == HPCCG_OK) {
       HPCCG_CUDA(cudaMemsetAsync(&m->st->status, 0, sizeof(int), c->stream));
-      k_spmv_lp_tma<<<tma_tile_grid(m->tile), kBlock, 0, c->stream>>>(m->tile, xmap, d_y, &m->st->status);
+      k_spmv_lp_tma<<<tma_tile_grid(m->tile), kBlock, kTmaRingBytes, c->stream>>>(m->tile, xmap, d_y, &m->st->status);
       HPCCG_CUDA(cudaGetLastError());
       int status = 0;
       HPCCG_CUDA(cudaMemcpyAsync(&status, &m->st->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -809,7 +812,7 @@ extern "C" int hpccg_gpu_time_mixed_kernels(hpccg_ctx *c, int32_t precision, int
       if (which == 0) {
         k_mp_update_p<<<c->grid, kBlock, 0, c->stream>>>(g);
       } else if (which == 1 && use_tma(c, m)) {
-        k_mp_spmv_dot_tma<<<tma_tile_grid(m->tile), kBlock, 0, c->stream>>>(g, m->tile, m->pmap);
+        k_mp_spmv_dot_tma<<<tma_tile_grid(m->tile), kBlock, kTmaRingBytes, c->stream>>>(g, m->tile, m->pmap);
       } else if (which == 1) {
         dispatch_lp(uses_stencil(c), precision, m->rpt[precision], [&](auto strat, auto *vt) {
           using St = decltype(strat);

@@ -25,7 +25,8 @@ constexpr int kTmaTileX = 32, kTmaTileY = 32 * kTmaRows;  // columns per CTA
 constexpr int kTmaBoxX = kTmaTileX + 8;                 // x0-4 .. x0+35 (16-byte aligned start)
 constexpr int kTmaBoxY = kTmaTileY + 2;                 // y0-1 .. y0+TY
 constexpr int kTmaSlotFloats = ((kTmaBoxX * kTmaBoxY * 4 + 127) / 128) * 128 / 4;
-constexpr int kTmaStages = 4;
+constexpr int kTmaStages = 6;
+constexpr int kTmaRingBytes = kTmaStages * kTmaSlotFloats * 4;  // dynamic shared memory of the kernels
 constexpr uint32_t kTmaBoxBytes = kTmaBoxX * kTmaBoxY * 4;
 static_assert(kBlock == (kTmaTileX / 4) * (kTmaTileY / kTmaRows), "one thread per 4 x kTmaRows columns");
 
@@ -69,7 +70,8 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 template <class Epi>
 __device__ __forceinline__ double stencil_rows_tma(const TmaTile &t, const CUtensorMap *map, Epi &epi,
                                                    int *status) {
-  __shared__ __align__(128) float ring[kTmaStages * kTmaSlotFloats];
+  extern __shared__ __align__(128) unsigned char tma_ring[];  // kTmaRingBytes
+  float *ring = reinterpret_cast<float *>(tma_ring);
   __shared__ uint64_t full[kTmaStages];
   __shared__ int s_fail;
   double part = 0.0;
