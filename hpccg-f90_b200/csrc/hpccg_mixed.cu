@@ -347,15 +347,19 @@ int make_stencil_tmap(CUtensorMap *map, const float *base, int nx, int ny, int n
 
 // Plan of the TMA SpMV for a context (nzc = 0: not usable).
 static TmaTile tma_plan(const hpccg_ctx *c) {
-  static int per_sm = 0;
-  if (!per_sm) {
-    cudaFuncSetAttribute(k_mp_spmv_dot_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaRingBytes);
-    cudaFuncSetAttribute(k_spmv_lp_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaRingBytes);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_spmv_dot_tma, kBlock, kTmaRingBytes) !=
-            cudaSuccess ||
-        per_sm < 1)
-      per_sm = 1;
+  // the attribute is per device: set it for the context's device every time
+  if (cudaFuncSetAttribute(k_mp_spmv_dot_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaRingBytes) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_spmv_lp_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaRingBytes) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return TmaTile{c->gx, c->gy, c->gz, 0, 0, 0, 0};  // not usable: the register walk runs instead
   }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_spmv_dot_tma, kBlock, kTmaRingBytes) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
   return tma_tile_plan(c->gx, c->gy, c->gz, c->num_sms * per_sm);
 }
 
