@@ -22,6 +22,7 @@
 
 #include "hpccg_rows.cuh"
 #include "hpccg_rows_lp.cuh"
+#include "hpccg_iter_tma.cuh"
 #include "hpccg_stencil_tma.cuh"
 
 namespace hpccg {
@@ -29,8 +30,11 @@ namespace hpccg {
 struct MixedState {
   double bb, rr64, scale, rel_tol, relres, target, inner_rtol, inner_floor;
   double rtrans, rr0, alpha, beta;
+  double pAp, rAp, ApAp;  // dots of the last fused pass
   int outer, max_outer, inner_k, max_inner, inner_total, status, pending, inner_break;
-  int cont_outer, cont_inner, pad[2];
+  int cont_outer, cont_inner;
+  int passes;  // fused passes run in this inner solve (selects the r, p buffers)
+  int pad;
 };
 
 struct MixedArgs {
@@ -126,6 +130,7 @@ __global__ void __launch_bounds__(kBlock) k_mp_start_inner(MixedArgs g) {
       st.inner_k = 0;
       st.pending = 0;
       st.inner_break = 0;
+      st.passes = 0;
       set_inner(g, rr > 0.0 && st.max_inner > 0);
     }
   }
@@ -284,11 +289,67 @@ __global__ void __launch_bounds__(kBlock) k_mp_update_r(MixedArgs g) {
 // d += alpha p (pending), x64 += ||r64|| d.
 __global__ void __launch_bounds__(kBlock) k_mp_end_inner(MixedArgs g) {
   const MixedState *st = g.st;
-  const float alpha = st->pending ? (float)st->alpha : 0.f;
+  const int pend = st->pending;
+  const float alpha = (float)st->alpha;
   const double scale = st->scale;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
-    const float di = fmaf(alpha, g.p[i], g.d[i]);
+    const float di = pend ? fmaf(alpha, g.p[i], g.d[i]) : g.d[i];
     g.x[i] = fma(scale, (double)di, g.x[i]);
+  }
+}
+
+// One fused pass of the matrix-free inner CG (hpccg_iter_tma.cuh).  Pass k
+// reads r and p from buffers k & 1 and writes buffers (k + 1) & 1; p0, p1
+// (box 40 x 68), r0, r1 (box 40 x 66) and dm (box 32 x 64, of g.d) are the
+// tensor maps of the buffers.
+struct IterBufs {
+  float *r[2], *p[2];
+};
+__global__ void __launch_bounds__(kBlock, 2) k_mp_iter_tma(MixedArgs g, TmaTile t, IterBufs b,
+                                                          const __grid_constant__ CUtensorMap p0,
+                                                          const __grid_constant__ CUtensorMap p1,
+                                                          const __grid_constant__ CUtensorMap r0,
+                                                          const __grid_constant__ CUtensorMap r1,
+                                                          const __grid_constant__ CUtensorMap dm) {
+  __shared__ double smem[4 * 32];
+  MixedState *st = g.st;
+  const int par = st->passes & 1;
+  const bool first = st->passes == 0;
+  IterScalars sc;
+  sc.alpha = (float)st->alpha;
+  sc.nalpha = -sc.alpha;
+  sc.beta = (float)st->beta;
+  double v[4];
+  if (first)
+    iter_rows_tma<true>(t, &p0, &r0, &dm, b.r[1], b.p[1], g.d, sc, v, &st->status);
+  else
+    iter_rows_tma<false>(t, par ? &p1 : &p0, par ? &r1 : &r0, &dm, b.r[par ^ 1], b.p[par ^ 1], g.d, sc, v,
+                         &st->status);
+  if (reduce4_last(g.red, v, smem) && threadIdx.x == 0) {
+    const double pAp = v[0], rAp = v[1], ApAp = v[2], rr = v[3];
+    st->pAp = pAp;
+    st->rAp = rAp;
+    st->ApAp = ApAp;
+    if (!first) {
+      st->inner_k += 1;
+      st->inner_total += 1;
+    }
+    st->passes += 1;
+    st->pending = 0;
+    st->rtrans = rr;
+    int cont = isfinite(rr) && (rr > st->target * st->target * st->rr0) && (st->inner_k < st->max_inner);
+    const double alpha = rr / pAp;
+    if (cont && (!(pAp > 0.0) || !isfinite(alpha))) {
+      st->inner_break = 1;
+      cont = 0;
+    }
+    if (cont) {
+      // ||r - alpha Ap||^2 for the next beta
+      const double rr1 = fma(alpha, fma(alpha, ApAp, -2.0 * rAp), rr);
+      st->alpha = alpha;
+      st->beta = fmax(rr1, 0.0) / rr;
+    }
+    set_inner(g, cont);
   }
 }
 
@@ -321,7 +382,7 @@ __global__ void __launch_bounds__(kBlock) k_spmv_lp_tma(TmaTile t, const __grid_
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 static std::mutex g_encode_mu;
 
-int make_stencil_tmap(CUtensorMap *map, const float *base, int nx, int ny, int nz) {
+int make_stencil_tmap(CUtensorMap *map, const float *base, int nx, int ny, int nz, int box_y, int box_x) {
   {
     std::lock_guard<std::mutex> lk(g_encode_mu);
     if (!g_encode) {
@@ -337,7 +398,7 @@ int make_stencil_tmap(CUtensorMap *map, const float *base, int nx, int ny, int n
   if ((reinterpret_cast<uintptr_t>(base) & 15) || nx % 4) return HPCCG_ERR_UNSUPPORTED;
   const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
   const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4};
-  const cuuint32_t box[3] = {kTmaBoxX, kTmaBoxY, 1};
+  const cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_y, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims, strides, box,
                               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -361,6 +422,23 @@ static TmaTile tma_plan(const hpccg_ctx *c) {
       per_sm < 1)
     per_sm = 1;
   return tma_tile_plan(c->gx, c->gy, c->gz, c->num_sms * per_sm);
+}
+
+// Plan of the fused one-pass iteration (nzc = 0: not usable).
+static TmaTile iter_plan(const hpccg_ctx *c) {
+  const TmaTile none{c->gx, c->gy, c->gz, 0, 0, 0, 0};
+  if (cudaFuncSetAttribute(k_mp_iter_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, kItSmemBytes) != cudaSuccess) {
+    cudaGetLastError();
+    return none;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_iter_tma, kBlock, kItSmemBytes) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    return none;
+  }
+  const TmaTile t = tma_tile_plan(c->gx, c->gy, c->gz, c->num_sms * per_sm);
+  return tma_tile_grid(t) <= kItMaxGrid ? t : none;
 }
 
 __global__ void k_to_lp(const double *src, float *f32, __nv_bfloat16 *b16, size_t count) {
@@ -410,6 +488,13 @@ struct MixedRes {
   TmaTile tile{};
   bool tma = false;
   int tma_gx = 0;  // grid the map was made for
+  // the fused one-pass iteration: second r and p buffers, maps of p0, p1, r0, r1
+  float *r2 = nullptr, *p2 = nullptr;
+  CUtensorMap itmap[5];  // p0, p1, r0, r1 and d
+  TmaTile itile{};
+  bool iter = false;
+  bool want_fused = true;  // hpccg_gpu_set_mixed_fused
+  bool exec_fused[3] = {false, false, false};
 };
 
 #include <map>
@@ -425,7 +510,7 @@ void release_mixed(const hpccg_ctx *c) {
   MixedRes *m = it->second;
   for (auto &e : m->exec)
     if (e) cudaGraphExecDestroy(e);
-  void *bufs[] = {m->r, m->p, m->Ap, m->d, m->x32, m->y32, m->val32, m->val16, m->col27, m->st};
+  void *bufs[] = {m->r, m->p, m->Ap, m->d, m->x32, m->y32, m->val32, m->val16, m->col27, m->st, m->r2, m->p2};
   for (void *b : bufs)
     if (b) cudaFree(b);
   delete m;
@@ -498,6 +583,24 @@ static int mixed_res(hpccg_ctx *c, int precision, MixedRes **out) {
   if (stencil && m->tma_gx != c->gx) {
     m->tile = tma_plan(c);
     m->tma = m->tile.nzc > 0 && make_stencil_tmap(&m->pmap, m->p, c->gx, c->gy, c->gz) == HPCCG_OK;
+    m->itile = iter_plan(c);
+    m->iter = false;
+    if (m->itile.nzc > 0) {
+      const size_t vec = sizeof(float) * (size_t)c->npad;
+      if (!m->r2) {
+        HPCCG_CUDA(cudaMalloc(&m->r2, vec));
+        HPCCG_CUDA(cudaMemsetAsync(m->r2, 0, vec, c->stream));
+      }
+      if (!m->p2) {
+        HPCCG_CUDA(cudaMalloc(&m->p2, vec));
+        HPCCG_CUDA(cudaMemsetAsync(m->p2, 0, vec, c->stream));
+      }
+      m->iter = make_stencil_tmap(&m->itmap[0], m->p, c->gx, c->gy, c->gz, kItPBoxY) == HPCCG_OK &&
+                make_stencil_tmap(&m->itmap[1], m->p2, c->gx, c->gy, c->gz, kItPBoxY) == HPCCG_OK &&
+                make_stencil_tmap(&m->itmap[2], m->r, c->gx, c->gy, c->gz, kItRBoxY) == HPCCG_OK &&
+                make_stencil_tmap(&m->itmap[3], m->r2, c->gx, c->gy, c->gz, kItRBoxY) == HPCCG_OK &&
+                make_stencil_tmap(&m->itmap[4], m->d, c->gx, c->gy, c->gz, kItTileY, kItTileX) == HPCCG_OK;
+    }
     m->tma_gx = c->gx;
   }
   *out = m;
@@ -505,6 +608,13 @@ static int mixed_res(hpccg_ctx *c, int precision, MixedRes **out) {
 }
 
 static bool use_tma(const hpccg_ctx *c, const MixedRes *m) { return uses_stencil(c) && m->tma; }
+static bool use_iter(const hpccg_ctx *c, const MixedRes *m) { return uses_stencil(c) && m->iter && m->want_fused; }
+
+static void launch_iter(hpccg_ctx *c, MixedRes *m, const MixedArgs &g, cudaStream_t s) {
+  const IterBufs b{{m->r, m->r2}, {m->p, m->p2}};
+  k_mp_iter_tma<<<tma_tile_grid(m->itile), kBlock, kItSmemBytes, s>>>(g, m->itile, b, m->itmap[0], m->itmap[1],
+                                                                      m->itmap[2], m->itmap[3], m->itmap[4]);
+}
 
 static MixedArgs mixed_args(hpccg_ctx *c, MixedRes *m, int precision) {
   MixedArgs g{};
@@ -527,6 +637,10 @@ static MixedArgs mixed_args(hpccg_ctx *c, MixedRes *m, int precision) {
 }
 
 static int launch_inner_body(hpccg_ctx *c, MixedRes *m, int precision, const MixedArgs &g, cudaStream_t s) {
+  if (use_iter(c, m)) {
+    launch_iter(c, m, g, s);
+    return (int)cudaGetLastError();
+  }
   k_mp_update_p<<<c->grid, kBlock, 0, s>>>(g);
   if (use_tma(c, m)) {
     k_mp_spmv_dot_tma<<<tma_tile_grid(m->tile), kBlock, kTmaRingBytes, s>>>(g, m->tile, m->pmap);
@@ -645,6 +759,7 @@ static int build_mixed_graph(hpccg_ctx *c, MixedRes *m, int precision) {
   }
   m->exec_rpt[precision] = m->rpt[precision];
   m->exec_stencil[precision] = uses_stencil(c);
+  m->exec_fused[precision] = use_iter(c, m);
   return HPCCG_OK;
 }
 
@@ -704,7 +819,7 @@ static int solve_mixed_common(hpccg_ctx *c, int precision, double rel_tol, int32
     if ((rc = run_mixed_eager(c, m, precision))) return rc;
   } else {
     if (!m->exec[precision] || m->exec_rpt[precision] != m->rpt[precision] ||
-        m->exec_stencil[precision] != uses_stencil(c))
+        m->exec_stencil[precision] != uses_stencil(c) || m->exec_fused[precision] != use_iter(c, m))
       if ((rc = build_mixed_graph(c, m, precision))) return rc;
     HPCCG_CUDA(cudaGraphLaunch(m->exec[precision], c->stream));
   }
@@ -809,6 +924,25 @@ extern "C" int hpccg_gpu_time_mixed_kernels(hpccg_ctx *c, int32_t precision, int
   HPCCG_CUDA(cudaMemcpyAsync(m->st, &h0, sizeof(MixedState), cudaMemcpyHostToDevice, c->stream));
   MixedArgs g = mixed_args(c, m, precision);
   g.use_cond = 0;
+  if (use_iter(c, m)) {  // one fused pass per iteration
+    HPCCG_CUDA(cudaMemsetAsync(m->r2, 0, vec, c->stream));
+    HPCCG_CUDA(cudaMemsetAsync(m->p2, 0, vec, c->stream));
+    h0.passes = 1;
+    HPCCG_CUDA(cudaMemcpyAsync(m->st, &h0, sizeof(MixedState), cudaMemcpyHostToDevice, c->stream));
+    for (int rep = -1; rep < reps; ++rep) {
+      if (rep == 0) HPCCG_CUDA(cudaEventRecord(c->ev0, c->stream));
+      launch_iter(c, m, g, c->stream);
+      HPCCG_CUDA(cudaGetLastError());
+    }
+    HPCCG_CUDA(cudaEventRecord(c->ev1, c->stream));
+    HPCCG_CUDA(cudaEventSynchronize(c->ev1));
+    float t = 0.f;
+    HPCCG_CUDA(cudaEventElapsedTime(&t, c->ev0, c->ev1));
+    ms[0] = 0.f;
+    ms[1] = t / (float)reps;
+    ms[2] = 0.f;
+    return HPCCG_OK;
+  }
   for (int which = 0; which < 3; ++which) {
     for (int rep = -1; rep < reps; ++rep) {
       if (rep == 0) HPCCG_CUDA(cudaEventRecord(c->ev0, c->stream));
@@ -836,4 +970,61 @@ extern "C" int hpccg_gpu_time_mixed_kernels(hpccg_ctx *c, int32_t precision, int
     ms[which] = t / (float)reps;
   }
   return HPCCG_OK;
+}
+
+extern "C" int hpccg_gpu_set_mixed_fused(hpccg_ctx *c, int32_t on) {
+  if (!c || (on != 0 && on != 1)) return HPCCG_ERR_INVALID_ARG;
+  for (int precision = HPCCG_PREC_FP32; precision <= HPCCG_PREC_BF16; ++precision) {
+    MixedRes *m = nullptr;
+    const int rc = mixed_res(c, precision, &m);
+    if (rc == HPCCG_ERR_UNSUPPORTED) return HPCCG_OK;  // no inner solver on this context: nothing to select
+    if (rc) return rc;
+    m->want_fused = on != 0;
+  }
+  return HPCCG_OK;
+}
+
+extern "C" int hpccg_gpu_mixed_fused(hpccg_ctx *c, int32_t *fused) {
+  if (!c || !fused) return HPCCG_ERR_INVALID_ARG;
+  MixedRes *m = nullptr;
+  const int rc = mixed_res(c, HPCCG_PREC_FP32, &m);
+  if (rc) return rc;
+  *fused = use_iter(c, m) ? 1 : 0;
+  return HPCCG_OK;
+}
+
+extern "C" int hpccg_gpu_mixed_pass(hpccg_ctx *c, const float *d_r, const float *d_p, float *d_d, float *d_r_out,
+                                    float *d_p_out, double alpha, double beta, int32_t first, double dots[4]) {
+  if (!c || !d_r || !d_p || !d_d || !d_r_out || !d_p_out || !dots || (first != 0 && first != 1))
+    return HPCCG_ERR_INVALID_ARG;
+  MixedRes *m = nullptr;
+  int rc = mixed_res(c, HPCCG_PREC_FP32, &m);
+  if (rc) return rc;
+  if (!uses_stencil(c) || !m->iter) return HPCCG_ERR_UNSUPPORTED;
+  CUtensorMap pm, rm, dm;
+  if (make_stencil_tmap(&pm, d_p, c->gx, c->gy, c->gz, kItPBoxY) != HPCCG_OK ||
+      make_stencil_tmap(&rm, d_r, c->gx, c->gy, c->gz, kItRBoxY) != HPCCG_OK ||
+      make_stencil_tmap(&dm, d_d, c->gx, c->gy, c->gz, kItTileY, kItTileX) != HPCCG_OK)
+    return HPCCG_ERR_UNSUPPORTED;
+  MixedState h0 = {};
+  h0.alpha = alpha;
+  h0.beta = beta;
+  h0.passes = first ? 0 : 2;  // even: read the maps of buffer 0
+  h0.max_inner = 1 << 30;
+  h0.rr0 = 1.0;
+  HPCCG_CUDA(cudaMemcpyAsync(m->st, &h0, sizeof(MixedState), cudaMemcpyHostToDevice, c->stream));
+  MixedArgs g = mixed_args(c, m, HPCCG_PREC_FP32);
+  g.use_cond = 0;
+  g.d = d_d;
+  const IterBufs b{{const_cast<float *>(d_r), d_r_out}, {const_cast<float *>(d_p), d_p_out}};
+  k_mp_iter_tma<<<tma_tile_grid(m->itile), kBlock, kItSmemBytes, c->stream>>>(g, m->itile, b, pm, pm, rm, rm, dm);
+  HPCCG_CUDA(cudaGetLastError());
+  MixedState hs;
+  HPCCG_CUDA(cudaMemcpyAsync(&hs, m->st, sizeof(MixedState), cudaMemcpyDeviceToHost, c->stream));
+  HPCCG_CUDA(cudaStreamSynchronize(c->stream));
+  dots[0] = hs.pAp;
+  dots[1] = hs.rAp;
+  dots[2] = hs.ApAp;
+  dots[3] = hs.rtrans;
+  return hs.status ? hs.status : HPCCG_OK;
 }

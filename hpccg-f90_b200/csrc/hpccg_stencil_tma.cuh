@@ -53,8 +53,10 @@ inline TmaTile tma_tile_plan(int nx, int ny, int nz, int resident_ctas) {
 }
 inline int tma_tile_grid(const TmaTile &t) { return t.tiles_x * t.tiles_y * t.nzc; }
 
-// Host: the tensor map of a FP32 grid vector x[nz][ny][nx] (base 16-byte aligned).
-int make_stencil_tmap(CUtensorMap *map, const float *base, int nx, int ny, int nz);
+// Host: the tensor map of a FP32 grid vector x[nz][ny][nx] (base 16-byte aligned),
+// box box_x x box_y x 1.
+int make_stencil_tmap(CUtensorMap *map, const float *base, int nx, int ny, int nz, int box_y = kTmaBoxY,
+                      int box_x = kTmaBoxX);
 
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1,
                                             int c2) {

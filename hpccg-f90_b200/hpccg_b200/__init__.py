@@ -110,6 +110,10 @@ _SIGS = {
     "hpccg_gpu_spmv_lowp": (_c.c_int, [_vp, _i32, _vp, _vp]),
     "hpccg_gpu_set_mixed_rows_per_thread": (_c.c_int, [_vp, _i32, _i32]),
     "hpccg_gpu_time_mixed_kernels": (_c.c_int, [_vp, _i32, _i32, _c.POINTER(_c.c_float)]),
+    "hpccg_gpu_set_mixed_fused": (_c.c_int, [_vp, _i32]),
+    "hpccg_gpu_mixed_fused": (_c.c_int, [_vp, _c.POINTER(_i32)]),
+    "hpccg_gpu_mixed_pass": (_c.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _c.c_double, _c.c_double, _i32,
+                                        _c.POINTER(_c.c_double)]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _fn = getattr(_lib, _name)
@@ -350,9 +354,27 @@ class Matrix:
         _check(_lib.hpccg_gpu_set_mixed_rows_per_thread(self._h, precision, rpt), "set_mixed_rows_per_thread")
 
     def time_mixed_kernels(self, precision: int, reps: int = 10):
+        """[p update, SpMV + p.Ap, r update] ms; [0, pass, 0] with the fused iteration."""
         ms = (_c.c_float * 3)()
         _check(_lib.hpccg_gpu_time_mixed_kernels(self._h, precision, reps, ms), "time_mixed_kernels")
         return [ms[0], ms[1], ms[2]]
+
+    def set_mixed_fused(self, on: bool):
+        """Select the one-pass fused inner iteration (default) or the three-kernel one."""
+        _check(_lib.hpccg_gpu_set_mixed_fused(self._h, 1 if on else 0), "set_mixed_fused")
+
+    def mixed_fused(self) -> bool:
+        f = _i32(0)
+        _check(_lib.hpccg_gpu_mixed_fused(self._h, _c.byref(f)), "mixed_fused")
+        return bool(f.value)
+
+    def mixed_pass(self, d_r, d_p, d_d, d_r_out, d_p_out, alpha: float, beta: float, first: bool):
+        """One fused inner-CG pass on FP32 device vectors; returns (p'.Ap', r'.Ap', Ap'.Ap', r'.r')."""
+        _sync_torch()
+        dots = (_c.c_double * 4)()
+        _check(_lib.hpccg_gpu_mixed_pass(self._h, _dptr(d_r), _dptr(d_p), _dptr(d_d), _dptr(d_r_out),
+                                         _dptr(d_p_out), alpha, beta, 1 if first else 0, dots), "mixed_pass")
+        return tuple(dots)
 
     def uniform_pm1(self, seed: int, d_out, offset: int = 0):
         """Fill a device tensor with the project's counter-based U[-1,1) stream."""

@@ -157,8 +157,29 @@ int hpccg_gpu_spmv_lowp(hpccg_ctx *ctx, int32_t precision, const float *d_x, flo
 int hpccg_gpu_set_mixed_rows_per_thread(hpccg_ctx *ctx, int32_t precision, int32_t rpt);
 
 /* Average ms of the inner-CG kernels (p update, low-precision SpMV + p.Ap,
- * r update + r.r), each launched `reps` times back to back. */
+ * r update + r.r), each launched `reps` times back to back.  When the inner
+ * iteration is one fused pass (hpccg_gpu_mixed_fused), ms[1] is that pass and
+ * ms[0] = ms[2] = 0. */
 int hpccg_gpu_time_mixed_kernels(hpccg_ctx *ctx, int32_t precision, int32_t reps, float *ms);
+
+/* The fused inner iteration of the matrix-free solve (HPCCG_SPMV_STENCIL
+ * contexts with nx % 4 == 0): one TMA-fed pass per CG iteration reads r, p
+ * and d and writes r, p and d (24 bytes per row instead of 40).  A p of the
+ * previous iteration is recomputed from p with a two-deep halo instead of
+ * being stored, and the next beta comes from the recurrence
+ * ||r - alpha Ap||^2 = r.r - 2 alpha r.Ap + alpha^2 Ap.Ap.  On by default;
+ * set_mixed_fused(ctx, 0) selects the three-kernel iteration.  mixed_fused
+ * reports whether the inner solves of ctx use it. */
+int hpccg_gpu_set_mixed_fused(hpccg_ctx *ctx, int32_t on);
+int hpccg_gpu_mixed_fused(hpccg_ctx *ctx, int32_t *fused);
+
+/* One fused pass on caller buffers (FP32, device, nrow each), for checks:
+ * with Ap = A p, r' = first ? r : r - alpha Ap, p' = first ? r : r' + beta p,
+ * d += alpha p (not when first), Ap' = A p'; writes r', p', d and returns
+ * dots = {p'.Ap', r'.Ap', Ap'.Ap', r'.r'}.  HPCCG_ERR_UNSUPPORTED when the
+ * context has no fused iteration. */
+int hpccg_gpu_mixed_pass(hpccg_ctx *ctx, const float *d_r, const float *d_p, float *d_d, float *d_r_out,
+                         float *d_p_out, double alpha, double beta, int32_t first, double dots[4]);
 
 /* ---- batched solves of many independent systems ------------------------
  *

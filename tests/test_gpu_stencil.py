@@ -163,3 +163,82 @@ def test_stencil_fp32_spmv(hp, torch, nx, ny, nz):
     M.spmv(x32.double(), ref)
     err = float((y32.double() - ref).abs().max())
     assert err <= 2e-5 * max(1.0, float(ref.abs().max())), err
+
+
+def _stencil64(x, nx, ny, nz):
+    """A x of the generate_matrix operator (27 on the diagonal, -1 for each
+    neighbour inside the grid) in FP64: 28 x - (sum of the 3x3x3 box)."""
+    g = np.asarray(x, np.float64).reshape(nz, ny, nx)
+    pad = np.pad(g, 1)
+    box = np.zeros_like(g)
+    for dz in range(3):
+        for dy in range(3):
+            for dx in range(3):
+                box += pad[dz:dz + nz, dy:dy + ny, dx:dx + nx]
+    return (28.0 * g - box).ravel()
+
+
+FUSED_SIZES = [(4, 4, 4), (8, 8, 1), (16, 1, 16), (12, 20, 7), (32, 64, 3), (48, 70, 9), (36, 5, 40),
+               (96, 130, 5)]
+
+
+@pytest.mark.parametrize("nx,ny,nz", FUSED_SIZES)
+@pytest.mark.parametrize("first", [True, False])
+def test_fused_pass_matches_fp64(hp, torch, nx, ny, nz, first):
+    """One fused inner-CG pass (r' = r - alpha A p, p' = r' + beta p,
+    d += alpha p, the four dots of A p') against the same algebra in FP64 on
+    the FP32 inputs; partial tiles in x and y, a single plane, a single row."""
+    n = nx * ny * nz
+    M = hp.Matrix.generated(nx, ny, nz)
+    M.set_spmv(hp.SPMV_STENCIL)
+    assert M.mixed_fused()
+    rng = np.random.default_rng(n * 7 + int(first))
+    r, p, d = (rng.uniform(-1, 1, n).astype(np.float32) for _ in range(3))
+    alpha, beta = 0.37, 0.81
+    dr, dp, dd = (torch.from_numpy(v.copy()).cuda() for v in (r, p, d))
+    ro, po = torch.full_like(dr, np.nan), torch.full_like(dr, np.nan)
+    dots = M.mixed_pass(dr, dp, dd, ro, po, alpha, beta, first)
+    a32, b32 = float(np.float32(alpha)), float(np.float32(beta))
+    r64, p64, d64 = (v.astype(np.float64) for v in (r, p, d))
+    if first:
+        rn, pn, dn = r64, r64, d64
+    else:
+        rn = r64 - a32 * _stencil64(p64, nx, ny, nz)
+        pn = rn + b32 * p64
+        dn = d64 + a32 * p64
+    apn = _stencil64(pn, nx, ny, nz)
+    assert float(np.abs(ro.cpu().numpy() - rn).max()) <= 1e-4
+    assert float(np.abs(po.cpu().numpy() - pn).max()) <= 1e-4
+    assert float(np.abs(dd.cpu().numpy() - dn).max()) <= 1e-6
+    want = [pn @ apn, rn @ apn, apn @ apn, rn @ rn]
+    scale = [np.abs(pn * apn).sum(), np.abs(rn * apn).sum(), apn @ apn, rn @ rn]
+    for got, w, s in zip(dots, want, scale):
+        assert abs(got - w) <= 1e-5 * s, (got, w)
+
+
+@pytest.mark.parametrize("n", [48, 64, 100])
+def test_fused_inner_solve_matches_three_kernel(hp, torch, n):
+    """The mixed FP32 stencil solve with the fused one-pass iteration meets the
+    FP64 target with about the iteration count of the three-kernel iteration."""
+    dx = torch.zeros(n ** 3, dtype=torch.float64, device="cuda")
+    db = torch.zeros_like(dx)
+    M = hp.Matrix.generated(n, n, n)
+    xs = torch.empty_like(dx)
+    M.uniform_pm1(99, xs)
+    M.spmv(xs, db)
+    M.set_spmv(hp.SPMV_STENCIL)
+    assert M.mixed_fused()
+    ms = M.time_mixed_kernels(hp.PREC_FP32, 3)
+    assert ms[0] == 0.0 and ms[2] == 0.0 and ms[1] > 0.0
+    info_f, rc_f = M.solve_mixed_device(db, dx, hp.PREC_FP32, rel_tol=1e-8)
+    assert rc_f == hp.HPCCG_OK and info_f.relres <= 1e-8
+    r = torch.empty_like(dx)
+    M.spmv(dx, r)
+    assert float(torch.linalg.vector_norm(db - r) / torch.linalg.vector_norm(db)) <= 1e-8
+    M.set_mixed_fused(False)
+    assert not M.mixed_fused()
+    dx.zero_()
+    info_3, rc_3 = M.solve_mixed_device(db, dx, hp.PREC_FP32, rel_tol=1e-8)
+    assert rc_3 == hp.HPCCG_OK
+    assert abs(info_f.inner_iters - info_3.inner_iters) <= max(3, info_3.inner_iters // 10)
+    assert info_f.outer_iters <= info_3.outer_iters + 1
