@@ -294,9 +294,12 @@ def run_ours(args):
     dev = torch.device("cuda", local if ws > 1 else 0)
     torch.cuda.set_device(dev)
     n = args.n
-    N = n ** 3
+    nz = args.nz or n  # an n x n x nz grid (cubic unless --nz is given)
+    N = n * n * nz
+    cubic = nz == n
+    grid_name = f"{n}^3" if cubic else f"{n}x{n}x{nz}"
     d_x = torch.zeros(N, dtype=torch.float64, device=dev)
-    M = hp.Matrix.generated(n, n, n, d_x, None, None)
+    M = hp.Matrix.generated(n, n, nz, d_x, None, None)
     xstar = torch.empty(N, dtype=torch.float64, device=dev)
     M.uniform_pm1(SEED_XSTAR, xstar)
     d_b = torch.empty_like(xstar)
@@ -319,7 +322,10 @@ def run_ours(args):
         def run():
             info, st = M.solve_mixed_device(d_b, d_x, prec, REL_TOL)
             assert st == hp.HPCCG_OK, st
-            launches = 1 + (info.outer_iters + 1) + 2 * info.outer_iters + 3 * info.inner_iters
+            # inner iteration: three kernels, or one fused pass (plus the first pass of each inner solve)
+            fused = M.get_spmv()[0] == hp.SPMV_STENCIL and M.mixed_fused()
+            inner = info.inner_iters + info.outer_iters if fused else 3 * info.inner_iters
+            launches = 1 + (info.outer_iters + 1) + 2 * info.outer_iters + inner
             return {"outer": info.outer_iters, "inner": info.inner_iters, "device_relres": info.relres}, launches
         return run
 
@@ -330,10 +336,10 @@ def run_ours(args):
                 ELL),
                ("fp64_cg_stencil", "plain FP64 CG with the matrix-free stencil SpMV (bit-identical to fp64_cg)",
                 fp64_cg, STENCIL),
-               ("fp32_ir_stencil", "FP64 iterative refinement (FP64 stencil residual), FP32 matrix-free inner CG",
-                mixed(hp.PREC_FP32), STENCIL)]
+               ("fp32_ir_stencil", "FP64 iterative refinement (FP64 stencil residual), FP32 matrix-free inner CG "
+                "(one fused TMA pass per iteration when nx % 4 == 0)", mixed(hp.PREC_FP32), STENCIL)]
     learned_info = None
-    if not args.no_learned:
+    if not args.no_learned and cubic:
         from hpccg_b200 import learned
 
         t0 = time.time()
@@ -434,7 +440,7 @@ def run_ours(args):
     roof64 = {"bound": "hbm", "kernel": "k_cg_spmv_dot (FP64 SpMV + p.Ap)", "kernel_ms": kms64[1],
               "alg_bytes_per_launch": alg64, "achieved": alg64 / (kms64[1] * 1e-3) / 1e9, "peak": hbm,
               "unit": "GB/s", "peak_source": peak_kind,
-              "traffic": _traffic_from_profile() if n == 256 else None}
+              "traffic": _traffic_from_profile() if n == 256 and cubic else None}
     roof64["frac"] = roof64["achieved"] / hbm
     roofs = {"fp64_cg": roof64}
     for name, prec, vb in (("fp32_ir", hp.PREC_FP32, 4), ("bf16_ir", hp.PREC_BF16, 2)):
@@ -452,20 +458,24 @@ def run_ours(args):
                                 "kernel_ms": kst[1], "alg_bytes_per_launch": alg,
                                 "achieved": alg / (kst[1] * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                                 "peak_source": peak_kind,
-                                "traffic": _traffic_from_profile("stencil_spmv_256.txt") if n == 256 else None,
+                                "traffic": _traffic_from_profile("stencil_spmv_256.txt") if n == 256 and cubic else None,
                                 "iteration_ms": sum(kst)}
     roofs["fp64_cg_stencil"]["frac"] = roofs["fp64_cg_stencil"]["achieved"] / hbm
+    fused = M.mixed_fused()
     km = M.time_mixed_kernels(hp.PREC_FP32, 20)
-    alg = 8 * N + 4
-    roofs["fp32_ir_stencil"] = {"bound": "hbm",
-                                "kernel": "k_mp_spmv_dot_tma (matrix-free FP32 SpMV, TMA-fed, + p.Ap)"
-                                if n % 4 == 0 else "k_mp_spmv_dot<StratLpStencil> (matrix-free FP32 SpMV + p.Ap)",
+    if fused:  # one pass reads r, p, d and writes r, p, d (FP32), plus four FP64 partials per CTA
+        alg = 24 * N + 32
+        kname = "k_mp_iter_tma (one fused FP32 matrix-free inner-CG pass, TMA-fed: r, p, d in and out)"
+        traffic = _traffic_from_profile("inner_cg_pass_256.txt", "iter_dram_bytes_per_launch_full_size")
+    else:
+        alg = 8 * N + 4
+        kname = ("k_mp_spmv_dot_tma (matrix-free FP32 SpMV, TMA-fed, + p.Ap)" if n % 4 == 0
+                 else "k_mp_spmv_dot<StratLpStencil> (matrix-free FP32 SpMV + p.Ap)")
+        traffic = _traffic_from_profile("stencil_spmv_256.txt", "fp32_tma_dram_bytes_per_launch_full_size")
+    roofs["fp32_ir_stencil"] = {"bound": "hbm", "kernel": kname,
                                 "kernel_ms": km[1], "alg_bytes_per_launch": alg,
                                 "achieved": alg / (km[1] * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
-                                "peak_source": peak_kind,
-                                "traffic": _traffic_from_profile("stencil_spmv_256.txt",
-                                                                 "fp32_tma_dram_bytes_per_launch_full_size")
-                                if n == 256 else None,
+                                "peak_source": peak_kind, "traffic": traffic if n == 256 and cubic else None,
                                 "inner_iteration_ms": sum(km)}
     roofs["fp32_ir_stencil"]["frac"] = roofs["fp32_ir_stencil"]["achieved"] / hbm
     roofs["learned_fcg"] = roofs["fp64_cg_stencil"]
@@ -476,7 +486,7 @@ def run_ours(args):
         return 0
 
     cpu = None
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and cubic:
         it64 = results["fp64_cg"]["iterations"]
         c = cpu_reference_time(n, args.ref_sample_iters, 1, 0, iters_needed=it64)
         cpu = {"value": c["value"], "unit": "s", "cores": c["cores"], "kind": "port",
@@ -489,7 +499,7 @@ def run_ours(args):
         "vs_baseline": None, "dtype": "f64" if head.startswith("fp64") or head == "learned_fcg"
         else "f32/bf16 inner, f64 outer",
         "data": "synthetic",
-        "config": {"workload": f"{n}^3 27-point HPCCG matrix ({N} rows, {nnz} nonzeros), x* U[-1,1) seed 1234, "
+        "config": {"workload": f"{grid_name} 27-point HPCCG matrix ({N} rows, {nnz} nonzeros), x* U[-1,1) seed 1234, "
                                f"b = A x*, x0 = 0, solved to FP64 ||b - A x|| <= 1e-8 ||b||",
                    "method": head, "speedup_vs_plain_gpu_cg": plain_ms / hr["ms"],
                    "speedup_vs_plain_gpu_cg_stencil": results["fp64_cg_stencil"]["ms"] / hr["ms"],
@@ -518,6 +528,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--nz", type=int, default=0, help="planes of an n x n x nz grid (default n; profiling cases)")
     ap.add_argument("--ref-sample-iters", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip training/timing the learned preconditioner")
