@@ -191,8 +191,15 @@ def cpu_reference_time(n: int, sample_iters: int, steps: int, warmup: int, iters
         if s >= warmup:
             per_iter.append(dt)
     value = float(np.median(per_iter)) * iters_needed
+    # the same on one thread (the oracle's sequential build): median of three one-iteration samples
+    per_iter_1t = []
+    for _ in range(3):
+        t = time.perf_counter()
+        oracle.cg(A, b, x0, 1, 0.0, omp=False)
+        per_iter_1t.append(time.perf_counter() - t)
     return {"value": value, "per_iter_s": per_iter, "iters": iters_needed, "cores": cores,
-            "full_solve_s": full_s, "sample_iters": sample_iters}
+            "full_solve_s": full_s, "sample_iters": sample_iters,
+            "value_1thread": float(np.median(per_iter_1t)) * iters_needed, "per_iter_1thread_s": per_iter_1t}
 
 
 def run_reference(args):
@@ -210,7 +217,10 @@ def run_reference(args):
         "config": {"workload": f"{args.n}^3 27-point HPCCG matrix, x* U[-1,1) seed 1234, b = A x*, x0 = 0, FP64 CG to ||r||/||b|| <= 1e-8",
                    "reference_build": "unavailable (Fortran 90; no Fortran compiler in this image) -> C restatement of MPI/src",
                    "iterations": r["iters"]},
-        "cpu_baseline": {"value": r["value"], "unit": "s", "cores": r["cores"], "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": r["value"], "unit": "s", "cores": r["cores"], "kind": "port", "sample": sample,
+                         "value_1thread": r["value_1thread"],
+                         "sample_1thread": "median of 3 one-iteration samples, sequential build, times the same "
+                                           "iteration count"},
         "e2e": {"value": r["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -488,10 +498,12 @@ def run_ours(args):
     cpu = None
     if not args.no_cpu_baseline and cubic:
         it64 = results["fp64_cg"]["iterations"]
-        c = cpu_reference_time(n, args.ref_sample_iters, 1, 0, iters_needed=it64)
+        c = cpu_reference_time(n, args.ref_sample_iters, 3, 0, iters_needed=it64)
         cpu = {"value": c["value"], "unit": "s", "cores": c["cores"], "kind": "port",
-               "sample": f"{args.ref_sample_iters} CG iterations of the C restatement of MPI/src at {n}^3 "
-                         f"(OpenMP, {c['cores']} threads) x {it64} iterations (the GPU FP64 count)"}
+               "value_1thread": c["value_1thread"],
+               "sample": f"median of 3 samples of {args.ref_sample_iters} CG iterations of the C restatement of "
+                         f"MPI/src at {n}^3 (OpenMP, {c['cores']} threads) x {it64} iterations (the GPU FP64 count); "
+                         f"value_1thread: median of 3 one-iteration samples of the sequential build, same count"}
     hr = results[head]
     line = {
         "metric": METRIC, "value": hr["ms"] / 1e3, "unit": "s", "n_gpus": ws, "steps": args.steps,
