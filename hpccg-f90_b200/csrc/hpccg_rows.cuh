@@ -137,12 +137,14 @@ __device__ __forceinline__ double csr_vector_rows(int n, const int32_t *__restri
 }
 
 // ---- epilogues --------------------------------------------------------------
+// The three-argument forms receive x_i (the matrix-free walk has it at hand).
 struct EpiStore {  // y = A x
   double *y;
   __device__ __forceinline__ double operator()(int i, double s) const {
     y[i] = s;
     return 0.0;
   }
+  __device__ __forceinline__ double operator()(int i, double s, double) const { return (*this)(i, s); }
 };
 struct EpiDot {  // Ap = A p, contribution p_i * Ap_i
   const double *p;
@@ -150,6 +152,10 @@ struct EpiDot {  // Ap = A p, contribution p_i * Ap_i
   __device__ __forceinline__ double operator()(int i, double s) const {
     y[i] = s;
     return __dmul_rn(__ldg(p + i), s);
+  }
+  __device__ __forceinline__ double operator()(int i, double s, double pi) const {
+    y[i] = s;
+    return __dmul_rn(pi, s);
   }
 };
 struct EpiResidual {  // r = 1*b + (-1)*(A x), contribution r_i^2
@@ -160,6 +166,7 @@ struct EpiResidual {  // r = 1*b + (-1)*(A x), contribution r_i^2
     r[i] = ri;
     return __dmul_rn(ri, ri);
   }
+  __device__ __forceinline__ double operator()(int i, double s, double) const { return (*this)(i, s); }
 };
 
 // Arguments every row strategy may need.

@@ -120,13 +120,17 @@ __device__ __forceinline__ unsigned stencil_mask(const StencilGeom &g, int ix, i
 
 // Loads the 3x3 neighbourhood (sy, sx order) of the thread's column in the
 // plane that `p` points into (p = &x[column + z*plane]); `mask` bit j clear
-// (or zin false) gives 0 for neighbour j, which lies outside the grid.
-template <typename Real>
+// (or zin false) gives 0 for neighbour j, which lies outside the grid.  FULL:
+// the caller knows all nine neighbours lie inside the grid (mask == 0x1FF).
+template <typename Real, bool FULL = false>
 __device__ __forceinline__ void stencil_plane(const Real *__restrict__ p, int nx, unsigned mask, bool zin, Real *v) {
 #pragma unroll
   for (int j = 0; j < 9; ++j) {
     const int off = (j / 3 - 1) * nx + (j % 3 - 1);
-    v[j] = (zin && ((mask >> j) & 1u)) ? __ldg(p + off) : Real(0);
+    if (FULL)
+      v[j] = zin ? __ldg(p + off) : Real(0);
+    else
+      v[j] = (zin && ((mask >> j) & 1u)) ? __ldg(p + off) : Real(0);
   }
 }
 
@@ -354,7 +358,33 @@ __device__ __forceinline__ double stencil_rows_box64x4(const StencilGeom &g, con
   return part;
 }
 
-// All rows of the calling thread; epi(i, rowsum) stores and returns a dot term.
+// The z walk of one column (plane map): the row sum starts with the 9 terms
+// of plane z-1 added to 0 in order; that prefix depends on plane z-1 alone,
+// so it is formed once per plane (lead) and the window keeps only planes z
+// and z+1 in full.  epi(i, rowsum, x_i) stores and returns a dot term.
+template <typename Real, bool FULL, class Epi>
+__device__ __forceinline__ double stencil_column(const PlaneSpan &sp, const StencilGeom &g, const PlaneMap &m,
+                                                 unsigned mask, const Real *__restrict__ pc, Epi &epi) {
+  double part = 0.0;
+  Real b[9], c[9];
+  stencil_plane<Real, FULL>(pc + (int64_t)(sp.z0 - 1) * m.plane, g.nx, mask, sp.z0 > 0, c);
+  Real lead = stencil_lead<Real>(c);
+  stencil_plane<Real, FULL>(pc + (int64_t)sp.z0 * m.plane, g.nx, mask, true, b);
+  for (int z = sp.z0; z < sp.z1; ++z) {
+    stencil_plane<Real, FULL>(pc + (int64_t)(z + 1) * m.plane, g.nx, mask, z + 1 < g.nz, c);
+    const Real s = stencil_tail<Real>(lead, b, c);
+    if constexpr (sizeof(Real) == 8)
+      part = __dadd_rn(part, epi(sp.c + z * m.plane, s, b[4]));
+    else
+      part += epi(sp.c + z * m.plane, s, b[4]);
+    lead = stencil_lead<Real>(b);
+#pragma unroll
+    for (int j = 0; j < 9; ++j) b[j] = c[j];
+  }
+  return part;
+}
+
+// All rows of the calling thread; epi(i, rowsum, x_i) stores and returns a dot term.
 template <typename Real, class Epi>
 __device__ __forceinline__ double stencil_rows(int n, const StencilGeom &g, const PlaneMap &m,
                                                const Real *__restrict__ x, Epi &epi) {
@@ -364,26 +394,11 @@ __device__ __forceinline__ double stencil_rows(int n, const StencilGeom &g, cons
     if (sp.z0 >= sp.z1) return part;
     const int iy = sp.c / g.nx, ix = sp.c - iy * g.nx;
     const unsigned mask = stencil_mask(g, ix, iy);
-    const Real *pc = x + sp.c;
-    // The row sum starts with the 9 terms of plane z-1 added to 0 in order:
-    // that prefix depends on plane z-1 alone, so it is formed once per plane
-    // (lead) and the window keeps only planes z and z+1 in full.
-    Real b[9], c[9];
-    stencil_plane<Real>(pc + (int64_t)(sp.z0 - 1) * m.plane, g.nx, mask, sp.z0 > 0, c);
-    Real lead = stencil_lead<Real>(c);
-    stencil_plane<Real>(pc + (int64_t)sp.z0 * m.plane, g.nx, mask, true, b);
-    for (int z = sp.z0; z < sp.z1; ++z) {
-      stencil_plane<Real>(pc + (int64_t)(z + 1) * m.plane, g.nx, mask, z + 1 < g.nz, c);
-      const Real s = stencil_tail<Real>(lead, b, c);
-      if constexpr (sizeof(Real) == 8)
-        part = __dadd_rn(part, epi(sp.c + z * m.plane, s));
-      else
-        part += epi(sp.c + z * m.plane, s);
-      lead = stencil_lead<Real>(b);
-#pragma unroll
-      for (int j = 0; j < 9; ++j) b[j] = c[j];
-    }
-    return part;
+    // warps whose columns all lie off the x and y faces load without the
+    // per-neighbour tests (the sums are the same: masked terms are zeros)
+    if (__all_sync(__activemask(), mask == 0x1FFu))
+      return stencil_column<Real, true>(sp, g, m, mask, x + sp.c, epi);
+    return stencil_column<Real, false>(sp, g, m, mask, x + sp.c, epi);
   }
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {

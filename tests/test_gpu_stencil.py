@@ -242,3 +242,55 @@ def test_fused_inner_solve_matches_three_kernel(hp, torch, n):
     assert rc_3 == hp.HPCCG_OK
     assert abs(info_f.inner_iters - info_3.inner_iters) <= max(3, info_3.inner_iters // 10)
     assert info_f.outer_iters <= info_3.outer_iters + 1
+
+
+def _fused_problem(hp, n, seed=1234):
+    A, x, b1, xe = oracle.generate_matrix(n, n, n)
+    xstar = oracle.uniform_pm1(seed, A.nrow)
+    b = oracle.spmv(A, xstar)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    M.set_geometry(n, n, n)
+    M.set_spmv(hp.SPMV_STENCIL)
+    assert M.mixed_fused()
+    return A, b, xstar, M
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+def test_fused_solve_meets_target_against_oracle(hp, prec):
+    """The fused inner iteration inside FP64 refinement: the CPU oracle's FP64
+    residual of the returned x meets 1e-8 and x is within 1e-7 of the oracle's
+    FP64 CG solution and of x*."""
+    A, b, xstar, M = _fused_problem(hp, 20)
+    x, info, status = M.solve_mixed(b, np.zeros_like(b), prec, rel_tol=1e-8)
+    assert status == hp.HPCCG_OK
+    rel = oracle.true_relres(A, b, x)
+    assert rel <= 1e-8 and abs(rel - info.relres) <= 1e-3 * 1e-8
+    xo, it, _, _ = oracle.cg(A, b, np.zeros_like(b), 1000, 1e-8 * np.linalg.norm(b))
+    assert np.abs(x - xo).max() <= 1e-7 and np.abs(x - xstar).max() <= 1e-7
+
+
+def test_fused_eager_equals_graph_and_is_deterministic(hp, monkeypatch):
+    A, b, xstar, M = _fused_problem(hp, 24)
+    xg, ig, sg = M.solve_mixed(b, np.zeros_like(b), 1, rel_tol=1e-8)
+    xg2, ig2, _ = M.solve_mixed(b, np.zeros_like(b), 1, rel_tol=1e-8)
+    monkeypatch.setenv("HPCCG_EAGER", "1")
+    xe, ie, se = M.solve_mixed(b, np.zeros_like(b), 1, rel_tol=1e-8)
+    assert sg == se == hp.HPCCG_OK
+    assert np.array_equal(_bits(xg), _bits(xg2)) and np.array_equal(_bits(xg), _bits(xe))
+    assert (ig.outer_iters, ig.inner_iters) == (ie.outer_iters, ie.inner_iters) == (ig2.outer_iters, ig2.inner_iters)
+
+
+def test_fused_zero_rhs_exact_start_and_caps(hp):
+    A, b, xstar, M = _fused_problem(hp, 16)
+    x, info, status = M.solve_mixed(np.zeros_like(b), np.zeros_like(b), 1, rel_tol=1e-8)
+    assert status == hp.HPCCG_OK and info.outer_iters == 0 and np.all(x == 0)
+    x, info, status = M.solve_mixed(b, xstar.copy(), 1, rel_tol=1e-8)  # r = 0 already
+    assert status == hp.HPCCG_OK and info.outer_iters == 0
+    # a loose fixed inner target needs more refinement cycles; a cycle cap stops early
+    x, info, status = M.solve_mixed(b, np.zeros_like(b), 1, rel_tol=1e-8, inner_rtol=1e-2)
+    assert status == hp.HPCCG_OK and info.outer_iters >= 4
+    x, info, status = M.solve_mixed(b, np.zeros_like(b), 1, rel_tol=1e-12, max_outer=1, inner_rtol=1e-3)
+    assert status == hp.HPCCG_ERR_NOT_CONVERGED and info.outer_iters == 1 and 1e-12 < info.relres < 1e-2
+    # the inner iteration cap: at most max_inner x updates per cycle
+    x, info, status = M.solve_mixed(b, np.zeros_like(b), 1, rel_tol=1e-8, max_outer=30, max_inner=3)
+    assert status == hp.HPCCG_OK and info.inner_iters <= 3 * info.outer_iters
