@@ -335,7 +335,8 @@ def run_ours(args):
             # inner iteration: three kernels, or one fused pass (plus the first pass of each inner solve)
             fused = M.get_spmv()[0] == hp.SPMV_STENCIL and M.mixed_fused()
             inner = info.inner_iters + info.outer_iters if fused else 3 * info.inner_iters
-            launches = 1 + (info.outer_iters + 1) + 2 * info.outer_iters + inner
+            # b.b (its own kernel unless fused into the first residual), residuals, inner start/end
+            launches = (0 if fused else 1) + (info.outer_iters + 1) + 2 * info.outer_iters + inner
             return {"outer": info.outer_iters, "inner": info.inner_iters, "device_relres": info.relres}, launches
         return run
 

@@ -14,7 +14,8 @@
 //   Ap'    = 28 p' - box27(p')               (A p_k, reduced into the dots only)
 //   dots   = p'.Ap', r'.Ap', Ap'.Ap', r'.r'
 //
-// The first pass of an inner solve (k = 0) sets p' = r' = r.  From the dots the
+// The first pass of an inner solve (k = 0) sets p' = r' = r / ||r|| (the
+// refinement residual arrives unscaled) and d = 0.  From the dots the
 // last block forms alpha_k = r'.r' / p'.Ap' and the next beta from the
 // recurrence ||r_k - alpha_k Ap_k||^2 = r'.r' - 2 alpha_k r'.Ap' +
 // alpha_k^2 Ap'.Ap', which the next pass needs before it can build p_{k+1}.
@@ -64,6 +65,7 @@ static_assert(kBlock == (kItTileX / 4) * (kItTileY / 2), "one thread per 4 x 2 c
 
 struct IterScalars {
   float alpha, nalpha, beta;
+  float inv;  // first pass: r arrives unscaled and is multiplied by inv = 1/||r||
 };
 
 // 3-point line sums of the four columns at r[0..3] (r[-1] and r[4] are the
@@ -197,7 +199,9 @@ __device__ __forceinline__ bool it_step(const int s, const ItCta &c, unsigned ch
       const float4 ro = *reinterpret_cast<const float4 *>(R + c.tyo + j * kItBoxX + c.txo);
       float4 rn, pn;
       if (FIRST) {
-        rn = pn = ro;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) f4(rn, i) = f4(ro, i) * sc.inv;
+        pn = rn;
       } else {
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
@@ -213,7 +217,9 @@ __device__ __forceinline__ bool it_step(const int s, const ItCta &c, unsigned ch
         const int gi = (s - 1) * c.plane + (c.yc + j) * c.nx + c.xc;
         *reinterpret_cast<float4 *>(r_out + gi) = rn;
         *reinterpret_cast<float4 *>(p_out + gi) = pn;
-        if (!FIRST) {
+        if (FIRST) {
+          *reinterpret_cast<float4 *>(d + gi) = z4;  // the correction of a new inner solve starts at 0
+        } else {
           float4 dv = *reinterpret_cast<const float4 *>(D + c.dofs + j * kItTileX);
 #pragma unroll
           for (int i = 0; i < 4; ++i) f4(dv, i) = fmaf(sc.alpha, f4(prv.pc[j], i), f4(dv, i));
@@ -228,7 +234,7 @@ __device__ __forceinline__ bool it_step(const int s, const ItCta &c, unsigned ch
       const float ro = R[c.hofs];
       float pn;
       if (FIRST) {
-        pn = ro;
+        pn = ro * sc.inv;
       } else {
         const float ap = fmaf(28.f, prv.pch, -(run.Th + cur.b2h));
         pn = fmaf(sc.beta, prv.pch, fmaf(sc.nalpha, ap, ro));

@@ -109,6 +109,66 @@ __global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_residual64(SpmvArg
   }
 }
 
+// The refinement residual of the fused inner iteration: r = b - A x in FP64,
+// stored unscaled in FP32 (the first fused pass scales it by 1/||r||), its
+// norm and the outer decision; with FIRST also b.b (the solve's first call).
+struct EpiResidualF {
+  const double *b;
+  float *r;
+  double bb;
+  __device__ __forceinline__ double operator()(int i, double s) {
+    const double bi = __ldg(b + i);
+    bb = __dadd_rn(bb, __dmul_rn(bi, bi));
+    const double ri = __dsub_rn(bi, s);
+    r[i] = (float)ri;
+    return __dmul_rn(ri, ri);
+  }
+  __device__ __forceinline__ double operator()(int i, double s, double) { return (*this)(i, s); }
+};
+template <class S, bool FIRST>
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_residual_f(SpmvArgs a, MixedArgs g) {
+  __shared__ double smem[4 * 32];
+  EpiResidualF epi{g.b, g.r, 0.0};
+  double v[4] = {S::rows(a, g.x, epi), 0.0, 0.0, 0.0};
+  v[1] = epi.bb;
+  if (reduce4_last(g.red, v, smem) && threadIdx.x == 0) {
+    MixedState &st = *g.st;
+    if (FIRST) {
+      st.bb = v[1];
+      st.outer = 0;
+      st.inner_total = 0;
+      st.status = HPCCG_OK;
+    }
+    const double rr = v[0];
+    st.rr64 = rr;
+    st.relres = st.bb > 0.0 ? sqrt(rr / st.bb) : 0.0;
+    int cont = (st.relres > st.rel_tol) && (st.outer < st.max_outer);
+    if (!isfinite(st.relres)) {
+      st.status = HPCCG_ERR_BREAKDOWN;
+      cont = 0;
+    }
+    if (cont) {
+      st.scale = sqrt(rr);
+      st.target = st.inner_rtol > 0.0 ? st.inner_rtol : fmax(st.inner_floor, 0.5 * st.rel_tol / st.relres);
+      st.outer += 1;
+    }
+    set_outer(g, cont);
+  }
+}
+
+// Start of an inner solve of the fused iteration: scalar state only (the
+// first pass scales r, clears d and forms rr0).
+__global__ void k_mp_start_inner_f(MixedArgs g) {
+  if (threadIdx.x == 0) {
+    MixedState &st = *g.st;
+    st.inner_k = 0;
+    st.pending = 0;
+    st.inner_break = 0;
+    st.passes = 0;
+    set_inner(g, st.rr64 > 0.0 && st.max_inner > 0);
+  }
+}
+
 // r32 = r64 / ||r64||, d = 0, rr0 = ||r32||^2.
 __global__ void __launch_bounds__(kBlock) k_mp_start_inner(MixedArgs g) {
   __shared__ double smem[32];
@@ -319,6 +379,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_mp_iter_tma(MixedArgs g, TmaTile 
   sc.alpha = (float)st->alpha;
   sc.nalpha = -sc.alpha;
   sc.beta = (float)st->beta;
+  sc.inv = first ? (float)(1.0 / st->scale) : 1.f;
   double v[4];
   if (first)
     iter_rows_tma<true>(t, &p0, &r0, &dm, b.r[1], b.p[1], g.d, sc, v, &st->status);
@@ -337,6 +398,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_mp_iter_tma(MixedArgs g, TmaTile 
     st->passes += 1;
     st->pending = 0;
     st->rtrans = rr;
+    if (first) st->rr0 = rr;
     int cont = isfinite(rr) && (rr > st->target * st->target * st->rr0) && (st->inner_k < st->max_inner);
     const double alpha = rr / pAp;
     if (cont && (!(pAp > 0.0) || !isfinite(alpha))) {
@@ -658,6 +720,27 @@ static int launch_inner_body(hpccg_ctx *c, MixedRes *m, int precision, const Mix
   return (int)cudaGetLastError();
 }
 
+// The refinement residual of the fused iteration (FIRST: also b.b).
+static int launch_residual_f(hpccg_ctx *c, const MixedArgs &g, cudaStream_t s, bool first) {
+  SpmvArgs a = spmv_args(c);
+  auto go = [&](auto strat) {
+    using St = decltype(strat);
+    const int grid = St::grid(a, c->grid);
+    if (grid > kItMaxGrid) return (int)HPCCG_ERR_UNSUPPORTED;
+    if (first)
+      k_mp_residual_f<St, true><<<grid, kBlock, 0, s>>>(a, g);
+    else
+      k_mp_residual_f<St, false><<<grid, kBlock, 0, s>>>(a, g);
+    return (int)cudaGetLastError();
+  };
+  const PlaneMap q = boxw_map(4, c->gx, c->gy, c->gz, (int64_t)c->num_sms * StratStencilBox64::kMinBlocks * kBlock);
+  if (q.plane > 0) {
+    a.pm = q;
+    return go(StratStencilBox64{});
+  }
+  return go(StratStencil{});
+}
+
 static int launch_residual64(hpccg_ctx *c, const MixedArgs &g, cudaStream_t s) {
   SpmvArgs a = spmv_args(c);
   if (a.kind == HPCCG_SPMV_STENCIL) {  // the FP64 box walk, four columns per thread
@@ -724,9 +807,14 @@ static int build_mixed_graph(hpccg_ctx *c, MixedRes *m, int precision) {
   MixedArgs ga = mixed_args(c, m, precision);
   ga.cond_outer = ho;
   ga.use_cond = 1;
+  const bool fused = use_iter(c, m);
   if (e == cudaSuccess) {
-    k_mp_bnorm<<<c->grid, kBlock, 0, s>>>(ga);
-    e = (cudaError_t)launch_residual64(c, ga, s);
+    if (fused) {
+      e = (cudaError_t)launch_residual_f(c, ga, s, true);
+    } else {
+      k_mp_bnorm<<<c->grid, kBlock, 0, s>>>(ga);
+      e = (cudaError_t)launch_residual64(c, ga, s);
+    }
   }
   if (e == cudaSuccess)
     e = capture_while(s, ho, [&](cudaStream_t os, cudaGraph_t og) -> cudaError_t {
@@ -735,7 +823,10 @@ static int build_mixed_graph(hpccg_ctx *c, MixedRes *m, int precision) {
       if (ee != cudaSuccess) return ee;
       MixedArgs gi = ga;
       gi.cond_inner = hi;
-      k_mp_start_inner<<<c->grid, kBlock, 0, os>>>(gi);
+      if (fused)
+        k_mp_start_inner_f<<<1, 32, 0, os>>>(gi);
+      else
+        k_mp_start_inner<<<c->grid, kBlock, 0, os>>>(gi);
       ee = cudaGetLastError();
       if (ee == cudaSuccess)
         ee = capture_while(os, hi, [&](cudaStream_t is, cudaGraph_t) -> cudaError_t {
@@ -745,7 +836,8 @@ static int build_mixed_graph(hpccg_ctx *c, MixedRes *m, int precision) {
         k_mp_end_inner<<<c->grid, kBlock, 0, os>>>(gi);
         ee = cudaGetLastError();
       }
-      if (ee == cudaSuccess) ee = (cudaError_t)launch_residual64(c, gi, os);
+      if (ee == cudaSuccess)
+        ee = (cudaError_t)(fused ? launch_residual_f(c, gi, os, false) : launch_residual64(c, gi, os));
       return ee;
     });
   cudaGraph_t out = nullptr;
@@ -766,15 +858,24 @@ static int build_mixed_graph(hpccg_ctx *c, MixedRes *m, int precision) {
 static int run_mixed_eager(hpccg_ctx *c, MixedRes *m, int precision) {
   MixedArgs g = mixed_args(c, m, precision);
   g.use_cond = 0;
-  k_mp_bnorm<<<c->grid, kBlock, 0, c->stream>>>(g);
-  int rc = launch_residual64(c, g, c->stream);
+  const bool fused = use_iter(c, m);
+  int rc;
+  if (fused) {
+    rc = launch_residual_f(c, g, c->stream, true);
+  } else {
+    k_mp_bnorm<<<c->grid, kBlock, 0, c->stream>>>(g);
+    rc = launch_residual64(c, g, c->stream);
+  }
   if (rc) return set_cuda_error((cudaError_t)rc, "residual64", __FILE__, __LINE__);
   for (;;) {
     int cont = 0;
     HPCCG_CUDA(cudaMemcpyAsync(&cont, &m->st->cont_outer, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     HPCCG_CUDA(cudaStreamSynchronize(c->stream));
     if (!cont) break;
-    k_mp_start_inner<<<c->grid, kBlock, 0, c->stream>>>(g);
+    if (fused)
+      k_mp_start_inner_f<<<1, 32, 0, c->stream>>>(g);
+    else
+      k_mp_start_inner<<<c->grid, kBlock, 0, c->stream>>>(g);
     for (;;) {
       int ci = 0;
       HPCCG_CUDA(cudaMemcpyAsync(&ci, &m->st->cont_inner, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -784,7 +885,7 @@ static int run_mixed_eager(hpccg_ctx *c, MixedRes *m, int precision) {
       if (rc) return set_cuda_error((cudaError_t)rc, "inner", __FILE__, __LINE__);
     }
     k_mp_end_inner<<<c->grid, kBlock, 0, c->stream>>>(g);
-    rc = launch_residual64(c, g, c->stream);
+    rc = fused ? launch_residual_f(c, g, c->stream, false) : launch_residual64(c, g, c->stream);
     if (rc) return set_cuda_error((cudaError_t)rc, "residual64", __FILE__, __LINE__);
   }
   return HPCCG_OK;
@@ -1012,6 +1113,7 @@ extern "C" int hpccg_gpu_mixed_pass(hpccg_ctx *c, const float *d_r, const float 
   h0.passes = first ? 0 : 2;  // even: read the maps of buffer 0
   h0.max_inner = 1 << 30;
   h0.rr0 = 1.0;
+  h0.scale = 1.0;  // the first pass divides r by it
   HPCCG_CUDA(cudaMemcpyAsync(m->st, &h0, sizeof(MixedState), cudaMemcpyHostToDevice, c->stream));
   MixedArgs g = mixed_args(c, m, HPCCG_PREC_FP32);
   g.use_cond = 0;

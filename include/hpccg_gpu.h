@@ -175,7 +175,7 @@ int hpccg_gpu_mixed_fused(hpccg_ctx *ctx, int32_t *fused);
 
 /* One fused pass on caller buffers (FP32, device, nrow each), for checks:
  * with Ap = A p, r' = first ? r : r - alpha Ap, p' = first ? r : r' + beta p,
- * d += alpha p (not when first), Ap' = A p'; writes r', p', d and returns
+ * d += alpha p (d = 0 when first), Ap' = A p'; writes r', p', d and returns
  * dots = {p'.Ap', r'.Ap', Ap'.Ap', r'.r'}.  HPCCG_ERR_UNSUPPORTED when the
  * context has no fused iteration. */
 int hpccg_gpu_mixed_pass(hpccg_ctx *ctx, const float *d_r, const float *d_p, float *d_d, float *d_r_out,

@@ -200,8 +200,8 @@ def test_fused_pass_matches_fp64(hp, torch, nx, ny, nz, first):
     dots = M.mixed_pass(dr, dp, dd, ro, po, alpha, beta, first)
     a32, b32 = float(np.float32(alpha)), float(np.float32(beta))
     r64, p64, d64 = (v.astype(np.float64) for v in (r, p, d))
-    if first:
-        rn, pn, dn = r64, r64, d64
+    if first:  # the first pass of an inner solve (scale 1 here) also clears d
+        rn, pn, dn = r64, r64, np.zeros_like(d64)
     else:
         rn = r64 - a32 * _stencil64(p64, nx, ny, nz)
         pn = rn + b32 * p64
