@@ -5,7 +5,7 @@
 // boundary.  A schedule cuts every system into tiles of whole chunks; one
 // persistent kernel per CG phase walks the tiles of all systems that are still
 // active.  Every dot product is reduced per 512-row chunk in a fixed order
-// (thread pair sums, fixed block butterfly), and per system over its chunks in
+// (each lane's rows in order, then the fixed warp butterfly), and per system over its chunks in
 // index order, so the result does not depend on the schedule: the autotuner
 // may pick any tile size / grid and every iterate stays bit-identical.
 //
@@ -31,7 +31,7 @@
 
 namespace hpccg {
 
-constexpr int kChunk = 512;  // rows per reduction chunk (2 per thread of a 256-thread block)
+constexpr int kChunk = 512;  // rows per reduction chunk (16 per lane of one warp)
 
 struct BatchSys {
   double bb, tol2, rtrans, pAp, alpha, beta, relres, scale, target, rr0;
@@ -92,12 +92,21 @@ __device__ __forceinline__ float row_lp(const BatchArgs &g, int i, int sys, cons
 }
 
 // ---- the phases ----------------------------------------------------------------
-// Each phase: active(s) selects the systems it touches, row(i, s) does the row's
-// work and returns its dot-product term, finalize(s, total) runs once per
-// active system in the last block, cond() names the loop condition it sets.
+// Each phase: active(s) selects the systems it touches; value(i, s) reads and
+// computes row i (no stores) and commit(i, s, v) stores it and returns the
+// row's dot-product term, so a lane can issue the loads of kUnroll rows before
+// any store (the vectors are not restrict-qualified and would otherwise be
+// read one row at a time); finalize(s, total) runs once per active system in
+// the last block; kCond names the loop condition it sets.
+struct V2 {
+  double a, b;
+};
 struct PhBnorm {  // bb = b.b
+  static constexpr int kUnroll = 4;
+  static constexpr bool kGather = false;
   static __device__ bool active(const BatchArgs &g, int s) { return true; }
-  static __device__ double row(const BatchArgs &g, int i, int s) { return __dmul_rn(g.b[i], g.b[i]); }
+  static __device__ V2 value(const BatchArgs &g, int i, int s) { return {g.b[i], 0.0}; }
+  static __device__ double commit(const BatchArgs &g, int i, int s, const V2 &v) { return __dmul_rn(v.a, v.a); }
   static __device__ void finalize(const BatchArgs &g, int s, double t) {
     BatchSys &y = g.sys[s];
     y.bb = t;
@@ -112,11 +121,15 @@ struct PhBnorm {  // bb = b.b
 };
 
 struct PhInit64 {  // r = b - A x, p = r, rtrans = r.r
+  static constexpr int kUnroll = 1;  // a row's 27 loads already overlap
+  static constexpr bool kGather = true;
   static __device__ bool active(const BatchArgs &g, int s) { return true; }
-  static __device__ double row(const BatchArgs &g, int i, int s) {
-    const double ri = __dsub_rn(g.b[i], row_fp64(g, i, s, g.x));
-    g.r[i] = ri;
-    return __dmul_rn(ri, ri);
+  static __device__ V2 value(const BatchArgs &g, int i, int s) {
+    return {__dsub_rn(g.b[i], row_fp64(g, i, s, g.x)), 0.0};
+  }
+  static __device__ double commit(const BatchArgs &g, int i, int s, const V2 &v) {
+    g.r[i] = v.a;
+    return __dmul_rn(v.a, v.a);
   }
   static __device__ void finalize(const BatchArgs &g, int s, double t) {
     BatchSys &y = g.sys[s];
@@ -130,11 +143,13 @@ struct PhInit64 {  // r = b - A x, p = r, rtrans = r.r
 };
 
 struct PhSpmvDot64 {  // Ap = A p, alpha = rtrans / p.Ap
+  static constexpr int kUnroll = 1;  // a row's 27 loads already overlap
+  static constexpr bool kGather = true;
   static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].active; }
-  static __device__ double row(const BatchArgs &g, int i, int s) {
-    const double ai = row_fp64(g, i, s, g.p);
-    g.Ap[i] = ai;
-    return __dmul_rn(g.p[i], ai);
+  static __device__ V2 value(const BatchArgs &g, int i, int s) { return {row_fp64(g, i, s, g.p), g.p[i]}; }
+  static __device__ double commit(const BatchArgs &g, int i, int s, const V2 &v) {
+    g.Ap[i] = v.a;
+    return __dmul_rn(v.b, v.a);
   }
   static __device__ void finalize(const BatchArgs &g, int s, double t) {
     BatchSys &y = g.sys[s];
@@ -151,13 +166,17 @@ struct PhSpmvDot64 {  // Ap = A p, alpha = rtrans / p.Ap
 };
 
 struct PhUpdate64 {  // x += alpha p, r -= alpha Ap, beta, per-system stop test
+  static constexpr int kUnroll = 4;
+  static constexpr bool kGather = false;
   static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].active; }
-  static __device__ double row(const BatchArgs &g, int i, int s) {
+  static __device__ V2 value(const BatchArgs &g, int i, int s) {
     const double a = g.sys[s].alpha;
-    g.x[i] = __dadd_rn(g.x[i], __dmul_rn(a, g.p[i]));
-    const double ri = __dadd_rn(g.r[i], __dmul_rn(-a, g.Ap[i]));
-    g.r[i] = ri;
-    return __dmul_rn(ri, ri);
+    return {__dadd_rn(g.x[i], __dmul_rn(a, g.p[i])), __dadd_rn(g.r[i], __dmul_rn(-a, g.Ap[i]))};
+  }
+  static __device__ double commit(const BatchArgs &g, int i, int s, const V2 &v) {
+    g.x[i] = v.a;
+    g.r[i] = v.b;
+    return __dmul_rn(v.b, v.b);
   }
   static __device__ void finalize(const BatchArgs &g, int s, double t) {
     BatchSys &y = g.sys[s];
@@ -176,11 +195,13 @@ struct PhUpdate64 {  // x += alpha p, r -= alpha Ap, beta, per-system stop test
 };
 
 struct PhResidual64 {  // final r = b - A x, relres (all systems)
+  static constexpr int kUnroll = 1;  // a row's 27 loads already overlap
+  static constexpr bool kGather = true;
   static __device__ bool active(const BatchArgs &g, int s) { return true; }
-  static __device__ double row(const BatchArgs &g, int i, int s) {
-    const double ri = __dsub_rn(g.b[i], row_fp64(g, i, s, g.x));
-    return __dmul_rn(ri, ri);
+  static __device__ V2 value(const BatchArgs &g, int i, int s) {
+    return {__dsub_rn(g.b[i], row_fp64(g, i, s, g.x)), 0.0};
   }
+  static __device__ double commit(const BatchArgs &g, int i, int s, const V2 &v) { return __dmul_rn(v.a, v.a); }
   static __device__ void finalize(const BatchArgs &g, int s, double t) {
     BatchSys &y = g.sys[s];
     y.relres = y.bb > 0.0 ? sqrt(t / y.bb) : 0.0;
@@ -191,11 +212,15 @@ struct PhResidual64 {  // final r = b - A x, relres (all systems)
 
 // -- iterative refinement phases --
 struct PhOuter64 {  // r64 = b - A x, relres, outer decision (systems still refining)
+  static constexpr int kUnroll = 1;  // a row's 27 loads already overlap
+  static constexpr bool kGather = true;
   static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].active; }
-  static __device__ double row(const BatchArgs &g, int i, int s) {
-    const double ri = __dsub_rn(g.b[i], row_fp64(g, i, s, g.x));
-    g.r[i] = ri;
-    return __dmul_rn(ri, ri);
+  static __device__ V2 value(const BatchArgs &g, int i, int s) {
+    return {__dsub_rn(g.b[i], row_fp64(g, i, s, g.x)), 0.0};
+  }
+  static __device__ double commit(const BatchArgs &g, int i, int s, const V2 &v) {
+    g.r[i] = v.a;
+    return __dmul_rn(v.a, v.a);
   }
   static __device__ void finalize(const BatchArgs &g, int s, double t) {
     BatchSys &y = g.sys[s];
@@ -217,9 +242,14 @@ struct PhOuter64 {  // r64 = b - A x, relres, outer decision (systems still refi
 };
 
 struct PhStartInner {  // r32 = r64 / ||r64||, d = 0, rr0
+  static constexpr int kUnroll = 4;
+  static constexpr bool kGather = false;
   static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].active; }
-  static __device__ double row(const BatchArgs &g, int i, int s) {
-    const float ri = (float)(g.r[i] / g.sys[s].scale);
+  static __device__ V2 value(const BatchArgs &g, int i, int s) {
+    return {(double)(float)(g.r[i] / g.sys[s].scale), 0.0};
+  }
+  static __device__ double commit(const BatchArgs &g, int i, int s, const V2 &v) {
+    const float ri = (float)v.a;
     g.r32[i] = ri;
     g.d32[i] = 0.f;
     return (double)ri * ri;
@@ -236,11 +266,16 @@ struct PhStartInner {  // r32 = r64 / ||r64||, d = 0, rr0
 
 template <typename VT>
 struct PhSpmvDotLp {
+  static constexpr int kUnroll = 1;  // a row's 27 loads already overlap
+  static constexpr bool kGather = true;
   static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].inner_active; }
-  static __device__ double row(const BatchArgs &g, int i, int s) {
-    const float ai = row_lp<VT>(g, i, s, g.p32);
+  static __device__ V2 value(const BatchArgs &g, int i, int s) {
+    return {(double)row_lp<VT>(g, i, s, g.p32), (double)g.p32[i]};
+  }
+  static __device__ double commit(const BatchArgs &g, int i, int s, const V2 &v) {
+    const float ai = (float)v.a;
     g.Ap32[i] = ai;
-    return (double)g.p32[i] * ai;
+    return v.b * ai;
   }
   static __device__ void finalize(const BatchArgs &g, int s, double t) {
     BatchSys &y = g.sys[s];
@@ -256,11 +291,16 @@ struct PhSpmvDotLp {
 };
 
 struct PhUpdateLp {  // d += alpha p, r -= alpha Ap, inner stop test
+  static constexpr int kUnroll = 4;
+  static constexpr bool kGather = false;
   static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].inner_active; }
-  static __device__ double row(const BatchArgs &g, int i, int s) {
+  static __device__ V2 value(const BatchArgs &g, int i, int s) {
     const float a = (float)g.sys[s].alpha;
-    g.d32[i] = fmaf(a, g.p32[i], g.d32[i]);
-    const float ri = fmaf(-a, g.Ap32[i], g.r32[i]);
+    return {(double)fmaf(a, g.p32[i], g.d32[i]), (double)fmaf(-a, g.Ap32[i], g.r32[i])};
+  }
+  static __device__ double commit(const BatchArgs &g, int i, int s, const V2 &v) {
+    const float ri = (float)v.b;
+    g.d32[i] = (float)v.a;
     g.r32[i] = ri;
     return (double)ri * ri;
   }
@@ -281,25 +321,90 @@ __device__ __forceinline__ void set_cond(const BatchArgs &g, int which, int v) {
   cudaGraphSetConditional(which == 1 ? g.c_outer : g.c_inner, (unsigned)v);
 }
 
+// Each warp takes whole tiles (tile t goes to warp t mod the grid's warps).
+// A chunk's partial: lane l sums rows r0 + l + 32k, k = 0..15, in k order,
+// then the fixed warp butterfly; so it depends on neither the schedule nor
+// the warp that forms it.
+// Stored-matrix rows of the SpMV phases (gathers through the column indices)
+// want more rows in flight: a block takes whole tiles, warp w reads rows
+// r0 + l + 32k for k = 2w, 2w+1, and warp 0 sums each lane's 16 terms in k
+// order before the butterfly, so the partial equals the one-warp form's bit
+// for bit (a row past the tile adds +0.0, which never changes such a sum).
 template <class Ph>
-__global__ void __launch_bounds__(256, 4) k_batch_phase(BatchArgs g) {
-  __shared__ double smem[32];
-  __shared__ bool s_last;
+__device__ __forceinline__ void phase_block_tiles(const BatchArgs &g, double (*sv)[32]) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
     const int4 tile = g.tiles[t];
     const int s = tile.x;
     if (!Ph::active(g, s)) continue;  // uniform over the block
     const int nch = (tile.z - tile.y + kChunk - 1) / kChunk;
     for (int c = 0; c < nch; ++c) {
-      const int r0 = tile.y + c * kChunk;
-      const int i0 = r0 + threadIdx.x, i1 = i0 + 256;
-      double v0 = 0.0, v1 = 0.0;
-      if (i0 < tile.z) v0 = Ph::row(g, i0, s);
-      if (i1 < tile.z) v1 = Ph::row(g, i1, s);
-      const double cs = block_sum<256>(__dadd_rn(v0, v1), smem);
-      if (threadIdx.x == 0) g.part[tile.w + c] = cs;
+      const int r0 = tile.y + c * kChunk, rend = min(tile.z, r0 + kChunk);
+      V2 val[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int i = r0 + (2 * w + u) * 32 + lane;
+        if (i < rend) val[u] = Ph::value(g, i, s);
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int i = r0 + (2 * w + u) * 32 + lane;
+        sv[2 * w + u][lane] = i < rend ? Ph::commit(g, i, s, val[u]) : 0.0;
+      }
+      __syncthreads();
+      if (w == 0) {
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < kChunk / 32; ++k) v = __dadd_rn(v, sv[k][lane]);
+        v = warp_sum(v);
+        if (lane == 0) {
+          g.part[tile.w + c] = v;
+          __threadfence();
+        }
+      }
+      __syncthreads();
     }
   }
+}
+
+template <class Ph>
+__global__ void __launch_bounds__(256, 4) k_batch_phase(BatchArgs g) {
+  __shared__ bool s_last;
+  __shared__ double sv[kChunk / 32][32];
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * 8;
+  if (Ph::kGather && !g.dims) {
+    phase_block_tiles<Ph>(g, sv);
+  } else
+  for (int t = blockIdx.x * 8 + (threadIdx.x >> 5); t < g.ntiles; t += nw) {
+    const int4 tile = g.tiles[t];
+    const int s = tile.x;
+    if (!Ph::active(g, s)) continue;  // uniform over the warp
+    const int nch = (tile.z - tile.y + kChunk - 1) / kChunk;
+    for (int c = 0; c < nch; ++c) {
+      const int r0 = tile.y + c * kChunk, rend = min(tile.z, r0 + kChunk);
+      double v = 0.0;
+      for (int k0 = 0; k0 < kChunk / 32; k0 += Ph::kUnroll) {
+        V2 val[Ph::kUnroll];
+#pragma unroll
+        for (int u = 0; u < Ph::kUnroll; ++u) {
+          const int i = r0 + (k0 + u) * 32 + lane;
+          if (i < rend) val[u] = Ph::value(g, i, s);
+        }
+#pragma unroll
+        for (int u = 0; u < Ph::kUnroll; ++u) {
+          const int i = r0 + (k0 + u) * 32 + lane;
+          if (i < rend) v = __dadd_rn(v, Ph::commit(g, i, s, val[u]));
+        }
+      }
+      v = warp_sum(v);
+      if (lane == 0) {
+        g.part[tile.w + c] = v;
+        __threadfence();
+      }
+    }
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     s_last = atomicAdd(g.counter, 1u) == gridDim.x - 1;
@@ -308,7 +413,7 @@ __global__ void __launch_bounds__(256, 4) k_batch_phase(BatchArgs g) {
   if (!s_last) return;
   __threadfence();
   // one warp per system: lanes stride the system's chunks, fixed butterfly
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int warp = threadIdx.x >> 5;
   for (int s = warp; s < g.nsys; s += 8) {
     if (!Ph::active(g, s)) continue;
     double v = 0.0;
@@ -331,38 +436,70 @@ __global__ void __launch_bounds__(256, 4) k_batch_phase(BatchArgs g) {
   }
 }
 
-// Element-wise phases without a reduction, persistent over the same tiles.
+// Element-wise phases without a reduction, persistent over the same tiles
+// (one warp per tile, 32 consecutive rows per step; each lane reads four rows
+// before it stores any, as in the phases above).
+template <class F>
+__device__ __forceinline__ void batch_rows4(int lo, int hi, F &&f) {
+  const int lane = threadIdx.x & 31;
+  for (int i0 = lo + lane; i0 < hi; i0 += 128) {
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (i0 + 32 * u < hi) v[u] = f.value(i0 + 32 * u);
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (i0 + 32 * u < hi) f.commit(i0 + 32 * u, v[u]);
+  }
+}
+
 __global__ void __launch_bounds__(256) k_batch_p64(BatchArgs g) {
-  for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
+  const int nw = gridDim.x * 8;
+  for (int t = blockIdx.x * 8 + (threadIdx.x >> 5); t < g.ntiles; t += nw) {
     const int4 tile = g.tiles[t];
     const BatchSys &y = g.sys[tile.x];
     if (!y.active) continue;
-    const bool first = y.k == 0;
-    const double beta = y.beta;
-    for (int i = tile.y + threadIdx.x; i < tile.z; i += 256)
-      g.p[i] = first ? g.r[i] : __dadd_rn(g.r[i], __dmul_rn(beta, g.p[i]));
+    struct {
+      const BatchArgs &g;
+      bool first;
+      double beta;
+      __device__ double value(int i) const { return first ? g.r[i] : __dadd_rn(g.r[i], __dmul_rn(beta, g.p[i])); }
+      __device__ void commit(int i, double v) const { g.p[i] = v; }
+    } f{g, y.k == 0, y.beta};
+    batch_rows4(tile.y, tile.z, f);
   }
 }
 
 __global__ void __launch_bounds__(256) k_batch_p32(BatchArgs g) {
-  for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
+  const int nw = gridDim.x * 8;
+  for (int t = blockIdx.x * 8 + (threadIdx.x >> 5); t < g.ntiles; t += nw) {
     const int4 tile = g.tiles[t];
     const BatchSys &y = g.sys[tile.x];
     if (!y.inner_active) continue;
-    const bool first = y.inner_k == 0;
-    const float beta = (float)y.beta;
-    for (int i = tile.y + threadIdx.x; i < tile.z; i += 256)
-      g.p32[i] = first ? g.r32[i] : fmaf(beta, g.p32[i], g.r32[i]);
+    struct {
+      const BatchArgs &g;
+      bool first;
+      float beta;
+      __device__ double value(int i) const { return first ? g.r32[i] : fmaf(beta, g.p32[i], g.r32[i]); }
+      __device__ void commit(int i, double v) const { g.p32[i] = (float)v; }
+    } f{g, y.inner_k == 0, (float)y.beta};
+    batch_rows4(tile.y, tile.z, f);
   }
 }
 
 __global__ void __launch_bounds__(256) k_batch_end_inner(BatchArgs g) {
-  for (int t = blockIdx.x; t < g.ntiles; t += gridDim.x) {
+  const int nw = gridDim.x * 8;
+  for (int t = blockIdx.x * 8 + (threadIdx.x >> 5); t < g.ntiles; t += nw) {
     const int4 tile = g.tiles[t];
     const BatchSys &y = g.sys[tile.x];
     if (!y.active) continue;
-    const double scale = y.scale;
-    for (int i = tile.y + threadIdx.x; i < tile.z; i += 256) g.x[i] = fma(scale, (double)g.d32[i], g.x[i]);
+    struct {
+      const BatchArgs &g;
+      double scale;
+      __device__ double value(int i) const { return fma(scale, (double)g.d32[i], g.x[i]); }
+      __device__ void commit(int i, double v) const { g.x[i] = v; }
+    } f{g, y.scale};
+    batch_rows4(tile.y, tile.z, f);
   }
 }
 

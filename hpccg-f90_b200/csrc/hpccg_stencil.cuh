@@ -75,12 +75,11 @@ __device__ __forceinline__ PlaneSpan plane_span(const PlaneMap &m, int nz) {
   return s;
 }
 
-// Grid-stride form (any row order): one row from 27 loads.
+// One row from 27 loads, row i at grid position (ix, iy, iz).
 template <typename Real>
-__device__ __forceinline__ Real stencil_row(int i, const StencilGeom &g, const Real *__restrict__ x) {
+__device__ __forceinline__ Real stencil_row_at(int i, int ix, int iy, int iz, const StencilGeom &g,
+                                               const Real *__restrict__ x) {
   const int nxy = g.nx * g.ny;
-  const int iz = i / nxy, rem = i - iz * nxy;
-  const int iy = rem / g.nx, ix = rem - iy * g.nx;
   const bool has_l = ix > 0, has_r = ix < g.nx - 1;
   Real s = Real(0);
 #pragma unroll
@@ -104,6 +103,14 @@ __device__ __forceinline__ Real stencil_row(int i, const StencilGeom &g, const R
     }
   }
   return s;
+}
+// Grid-stride form (any row order).
+template <typename Real>
+__device__ __forceinline__ Real stencil_row(int i, const StencilGeom &g, const Real *__restrict__ x) {
+  const int nxy = g.nx * g.ny;
+  const int iz = i / nxy, rem = i - iz * nxy;
+  const int iy = rem / g.nx, ix = rem - iy * g.nx;
+  return stencil_row_at<Real>(i, ix, iy, iz, g, x);
 }
 
 // Bit j = (sy+1)*3 + (sx+1) set when neighbour (sy, sx) of column (ix, iy)
