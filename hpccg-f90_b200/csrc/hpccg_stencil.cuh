@@ -127,17 +127,13 @@ __device__ __forceinline__ unsigned stencil_mask(const StencilGeom &g, int ix, i
 
 // Loads the 3x3 neighbourhood (sy, sx order) of the thread's column in the
 // plane that `p` points into (p = &x[column + z*plane]); `mask` bit j clear
-// (or zin false) gives 0 for neighbour j, which lies outside the grid.  FULL:
-// the caller knows all nine neighbours lie inside the grid (mask == 0x1FF).
-template <typename Real, bool FULL = false>
+// (or zin false) gives 0 for neighbour j, which lies outside the grid.
+template <typename Real>
 __device__ __forceinline__ void stencil_plane(const Real *__restrict__ p, int nx, unsigned mask, bool zin, Real *v) {
 #pragma unroll
   for (int j = 0; j < 9; ++j) {
     const int off = (j / 3 - 1) * nx + (j % 3 - 1);
-    if (FULL)
-      v[j] = zin ? __ldg(p + off) : Real(0);
-    else
-      v[j] = (zin && ((mask >> j) & 1u)) ? __ldg(p + off) : Real(0);
+    v[j] = (zin && ((mask >> j) & 1u)) ? __ldg(p + off) : Real(0);
   }
 }
 
@@ -369,16 +365,16 @@ __device__ __forceinline__ double stencil_rows_box64x4(const StencilGeom &g, con
 // of plane z-1 added to 0 in order; that prefix depends on plane z-1 alone,
 // so it is formed once per plane (lead) and the window keeps only planes z
 // and z+1 in full.  epi(i, rowsum, x_i) stores and returns a dot term.
-template <typename Real, bool FULL, class Epi>
+template <typename Real, class Epi>
 __device__ __forceinline__ double stencil_column(const PlaneSpan &sp, const StencilGeom &g, const PlaneMap &m,
                                                  unsigned mask, const Real *__restrict__ pc, Epi &epi) {
   double part = 0.0;
   Real b[9], c[9];
-  stencil_plane<Real, FULL>(pc + (int64_t)(sp.z0 - 1) * m.plane, g.nx, mask, sp.z0 > 0, c);
+  stencil_plane<Real>(pc + (int64_t)(sp.z0 - 1) * m.plane, g.nx, mask, sp.z0 > 0, c);
   Real lead = stencil_lead<Real>(c);
-  stencil_plane<Real, FULL>(pc + (int64_t)sp.z0 * m.plane, g.nx, mask, true, b);
+  stencil_plane<Real>(pc + (int64_t)sp.z0 * m.plane, g.nx, mask, true, b);
   for (int z = sp.z0; z < sp.z1; ++z) {
-    stencil_plane<Real, FULL>(pc + (int64_t)(z + 1) * m.plane, g.nx, mask, z + 1 < g.nz, c);
+    stencil_plane<Real>(pc + (int64_t)(z + 1) * m.plane, g.nx, mask, z + 1 < g.nz, c);
     const Real s = stencil_tail<Real>(lead, b, c);
     if constexpr (sizeof(Real) == 8)
       part = __dadd_rn(part, epi(sp.c + z * m.plane, s, b[4]));
@@ -387,6 +383,71 @@ __device__ __forceinline__ double stencil_column(const PlaneSpan &sp, const Sten
     lead = stencil_lead<Real>(b);
 #pragma unroll
     for (int j = 0; j < 9; ++j) b[j] = c[j];
+  }
+  return part;
+}
+
+// The 3x3 neighbourhood of an interior column in the plane `p` points into:
+// three row pointers with +-1 offsets (immediates), no tests.
+template <typename Real>
+__device__ __forceinline__ void stencil_plane3(const Real *__restrict__ p, int nx, Real *v) {
+  const Real *r0 = p - nx, *r2 = p + nx;
+  v[0] = __ldg(r0 - 1), v[1] = __ldg(r0), v[2] = __ldg(r0 + 1);
+  v[3] = __ldg(p - 1), v[4] = __ldg(p), v[5] = __ldg(p + 1);
+  v[6] = __ldg(r2 - 1), v[7] = __ldg(r2), v[8] = __ldg(r2 + 1);
+}
+// Row z from the lead (its plane z-1 prefix), plane z (b) and plane z+1 (c);
+// then the lead of row z+1.
+template <typename Real, class Epi>
+__device__ __forceinline__ void stencil_step(int i, Real &lead, const Real *b, const Real *c, double &part,
+                                             Epi &epi) {
+  const Real s = stencil_tail<Real>(lead, b, c);
+  if constexpr (sizeof(Real) == 8)
+    part = __dadd_rn(part, epi(i, s, b[4]));
+  else
+    part += epi(i, s, b[4]);
+  lead = stencil_lead<Real>(b);
+}
+// stencil_column for a column whose nine neighbours lie inside the grid in x
+// and y: the planes inside the grid load without selects (the last plane of
+// the grid is peeled off), and the loop runs two planes per trip so the
+// window's two halves trade roles instead of being copied.  Same sums.
+template <typename Real, class Epi>
+__device__ __forceinline__ double stencil_column_interior(const PlaneSpan &sp, const StencilGeom &g,
+                                                          const PlaneMap &m, const Real *__restrict__ pc,
+                                                          Epi &epi) {
+  double part = 0.0;
+  Real b[9], c[9];
+  const int64_t pl = m.plane;
+  if (sp.z0 > 0) {
+    stencil_plane3<Real>(pc + (sp.z0 - 1) * pl, g.nx, c);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) c[j] = Real(0);
+  }
+  Real lead = stencil_lead<Real>(c);
+  stencil_plane3<Real>(pc + sp.z0 * pl, g.nx, b);
+  const int zi = min(sp.z1, g.nz - 1);  // rows whose plane z+1 lies inside the grid
+  const Real *p = pc + (sp.z0 + 1) * pl;
+  int z = sp.z0;
+  for (; z + 1 < zi; z += 2) {
+    stencil_plane3<Real>(p, g.nx, c);
+    stencil_step<Real>(sp.c + z * m.plane, lead, b, c, part, epi);
+    stencil_plane3<Real>(p + pl, g.nx, b);
+    stencil_step<Real>(sp.c + (z + 1) * m.plane, lead, c, b, part, epi);
+    p += 2 * pl;
+  }
+  if (z < zi) {
+    stencil_plane3<Real>(p, g.nx, c);
+    stencil_step<Real>(sp.c + z * m.plane, lead, b, c, part, epi);
+#pragma unroll
+    for (int j = 0; j < 9; ++j) b[j] = c[j];
+    ++z;
+  }
+  if (z < sp.z1) {  // z = nz - 1: no plane above
+#pragma unroll
+    for (int j = 0; j < 9; ++j) c[j] = Real(0);
+    stencil_step<Real>(sp.c + z * m.plane, lead, b, c, part, epi);
   }
   return part;
 }
@@ -404,8 +465,8 @@ __device__ __forceinline__ double stencil_rows(int n, const StencilGeom &g, cons
     // warps whose columns all lie off the x and y faces load without the
     // per-neighbour tests (the sums are the same: masked terms are zeros)
     if (__all_sync(__activemask(), mask == 0x1FFu))
-      return stencil_column<Real, true>(sp, g, m, mask, x + sp.c, epi);
-    return stencil_column<Real, false>(sp, g, m, mask, x + sp.c, epi);
+      return stencil_column_interior<Real>(sp, g, m, x + sp.c, epi);
+    return stencil_column<Real>(sp, g, m, mask, x + sp.c, epi);
   }
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
