@@ -294,3 +294,32 @@ def test_fused_zero_rhs_exact_start_and_caps(hp):
     # the inner iteration cap: at most max_inner x updates per cycle
     x, info, status = M.solve_mixed(b, np.zeros_like(b), 1, rel_tol=1e-8, max_outer=30, max_inner=3)
     assert status == hp.HPCCG_OK and info.inner_iters <= 3 * info.outer_iters
+
+
+def test_fused_pass_entry_point_errors(hp, torch):
+    """The fused-pass entry points reject what they cannot run: a stored-matrix
+    context (no grid) has no fused iteration, a grid with nx % 4 != 0 neither;
+    bad arguments are HPCCG_ERR_INVALID_ARG."""
+    A, x, b, xe = oracle.generate_matrix(6, 5, 4)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    assert not M.mixed_fused()
+    v = torch.zeros(A.nrow, dtype=torch.float32, device="cuda")
+    with pytest.raises(hp.HpccgError) as e:
+        M.mixed_pass(v, v.clone(), v.clone(), v.clone(), v.clone(), 0.5, 0.5, False)
+    assert e.value.code == hp.HPCCG_ERR_UNSUPPORTED
+    G = hp.Matrix.generated(6, 5, 4)  # nx % 4 != 0: the three-kernel iteration
+    G.set_spmv(hp.SPMV_STENCIL)
+    assert not G.mixed_fused()
+    with pytest.raises(hp.HpccgError) as e:
+        G.mixed_pass(v, v.clone(), v.clone(), v.clone(), v.clone(), 0.5, 0.5, False)
+    assert e.value.code == hp.HPCCG_ERR_UNSUPPORTED
+    H = hp.Matrix.generated(8, 5, 4)
+    H.set_spmv(hp.SPMV_STENCIL)
+    assert H.mixed_fused()
+    with pytest.raises(hp.HpccgError) as e:
+        hp._check(hp._lib.hpccg_gpu_set_mixed_fused(H._h, 2), "set_mixed_fused")
+    assert e.value.code == hp.HPCCG_ERR_INVALID_ARG
+    H.set_mixed_fused(False)
+    assert not H.mixed_fused()
+    H.set_mixed_fused(True)
+    assert H.mixed_fused()
