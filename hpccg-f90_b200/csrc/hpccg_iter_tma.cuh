@@ -125,8 +125,9 @@ __device__ __forceinline__ bool it_step(const int s, const ItCta &c, unsigned ch
                                         ItGen &cur, const ItGen &prv, ItRun &run, float *r_out, float *p_out,
                                         float *d, const IterScalars &sc, int *status) {
   float *const nbuf = reinterpret_cast<float *>(smem + kItStages * kItStageBytes);
-  // ---- phase B: Ap'(s-3) from p' planes s-4 .. s-2 (plane s-2 made last step)
-  if (s >= c.z0 + 1) {
+  // ---- phase B: Ap'(s-3) from p' planes s-4 .. s-2 (plane s-2 made last step);
+  // nothing at s = z1 + 3, the extra step of an odd count under the two-step loop
+  if (s >= c.z0 + 1 && s <= c.z1 + 2) {
     float ls[4][4];
     const float *nb = nbuf + (s & 1) * kItNFloats + c.tyo - kItBoxX + c.txo;  // N(s-2), line yc-1
 #pragma unroll
