@@ -323,3 +323,21 @@ def test_fused_pass_entry_point_errors(hp, torch):
     assert not H.mixed_fused()
     H.set_mixed_fused(True)
     assert H.mixed_fused()
+
+
+def test_fused_solve_non_cubic_partial_tiles(hp):
+    """The fused inner iteration on a grid that fills no tile completely in x
+    or y (40 x 70 x 9: tiles of 32 x 64), FP32 and BF16, against the oracle."""
+    nx, ny, nz = 40, 70, 9
+    A, x, b1, xe = oracle.generate_matrix(nx, ny, nz)
+    xstar = oracle.uniform_pm1(77, A.nrow)
+    b = oracle.spmv(A, xstar)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    M.set_geometry(nx, ny, nz)
+    M.set_spmv(hp.SPMV_STENCIL)
+    assert M.mixed_fused()
+    for prec in (1, 2):
+        xs, info, status = M.solve_mixed(b, np.zeros_like(b), prec, rel_tol=1e-8)
+        assert status == hp.HPCCG_OK
+        assert oracle.true_relres(A, b, xs) <= 1e-8
+        assert np.abs(xs - xstar).max() <= 1e-7
