@@ -72,6 +72,7 @@ struct hpccg_ctx {
   // SpMV selection
   int spmv_kind = HPCCG_SPMV_AUTO;
   int spmv_param = 0;
+  bool mixed_fused_off = false;  // hpccg_gpu_set_mixed_fused(ctx, 0)
   bool spmv_tuned = false;
   // CG graph
   cudaGraph_t cg_graph = nullptr;

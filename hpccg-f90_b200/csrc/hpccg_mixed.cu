@@ -555,7 +555,6 @@ struct MixedRes {
   CUtensorMap itmap[5];  // p0, p1, r0, r1 and d
   TmaTile itile{};
   bool iter = false;
-  bool want_fused = true;  // hpccg_gpu_set_mixed_fused
   bool exec_fused[3] = {false, false, false};
 };
 
@@ -670,7 +669,9 @@ static int mixed_res(hpccg_ctx *c, int precision, MixedRes **out) {
 }
 
 static bool use_tma(const hpccg_ctx *c, const MixedRes *m) { return uses_stencil(c) && m->tma; }
-static bool use_iter(const hpccg_ctx *c, const MixedRes *m) { return uses_stencil(c) && m->iter && m->want_fused; }
+static bool use_iter(const hpccg_ctx *c, const MixedRes *m) {
+  return uses_stencil(c) && m->iter && !c->mixed_fused_off;
+}
 
 static void launch_iter(hpccg_ctx *c, MixedRes *m, const MixedArgs &g, cudaStream_t s) {
   const IterBufs b{{m->r, m->r2}, {m->p, m->p2}};
@@ -1073,20 +1074,17 @@ extern "C" int hpccg_gpu_time_mixed_kernels(hpccg_ctx *c, int32_t precision, int
   return HPCCG_OK;
 }
 
+// A flag of the context: allocates nothing (the next solve picks it up).
 extern "C" int hpccg_gpu_set_mixed_fused(hpccg_ctx *c, int32_t on) {
   if (!c || (on != 0 && on != 1)) return HPCCG_ERR_INVALID_ARG;
-  for (int precision = HPCCG_PREC_FP32; precision <= HPCCG_PREC_BF16; ++precision) {
-    MixedRes *m = nullptr;
-    const int rc = mixed_res(c, precision, &m);
-    if (rc == HPCCG_ERR_UNSUPPORTED) return HPCCG_OK;  // no inner solver on this context: nothing to select
-    if (rc) return rc;
-    m->want_fused = on != 0;
-  }
+  c->mixed_fused_off = on == 0;
   return HPCCG_OK;
 }
 
 extern "C" int hpccg_gpu_mixed_fused(hpccg_ctx *c, int32_t *fused) {
   if (!c || !fused) return HPCCG_ERR_INVALID_ARG;
+  *fused = 0;
+  if (!uses_stencil(c)) return HPCCG_OK;  // stored-matrix inner solves: three kernels (no values copied here)
   MixedRes *m = nullptr;
   const int rc = mixed_res(c, HPCCG_PREC_FP32, &m);
   if (rc) return rc;
