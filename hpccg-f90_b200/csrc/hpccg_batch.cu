@@ -1046,8 +1046,11 @@ static int ensure_lp(hpccg_batch *B, int precision) {
   return HPCCG_OK;
 }
 
-// Times one FP64 SpMV+dot phase per candidate schedule and keeps the fastest.
-// Candidates differ only in tile size and grid, so the solves they produce are
+// Times one FP64 CG iteration (p update, SpMV + dot, r update) per candidate
+// schedule and keeps the fastest.  It runs before a solve copies b and x in,
+// on the solver's scratch vectors, with every system's scalars reset before
+// each phase so that all systems stay active whatever the data.  Candidates
+// differ only in tile size and grid, so the solves they produce are
 // bit-identical.
 static int autotune(hpccg_batch *B) {
   if (B->tuned) return HPCCG_OK;
@@ -1060,19 +1063,30 @@ static int autotune(hpccg_batch *B) {
   for (auto &y : hs) {
     y = BatchSys{};
     y.active = 1;
+    y.k = 1;
     y.rtrans = 1.0;
+    y.alpha = 0.5;
+    y.beta = 0.5;
+    y.tol2 = -1.0;  // never converged
   }
+  const size_t sys_bytes = sizeof(BatchSys) * B->nsys;
   for (int t : tiles)
     for (int b : bps) {
       int rc = build_tiles(B, t);
       if (rc) return rc;
       B->blocks_per_sm = b;
       BatchArgs g = batch_args(B, HPCCG_PREC_FP64);
+      g.max_iter = 1 << 30;
       float ms = 0.f;
       for (int rep = 0; rep < 4; ++rep) {
-        HPCCG_CUDA(cudaMemcpyAsync(B->sys, hs.data(), sizeof(BatchSys) * B->nsys, cudaMemcpyHostToDevice, B->stream));
         if (rep == 1) HPCCG_CUDA(cudaEventRecord(B->ev0, B->stream));
+        HPCCG_CUDA(cudaMemcpyAsync(B->sys, hs.data(), sys_bytes, cudaMemcpyHostToDevice, B->stream));
+        k_batch_p64<<<grid_of(B), 256, 0, B->stream>>>(g);
+        HPCCG_CUDA(cudaGetLastError());
+        HPCCG_CUDA(cudaMemcpyAsync(B->sys, hs.data(), sys_bytes, cudaMemcpyHostToDevice, B->stream));
         HPCCG_CUDA(phase<PhSpmvDot64>(B, g, B->stream));
+        HPCCG_CUDA(cudaMemcpyAsync(B->sys, hs.data(), sys_bytes, cudaMemcpyHostToDevice, B->stream));
+        HPCCG_CUDA(phase<PhUpdate64>(B, g, B->stream));
       }
       HPCCG_CUDA(cudaEventRecord(B->ev1, B->stream));
       HPCCG_CUDA(cudaEventSynchronize(B->ev1));
