@@ -77,7 +77,7 @@ template <typename VT>
 __device__ __forceinline__ float row_lp(const BatchArgs &g, int i, int sys, const float *x) {
   if (g.dims) {
     const int4 d = g.dims[sys];
-    return stencil_row<float>(i - d.w, StencilGeom{d.x, d.y, d.z}, x + d.w);
+    return stencil_row_box(i - d.w, StencilGeom{d.x, d.y, d.z}, x + d.w);  // FP32 inner solves: box sums
   }
   float s = 0.f;
   const VT *val = reinterpret_cast<const VT *>(g.val_lp);
