@@ -500,6 +500,9 @@ static TmaTile iter_plan(const hpccg_ctx *c) {
     return none;
   }
   const TmaTile t = tma_tile_plan(c->gx, c->gy, c->gz, c->num_sms * per_sm);
+  // the refinement residual of the fused path reduces four values per block too
+  const PlaneMap q = boxw_map(4, c->gx, c->gy, c->gz, (int64_t)c->num_sms * StratStencilBox64::kMinBlocks * kBlock);
+  if (q.plane <= 0 || plane_grid(q) > kItMaxGrid) return none;
   return tma_tile_grid(t) <= kItMaxGrid ? t : none;
 }
 
@@ -735,11 +738,9 @@ static int launch_residual_f(hpccg_ctx *c, const MixedArgs &g, cudaStream_t s, b
     return (int)cudaGetLastError();
   };
   const PlaneMap q = boxw_map(4, c->gx, c->gy, c->gz, (int64_t)c->num_sms * StratStencilBox64::kMinBlocks * kBlock);
-  if (q.plane > 0) {
-    a.pm = q;
-    return go(StratStencilBox64{});
-  }
-  return go(StratStencil{});
+  if (q.plane <= 0) return HPCCG_ERR_UNSUPPORTED;  // iter_plan admits only grids where this map exists
+  a.pm = q;
+  return go(StratStencilBox64{});
 }
 
 static int launch_residual64(hpccg_ctx *c, const MixedArgs &g, cudaStream_t s) {
