@@ -52,6 +52,7 @@ struct BatchArgs {
   unsigned *counter;
   BatchSys *sys;
   const int4 *dims;         // (nx, ny, nz, first row) per system: matrix-free rows; null = ELL
+  const long long *walk;    // matrix-free rows: nsys+1 prefix of the column walks (columns x z chunks)
   double rel_tol, inner_rtol;
   int max_iter, max_outer, max_inner;
   cudaGraphConditionalHandle c_outer, c_inner;
@@ -314,6 +315,113 @@ struct PhUpdateLp {  // d += alpha p, r -= alpha Ap, inner stop test
   }
   static constexpr int kCond = 2;
 };
+
+// Matrix-free batches form A p by column walks (k_batch_walk64 / 32 below) and
+// then reduce p.Ap here, in the same chunk order as PhSpmvDot64 / PhSpmvDotLp.
+struct PhDot64 {  // alpha = rtrans / p.Ap
+  static constexpr int kUnroll = 4;
+  static constexpr bool kGather = false;
+  static __device__ bool active(const BatchArgs &g, int s) { return PhSpmvDot64::active(g, s); }
+  static __device__ V2 value(const BatchArgs &g, int i, int s) { return {g.Ap[i], g.p[i]}; }
+  static __device__ double commit(const BatchArgs &g, int i, int s, const V2 &v) { return __dmul_rn(v.b, v.a); }
+  static __device__ void finalize(const BatchArgs &g, int s, double t) { PhSpmvDot64::finalize(g, s, t); }
+  static constexpr int kCond = -1;
+};
+struct PhDotLp {
+  static constexpr int kUnroll = 4;
+  static constexpr bool kGather = false;
+  static __device__ bool active(const BatchArgs &g, int s) { return g.sys[s].inner_active; }
+  static __device__ V2 value(const BatchArgs &g, int i, int s) { return {(double)g.Ap32[i], (double)g.p32[i]}; }
+  static __device__ double commit(const BatchArgs &g, int i, int s, const V2 &v) { return v.b * (float)v.a; }
+  static __device__ void finalize(const BatchArgs &g, int s, double t) { PhSpmvDotLp<float>::finalize(g, s, t); }
+  static constexpr int kCond = -1;
+};
+
+// ---- column walks of matrix-free batches -------------------------------------------
+constexpr int kWalkZc = 32;  // z planes per walk
+
+// The walk of work item t: system, column and z range (prefix g.walk).
+struct WalkItem {
+  int s, c, z0, z1;
+  int4 d;
+};
+__device__ __forceinline__ bool walk_item(const BatchArgs &g, long long t, WalkItem &w) {
+  if (t >= g.walk[g.nsys]) return false;
+  int lo = 0, hi = g.nsys;  // g.walk[lo] <= t < g.walk[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (g.walk[mid] <= t) lo = mid;
+    else hi = mid;
+  }
+  w.s = lo;
+  w.d = g.dims[lo];
+  const int plane = w.d.x * w.d.y;
+  const long long local = t - g.walk[lo];
+  const int q = (int)(local / plane);
+  w.c = (int)(local - (long long)q * plane);
+  w.z0 = q * kWalkZc;
+  w.z1 = min(w.d.z, w.z0 + kWalkZc);
+  return true;
+}
+
+struct WalkStore {  // y[i] = row sum (stencil_column's epilogue)
+  double *y;
+  __device__ __forceinline__ double operator()(int i, double s, double) const {
+    y[i] = s;
+    return 0.0;
+  }
+};
+
+// Ap = A p of the active systems (FP64, reference term order: the rows equal
+// the ones PhSpmvDot64 forms, bit for bit).
+__global__ void __launch_bounds__(256, 4) k_batch_walk64(BatchArgs g) {
+  WalkItem w;
+  const bool have = walk_item(g, blockIdx.x * 256LL + threadIdx.x, w) && g.sys[w.s].active;
+  if (!have) return;
+  const StencilGeom geom{w.d.x, w.d.y, w.d.z};
+  const PlaneMap m{w.d.x * w.d.y, kWalkZc, 0, 1};
+  const PlaneSpan sp{w.c, w.z0, w.z1};
+  const int iy = w.c / w.d.x, ix = w.c - iy * w.d.x;
+  const unsigned mask = stencil_mask(geom, ix, iy);
+  WalkStore epi{g.Ap + w.d.w};
+  if (__all_sync(__activemask(), mask == 0x1FFu))
+    stencil_column_interior<double>(sp, geom, m, g.p + w.d.w + w.c, epi);
+  else
+    stencil_column<double>(sp, geom, m, mask, g.p + w.d.w + w.c, epi);
+}
+
+// The same for the FP32 inner solves, rows as 28 x - (plane box sums), the
+// form of stencil_row_box.
+__device__ __forceinline__ float walk_box32(const float *__restrict__ x, int nx, unsigned mask) {
+  float ln[3];
+#pragma unroll
+  for (int sy = 0; sy < 3; ++sy) {
+    const float *r = x + (sy - 1) * nx;
+    const float l = ((mask >> (3 * sy)) & 1u) ? __ldg(r - 1) : 0.f;
+    const float c = ((mask >> (3 * sy + 1)) & 1u) ? __ldg(r) : 0.f;
+    const float rr = ((mask >> (3 * sy + 2)) & 1u) ? __ldg(r + 1) : 0.f;
+    ln[sy] = (l + c) + rr;
+  }
+  return (ln[0] + ln[1]) + ln[2];
+}
+__global__ void __launch_bounds__(256, 4) k_batch_walk32(BatchArgs g) {
+  WalkItem w;
+  const bool have = walk_item(g, blockIdx.x * 256LL + threadIdx.x, w) && g.sys[w.s].inner_active;
+  if (!have) return;
+  const int plane = w.d.x * w.d.y;
+  const int iy = w.c / w.d.x, ix = w.c - iy * w.d.x;
+  const unsigned mask = stencil_mask(StencilGeom{w.d.x, w.d.y, w.d.z}, ix, iy);
+  const float *pc = g.p32 + w.d.w + w.c;
+  float *y = g.Ap32 + w.d.w + w.c;
+  float bm = w.z0 > 0 ? walk_box32(pc + (int64_t)(w.z0 - 1) * plane, w.d.x, mask) : 0.f;
+  float b0 = walk_box32(pc + (int64_t)w.z0 * plane, w.d.x, mask);
+  for (int z = w.z0; z < w.z1; ++z) {
+    const float bp = z + 1 < w.d.z ? walk_box32(pc + (int64_t)(z + 1) * plane, w.d.x, mask) : 0.f;
+    y[(int64_t)z * plane] = fmaf(28.f, __ldg(pc + (int64_t)z * plane), -((bm + b0) + bp));
+    bm = b0;
+    b0 = bp;
+  }
+}
 
 // ---- the persistent phase kernel --------------------------------------------------
 __device__ __forceinline__ void set_cond(const BatchArgs &g, int which, int v) {
@@ -590,6 +698,8 @@ struct hpccg_batch {
   int *d_sys_chunk0 = nullptr;
   int4 *d_tiles = nullptr;
   int4 *d_dims = nullptr;  // generated batches: (nx, ny, nz, first row) per system
+  long long *d_walk = nullptr;  // and the prefix of their column walks (nsys+1)
+  long long walk_total = 0;
   int spmv_kind = HPCCG_SPMV_ELL;
   int ntiles = 0;
   int tile_chunks = 0, blocks_per_sm = 0;  // schedule; 0 = not tuned yet
@@ -604,7 +714,7 @@ static void batch_free(hpccg_batch *B) {
   for (auto &e : B->exec)
     if (e) cudaGraphExecDestroy(e);
   void *bufs[] = {B->col, B->val, B->val32, B->val16, B->x, B->b, B->r, B->p, B->Ap, B->r32, B->p32,
-                  B->Ap32, B->d32, B->part, B->counter, B->sys, B->d_sys_chunk0, B->d_tiles, B->d_dims};
+                  B->Ap32, B->d32, B->part, B->counter, B->sys, B->d_sys_chunk0, B->d_tiles, B->d_dims, B->d_walk};
   for (void *q : bufs)
     if (q) cudaFree(q);
   if (B->ev0) cudaEventDestroy(B->ev0);
@@ -717,10 +827,19 @@ extern "C" int hpccg_batch_create_generated(int32_t nsys, const int32_t *sizes, 
                                                              B->off[s], B->npad, B->col, B->val);
   {
     std::vector<int4> dims(nsys);
-    for (int s = 0; s < nsys; ++s) dims[s] = make_int4(sizes[3 * s], sizes[3 * s + 1], sizes[3 * s + 2], B->off[s]);
+    std::vector<long long> walk(nsys + 1, 0);
+    for (int s = 0; s < nsys; ++s) {
+      dims[s] = make_int4(sizes[3 * s], sizes[3 * s + 1], sizes[3 * s + 2], B->off[s]);
+      const long long chunks = (sizes[3 * s + 2] + kWalkZc - 1) / kWalkZc;
+      walk[s + 1] = walk[s] + (long long)sizes[3 * s] * sizes[3 * s + 1] * chunks;
+    }
+    B->walk_total = walk[nsys];
     cudaError_t e = cudaMalloc(&B->d_dims, sizeof(int4) * nsys);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(B->d_dims, dims.data(), sizeof(int4) * nsys, cudaMemcpyHostToDevice, B->stream);
+    if (e == cudaSuccess) e = cudaMalloc(&B->d_walk, sizeof(long long) * (nsys + 1));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(B->d_walk, walk.data(), sizeof(long long) * (nsys + 1), cudaMemcpyHostToDevice, B->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
     if (e != cudaSuccess) {
       batch_free(B);
@@ -834,6 +953,7 @@ static BatchArgs batch_args(hpccg_batch *B, int precision) {
   g.counter = B->counter;
   g.sys = B->sys;
   g.dims = B->spmv_kind == HPCCG_SPMV_STENCIL ? B->d_dims : nullptr;
+  g.walk = B->d_walk;
   return g;
 }
 
@@ -845,10 +965,23 @@ static cudaError_t phase(hpccg_batch *B, const BatchArgs &g, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+static int walk_grid(const hpccg_batch *B) { return (int)((B->walk_total + 255) / 256); }
+
+// Ap = A p and alpha: one phase on the stored matrix, a column walk and a dot
+// phase on matrix-free rows.
+static cudaError_t launch_spmv_dot64(hpccg_batch *B, const BatchArgs &g, cudaStream_t s) {
+  if (g.dims && g.walk && B->walk_total > 0) {
+    k_batch_walk64<<<walk_grid(B), 256, 0, s>>>(g);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? phase<PhDot64>(B, g, s) : e;
+  }
+  return phase<PhSpmvDot64>(B, g, s);
+}
+
 static cudaError_t launch_cg64_body(hpccg_batch *B, const BatchArgs &g, cudaStream_t s) {
   k_batch_p64<<<grid_of(B), 256, 0, s>>>(g);
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = phase<PhSpmvDot64>(B, g, s);
+  if (e == cudaSuccess) e = launch_spmv_dot64(B, g, s);
   if (e == cudaSuccess) e = phase<PhUpdate64>(B, g, s);
   return e;
 }
@@ -857,7 +990,15 @@ template <typename VT>
 static cudaError_t launch_inner_body(hpccg_batch *B, const BatchArgs &g, cudaStream_t s) {
   k_batch_p32<<<grid_of(B), 256, 0, s>>>(g);
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = phase<PhSpmvDotLp<VT>>(B, g, s);
+  if (e == cudaSuccess) {
+    if (g.dims && g.walk && B->walk_total > 0) {
+      k_batch_walk32<<<walk_grid(B), 256, 0, s>>>(g);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = phase<PhDotLp>(B, g, s);
+    } else {
+      e = phase<PhSpmvDotLp<VT>>(B, g, s);
+    }
+  }
   if (e == cudaSuccess) e = phase<PhUpdateLp>(B, g, s);
   return e;
 }
@@ -1084,7 +1225,7 @@ static int autotune(hpccg_batch *B) {
         k_batch_p64<<<grid_of(B), 256, 0, B->stream>>>(g);
         HPCCG_CUDA(cudaGetLastError());
         HPCCG_CUDA(cudaMemcpyAsync(B->sys, hs.data(), sys_bytes, cudaMemcpyHostToDevice, B->stream));
-        HPCCG_CUDA(phase<PhSpmvDot64>(B, g, B->stream));
+        HPCCG_CUDA(launch_spmv_dot64(B, g, B->stream));
         HPCCG_CUDA(cudaMemcpyAsync(B->sys, hs.data(), sys_bytes, cudaMemcpyHostToDevice, B->stream));
         HPCCG_CUDA(phase<PhUpdate64>(B, g, B->stream));
       }
