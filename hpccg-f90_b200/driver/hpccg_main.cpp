@@ -1,7 +1,7 @@
 // hpccg_main.cpp -- host driver mirroring MPI/src/main.F90 (HPCCGmain, printInfo).
 //
-// The reference keeps its driver in Fortran 90; no Fortran compiler exists in
-// this build environment, so this C++ program is the host side above the
+// The reference keeps its driver in Fortran 90; without a Fortran compiler at
+// hand, this C++ program is the host side above the
 // C-ABI: same command line (`nx ny nz`), same generate_matrix -> printInfo ->
 // cg(max_iter=150, tolerance=0) sequence (main.F90:103-130), same report lines
 // (numerics.F90:103,125,150).  Extra options keep the reference defaults.
