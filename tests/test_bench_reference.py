@@ -1,0 +1,26 @@
+"""The reference arm of bench.py (`--impl reference`) on the CPU: it times the
+oracle (the C restatement of the reference's CG) on the host cores and prints
+one JSON line with the contract's keys, including the one-thread figure and an
+e2e entry that moves no bytes across PCIe.  A 16^3 grid keeps it to a second."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_reference_arm_prints_one_contract_line():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--n", "16",
+                          "--steps", "2", "--warmup", "3"], capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "s" and d["higher_is_better"] is False
+    assert d["value"] > 0 and d["steps"] == 2 and d["warmup"] >= 3
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"]
+    assert cb["value_1thread"] > 0
+    assert d["e2e"] == {"value": d["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert d["config"]["iterations"] > 0
