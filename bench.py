@@ -22,8 +22,9 @@ events on the library stream, max over ranks); config.methods lists every
 solver.  `e2e` is the same solve through the host-array C-ABI call
 (hpccg_gpu_cg / hpccg_gpu_solve_mixed) with b and x0 copied from pinned host
 memory and x copied back inside the timed region.  `roofline` covers the
-dominant kernel of that solver (its SpMV fused with p.Ap).  `cpu_baseline` times the CPU oracle (a C restatement of the
-reference, OpenMP over all host cores) on a bounded sample of the same solve.
+dominant kernel of that solver.  `cpu_baseline` times whole solves of the same
+system by the CPU oracle (a C restatement of the reference, OpenMP over all
+host cores; one-thread figure beside it).
 
 N > 1 GPUs run independent replicas (the path does not shard at one rank:
 no collective in the data path); each rank solves its own system and the
@@ -170,57 +171,68 @@ def _cpu_problem(n: int):
     return oracle, A, b
 
 
-def cpu_reference_time(n: int, sample_iters: int, steps: int, warmup: int, iters_needed: int | None = None):
-    """Seconds to rel-res 1e-8 for the oracle CG with OpenMP on all host cores, from
-    per-iteration samples x the iteration count of one full oracle solve."""
+def cpu_reference_time(n: int, solves: int, warmup: int, solves_1thread: int = 1):
+    """Seconds per complete solve to rel-res 1e-8 of the oracle CG (the reference's loop,
+    MPI/src/numerics.F90:91-147) with OpenMP on all host cores: the median of `solves` whole
+    solves after `warmup` untimed ones.  r, p and Ap are allocated and first-touched once,
+    outside the timed region.  The same for the sequential build (one thread), median of
+    `solves_1thread` whole solves."""
     oracle, A, b = _cpu_problem(n)
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     tol = REL_TOL * float(np.sqrt(np.dot(b, b)))
-    x0 = np.zeros(A.nrow)
-    full_s = None
-    if iters_needed is None:
-        t = time.perf_counter()
-        xs, it, normr, hist = oracle.cg(A, b, x0, 1000, tol, omp=True)
-        full_s = time.perf_counter() - t
-        iters_needed = it
-    per_iter = []
-    for s in range(warmup + steps):
-        t = time.perf_counter()
-        oracle.cg(A, b, x0, sample_iters, 0.0, omp=True)
-        dt = (time.perf_counter() - t) / sample_iters
-        if s >= warmup:
-            per_iter.append(dt)
-    value = float(np.median(per_iter)) * iters_needed
-    # the same on one thread (the oracle's sequential build): median of three one-iteration samples
-    per_iter_1t = []
-    for _ in range(3):
-        t = time.perf_counter()
-        oracle.cg(A, b, x0, 1, 0.0, omp=False)
-        per_iter_1t.append(time.perf_counter() - t)
-    return {"value": value, "per_iter_s": per_iter, "iters": iters_needed, "cores": cores,
-            "full_solve_s": full_s, "sample_iters": sample_iters,
-            "value_1thread": float(np.median(per_iter_1t)) * iters_needed, "per_iter_1thread_s": per_iter_1t}
+    x = np.zeros(A.nrow)
+
+    def timed(omp, count, skip):
+        work = oracle.CgWork(A, omp=omp)
+        out, iters = [], None
+        for s in range(skip + count):
+            x[:] = 0.0
+            t = time.perf_counter()
+            iters, _ = work.solve(b, x, 1000, tol)
+            dt = time.perf_counter() - t
+            if s >= skip:
+                out.append(dt)
+        return out, iters
+
+    per_solve, iters = timed(True, solves, warmup)
+    relres = oracle.true_relres(A, b, x)
+    per_solve_1t, iters_1t = timed(False, solves_1thread, 0) if solves_1thread > 0 else ([], None)
+    return {"value": float(np.median(per_solve)), "per_solve_s": per_solve, "iters": iters, "cores": cores,
+            "relres": relres, "value_1thread": float(np.median(per_solve_1t)) if per_solve_1t else None,
+            "per_solve_1thread_s": per_solve_1t, "iters_1thread": iters_1t}
+
+
+def _cpu_sample(r, n):
+    s = (f"whole solves to FP64 rel-res 1e-8 of the C restatement of MPI/src CG at {n}^3 ({r['iters']} iterations, "
+         f"true rel-res {r['relres']:.2e}): median of {len(r['per_solve_s'])} on {r['cores']} OpenMP threads")
+    if r["per_solve_1thread_s"]:
+        s += f"; value_1thread: median of {len(r['per_solve_1thread_s'])} on the sequential build"
+    return s + "; work arrays allocated once outside the timed region"
 
 
 def run_reference(args):
     ws, rank, _ = _dist()
+    if ws > 1:  # every rank joins (gloo: no GPU work in this arm); rank 0 alone times and prints
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+        ws = dist.get_world_size()
+        dist.barrier()
+        dist.destroy_process_group()
     if rank != 0:
         return 0
-    r = cpu_reference_time(args.n, args.ref_sample_iters, args.steps, args.warmup)
-    sample = (f"{args.ref_sample_iters} CG iterations of the C restatement of MPI/src (OpenMP, {r['cores']} threads) "
-              f"at {args.n}^3 per step, times {r['iters']} iterations (one full solve to rel-res 1e-8 during warm-up"
-              + (f": {r['full_solve_s']:.2f} s" if r["full_solve_s"] else "") + ")")
+    r = cpu_reference_time(args.n, args.steps, args.warmup, args.ref_1thread_solves)
     line = {
-        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.median(r["per_iter_s"])) * 1e3 * args.ref_sample_iters,
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": "s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["value"] * 1e3,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{args.n}^3 27-point HPCCG matrix, x* U[-1,1) seed 1234, b = A x*, x0 = 0, FP64 CG to ||r||/||b|| <= 1e-8",
                    "reference_build": "unavailable (Fortran 90; no Fortran compiler in this image) -> C restatement of MPI/src",
-                   "iterations": r["iters"]},
-        "cpu_baseline": {"value": r["value"], "unit": "s", "cores": r["cores"], "kind": "port", "sample": sample,
-                         "value_1thread": r["value_1thread"],
-                         "sample_1thread": "median of 3 one-iteration samples, sequential build, times the same "
-                                           "iteration count"},
+                   "iterations": r["iters"], "per_solve_s": r["per_solve_s"]},
+        "cpu_baseline": {"value": r["value"], "unit": "s", "cores": r["cores"], "kind": "port",
+                         "sample": _cpu_sample(r, args.n), "value_1thread": r["value_1thread"]},
         "e2e": {"value": r["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -498,13 +510,9 @@ def run_ours(args):
 
     cpu = None
     if not args.no_cpu_baseline and cubic:
-        it64 = results["fp64_cg"]["iterations"]
-        c = cpu_reference_time(n, args.ref_sample_iters, 3, 0, iters_needed=it64)
+        c = cpu_reference_time(n, 3, 1, args.ref_1thread_solves)
         cpu = {"value": c["value"], "unit": "s", "cores": c["cores"], "kind": "port",
-               "value_1thread": c["value_1thread"],
-               "sample": f"median of 3 samples of {args.ref_sample_iters} CG iterations of the C restatement of "
-                         f"MPI/src at {n}^3 (OpenMP, {c['cores']} threads) x {it64} iterations (the GPU FP64 count); "
-                         f"value_1thread: median of 3 one-iteration samples of the sequential build, same count"}
+               "value_1thread": c["value_1thread"], "iterations": c["iters"], "sample": _cpu_sample(c, n)}
     hr = results[head]
     line = {
         "metric": METRIC, "value": hr["ms"] / 1e3, "unit": "s", "n_gpus": ws, "steps": args.steps,
@@ -534,15 +542,31 @@ def run_ours(args):
     return 0
 
 
+def _relaunch(nproc: int, argv: list[str]) -> int:
+    """`--gpus N` without a launcher: start N ranks of this script under torch.distributed.run
+    (one process per GPU, rendezvous on 127.0.0.1) and return their exit status."""
+    import socket
+
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    # torch.distributed.run's own parser would read a bare "--n" as an abbreviation of its options
+    argv = ["--grid" if a == "--n" else ("--grid=" + a[4:] if a.startswith("--n=") else a) for a in argv]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={nproc}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *argv]
+    return subprocess.run(cmd).returncode
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--n", "--grid", dest="n", type=int, default=256)
     ap.add_argument("--nz", type=int, default=0, help="planes of an n x n x nz grid (default n; profiling cases)")
-    ap.add_argument("--ref-sample-iters", type=int, default=4)
+    ap.add_argument("--ref-1thread-solves", type=int, default=1,
+                    help="whole one-thread oracle solves for cpu_baseline.value_1thread (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip training/timing the learned preconditioner")
     ap.add_argument("--train-steps", type=int, default=400)
@@ -551,6 +575,12 @@ def main(argv=None):
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
+    ws_env = os.environ.get("WORLD_SIZE")
+    if ws_env is None and args.gpus > 1:
+        return _relaunch(args.gpus, sys.argv[1:] if argv is None else list(argv))
+    if int(ws_env or 1) != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but the launcher started WORLD_SIZE={ws_env} ranks", file=sys.stderr)
+        return 2
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

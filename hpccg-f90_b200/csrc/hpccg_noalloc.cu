@@ -14,8 +14,6 @@
 // n is limited to kMaxPartials * kChunk = 134,217,728 elements; larger n is
 // rejected with HPCCG_ERR_TOO_LARGE.  Every GPU that loads the library keeps
 // this 512 KiB array (plus a few words) for the life of the process.
-#include <mutex>
-
 #include "hpccg_internal.cuh"
 
 namespace {
@@ -30,7 +28,6 @@ constexpr int64_t kMaxN = kChunk * kMaxPartials;  // 134,217,728
 constexpr int kResult = kMaxPartials;
 constexpr int kCounter = kMaxPartials + 1;
 constexpr int kScratchWords = kMaxPartials + 32;
-constexpr int kMaxDevices = 64;
 
 }  // namespace
 
@@ -72,25 +69,18 @@ __global__ void __launch_bounds__(kNaBlock) k_ddot_noalloc(int64_t n, const doub
   }
 }
 
-std::mutex g_noalloc_mu;
-double *g_noalloc_ptr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device, looked up once
-// per device with that device current.  The name g_noalloc_scratch in host
-// code is only a host-side stand-in, not a device address.
+// Device address of the scratch array on the current device.  The name
+// g_noalloc_scratch in host code is only a host-side stand-in, not a device
+// address, so every call asks the runtime for the address on the device that
+// is current now.  The lookup is cheap next to the call's synchronisation, and
+// unlike an address cached per device index it stays right after the device's
+// context is re-created (cudaDeviceReset re-loads the library's module, and the
+// array may then sit elsewhere).
 int scratch_for_current_device(double **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return hpccg::set_cuda_error(e, "cudaGetDevice", __FILE__, __LINE__);
-  if (dev < 0 || dev >= kMaxDevices) return HPCCG_ERR_UNSUPPORTED;
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return hpccg::set_cuda_error(e, "cudaGetSymbolAddress", __FILE__, __LINE__);
-    g_noalloc_ptr[dev] = static_cast<double *>(p);
-  }
-  *out = g_noalloc_ptr[dev];
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return hpccg::set_cuda_error(e, "cudaGetSymbolAddress", __FILE__, __LINE__);
+  *out = static_cast<double *>(p);
   return HPCCG_OK;
 }
 

@@ -327,9 +327,10 @@ int hpccg_gpu_uniform_pm1(hpccg_ctx *ctx, uint64_t seed, int64_t offset, int64_t
  * until the process exits; so n is limited to 134,217,728 elements and larger
  * n returns HPCCG_ERR_TOO_LARGE.  The work runs on `stream` (a cudaStream_t;
  * NULL = the legacy default stream) on the current device, and the call
- * returns after *result (host memory) is written.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  All calls share
+ * returns after *result (host memory) is written.  Every call looks up the
+ * array's device address on the current device (cudaGetSymbolAddress); the
+ * first call on a device also loads the library's kernels there, so make that
+ * first call before any stream capture.  All calls share
  * the one array: calls that overlap on the GPU (from several host threads or
  * streams at once) race and must be serialised by the caller. */
 int hpccg_gpu_ddot_noalloc(int32_t n, const double *d_x, const double *d_y, double *result,

@@ -166,23 +166,80 @@ void orc_vcopy(int32_t n, const double *x, double *y)
         y[i] = x[i];
 }
 
+/* generate_matrix's operator applied without storing it
+ * (MPI/src/SparseMatrix.F90:138-159 fused with spmv, :213-232): row i sums, from
+ * 0.0, value*x(col) over the stencil in the sz -> sy -> sx order the CSR stores,
+ * with 27.0 on the diagonal and -1.0 elsewhere, skipping the neighbours the
+ * generator drops.  The operations are those of orc_spmv on the generated CSR,
+ * so y is bit-identical to it; only the 12 bytes per nonzero are not needed. */
+void orc_grid_spmv(int32_t nx, int32_t ny, int32_t nz, const double *x, double *y)
+{
+    const int64_t nxy = (int64_t)nx * ny;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int32_t iz = 0; iz < nz; ++iz) {
+        for (int32_t iy = 0; iy < ny; ++iy) {
+            for (int32_t ix = 0; ix < nx; ++ix) {
+                const int64_t row = iz * nxy + (int64_t)iy * nx + ix;
+                double rowsum = 0.0;
+                for (int32_t sz = -1; sz <= 1; ++sz) {
+                    if (iz + sz < 0 || iz + sz >= nz)
+                        continue;
+                    for (int32_t sy = -1; sy <= 1; ++sy) {
+                        if (iy + sy < 0 || iy + sy >= ny)
+                            continue;
+                        for (int32_t sx = -1; sx <= 1; ++sx) {
+                            if (ix + sx < 0 || ix + sx >= nx)
+                                continue;
+                            const int64_t col = row + sz * nxy + (int64_t)sy * nx + sx;
+                            const double v = (col == row) ? 27.0 : -1.0;
+                            rowsum = rowsum + v * x[col];
+                        }
+                    }
+                }
+                y[row] = rowsum;
+            }
+        }
+    }
+}
+
+/* The operator orc_cg applies: a stored CSR or the generator's grid. */
+typedef struct {
+    int32_t nrow;
+    const int32_t *rowindex, *colindex;
+    const double *values;
+    int32_t nx, ny, nz; /* grid operator when rowindex == NULL */
+} orc_op;
+
+static void op_apply(const orc_op *op, const double *x, double *y)
+{
+    if (op->rowindex)
+        orc_spmv(op->nrow, op->rowindex, op->colindex, op->values, x, y);
+    else
+        orc_grid_spmv(op->nx, op->ny, op->nz, x, y);
+}
+
 /* MPI/src/numerics.F90:41-162 cg, single rank (exchange_externals is a no-op,
  * SparseMatrix.F90:643-645).  Operation order as in the reference:
  * prepare (:91-104), then per k (:108-147): stop test on the normr of the
  * previous iteration, k==1 vcopy else ddot1/beta/wxbw, normr = sqrt(rtrans),
  * spmv, ddot, alpha, r update before x update. */
-int orc_cg(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
-           const double *values, const double *b, double *x, int32_t max_iter,
-           double tolerance, int32_t *niters, double *normr_out, double *hist)
+static int cg_core(const orc_op *op, const double *b, double *x, int32_t max_iter,
+                   double tolerance, int32_t *niters, double *normr_out, double *hist,
+                   double *work)
 {
-    double *r = (double *)malloc(sizeof(double) * (size_t)nrow);
-    double *p = (double *)malloc(sizeof(double) * (size_t)nrow);
-    double *Ap = (double *)malloc(sizeof(double) * (size_t)nrow);
+    const int32_t nrow = op->nrow;
+    /* r, p, Ap: the reference allocates them per call (numerics.F90:83-85);
+     * a caller that times repeated solves may pass them in (3*nrow doubles) */
+    double *r = work ? work : (double *)malloc(sizeof(double) * (size_t)nrow);
+    double *p = work ? work + nrow : (double *)malloc(sizeof(double) * (size_t)nrow);
+    double *Ap = work ? work + 2 * (size_t)nrow : (double *)malloc(sizeof(double) * (size_t)nrow);
     double normr = 0.0, rtrans = 0.0, oldrtrans = 0.0, alpha, beta;
     int32_t it = 0;
 
     orc_vcopy(nrow, x, p);
-    orc_spmv(nrow, rowindex, colindex, values, p, Ap);
+    op_apply(op, p, Ap);
     orc_waxpby(nrow, 1.0, b, -1.0, Ap, r);
     rtrans = orc_ddot1(nrow, r);
     normr = sqrt(rtrans);
@@ -203,7 +260,7 @@ int orc_cg(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
         normr = sqrt(rtrans);
         if (hist)
             hist[k] = normr;
-        orc_spmv(nrow, rowindex, colindex, values, p, Ap);
+        op_apply(op, p, Ap);
         alpha = orc_ddot(nrow, p, Ap);
         alpha = rtrans / alpha;
         orc_wwpby(nrow, -alpha, Ap, r);
@@ -212,10 +269,37 @@ int orc_cg(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
     }
     *niters = it;
     *normr_out = normr;
-    free(r);
-    free(p);
-    free(Ap);
+    if (!work) {
+        free(r);
+        free(p);
+        free(Ap);
+    }
     return 0;
+}
+
+int orc_cg(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
+           const double *values, const double *b, double *x, int32_t max_iter,
+           double tolerance, int32_t *niters, double *normr_out, double *hist)
+{
+    const orc_op op = {nrow, rowindex, colindex, values, 0, 0, 0};
+    return cg_core(&op, b, x, max_iter, tolerance, niters, normr_out, hist, NULL);
+}
+
+int orc_cg_work(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
+                const double *values, const double *b, double *x, int32_t max_iter,
+                double tolerance, int32_t *niters, double *normr_out, double *hist,
+                double *work)
+{
+    const orc_op op = {nrow, rowindex, colindex, values, 0, 0, 0};
+    return cg_core(&op, b, x, max_iter, tolerance, niters, normr_out, hist, work);
+}
+
+int orc_cg_grid(int32_t nx, int32_t ny, int32_t nz, const double *b, double *x,
+                int32_t max_iter, double tolerance, int32_t *niters, double *normr_out,
+                double *hist)
+{
+    const orc_op op = {nx * ny * nz, NULL, NULL, NULL, nx, ny, nz};
+    return cg_core(&op, b, x, max_iter, tolerance, niters, normr_out, hist, NULL);
 }
 
 /* MPI/src/numerics.F90:164-198 compute_residual (max-norm of v1-v2). */
@@ -235,6 +319,22 @@ double orc_true_relres(int32_t nrow, const int32_t *rowindex, const int32_t *col
 {
     double *Ax = (double *)malloc(sizeof(double) * (size_t)nrow);
     orc_spmv(nrow, rowindex, colindex, values, x, Ax);
+    double rr = 0.0, bb = 0.0;
+    for (int32_t i = 0; i < nrow; ++i) {
+        const double ri = b[i] - Ax[i];
+        rr = rr + ri * ri;
+        bb = bb + b[i] * b[i];
+    }
+    free(Ax);
+    return sqrt(rr) / sqrt(bb);
+}
+
+double orc_grid_true_relres(int32_t nx, int32_t ny, int32_t nz, const double *b,
+                            const double *x)
+{
+    const int32_t nrow = nx * ny * nz;
+    double *Ax = (double *)malloc(sizeof(double) * (size_t)nrow);
+    orc_grid_spmv(nx, ny, nz, x, Ax);
     double rr = 0.0, bb = 0.0;
     for (int32_t i = 0; i < nrow; ++i) {
         const double ri = b[i] - Ax[i];

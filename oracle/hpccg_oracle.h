@@ -59,6 +59,27 @@ int orc_cg(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
            const double *values, const double *b, double *x, int32_t max_iter,
            double tolerance, int32_t *niters, double *normr, double *hist);
 
+/* generate_matrix(nx,ny,nz)'s operator applied from the grid without storing
+ * the CSR (MPI/src/SparseMatrix.F90:138-159 with spmv, :213-232): the same
+ * terms in the same order, so y equals orc_spmv on the generated CSR bit for
+ * bit.  For checks at sizes where the host CSR (12 bytes per nonzero) is
+ * wasteful: 256^3 holds 5.4 GB of it. */
+void orc_grid_spmv(int32_t nx, int32_t ny, int32_t nz, const double *x, double *y);
+/* orc_cg with orc_grid_spmv as the operator (identical arithmetic). */
+int orc_cg_grid(int32_t nx, int32_t ny, int32_t nz, const double *b, double *x,
+                int32_t max_iter, double tolerance, int32_t *niters, double *normr,
+                double *hist);
+/* orc_true_relres with orc_grid_spmv as the operator. */
+double orc_grid_true_relres(int32_t nx, int32_t ny, int32_t nz, const double *b,
+                            const double *x);
+
+/* orc_cg with caller-owned work arrays (work: 3*nrow doubles for r, p, Ap),
+ * so that repeated timed solves neither allocate nor first-touch memory. */
+int orc_cg_work(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
+                const double *values, const double *b, double *x, int32_t max_iter,
+                double tolerance, int32_t *niters, double *normr, double *hist,
+                double *work);
+
 /* MPI/src/numerics.F90:164-198 compute_residual: max_i |v1(i)-v2(i)|. */
 double orc_compute_residual(int32_t n, const double *v1, const double *v2);
 

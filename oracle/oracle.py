@@ -52,6 +52,8 @@ def _lib(omp: bool = False) -> ctypes.CDLL:
     lib.orc_cg.argtypes = [ctypes.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p, ctypes.c_int32,
                            ctypes.c_double, ctypes.POINTER(ctypes.c_int32),
                            ctypes.POINTER(ctypes.c_double), _f64p]
+    lib.orc_cg_work.restype = ctypes.c_int
+    lib.orc_cg_work.argtypes = lib.orc_cg.argtypes + [_f64p]
     lib.orc_compute_residual.restype = ctypes.c_double
     lib.orc_compute_residual.argtypes = [ctypes.c_int32, _f64p, _f64p]
     lib.orc_true_relres.restype = ctypes.c_double
@@ -62,6 +64,14 @@ def _lib(omp: bool = False) -> ctypes.CDLL:
     lib.orc_uniform_pm1.argtypes = [ctypes.c_uint64, ctypes.c_int64, _f64p]
     lib.orc_set_dot_mode.restype = None
     lib.orc_set_dot_mode.argtypes = [ctypes.c_int]
+    lib.orc_grid_spmv.restype = None
+    lib.orc_grid_spmv.argtypes = [ctypes.c_int32] * 3 + [_f64p, _f64p]
+    lib.orc_cg_grid.restype = ctypes.c_int
+    lib.orc_cg_grid.argtypes = [ctypes.c_int32] * 3 + [_f64p, _f64p, ctypes.c_int32, ctypes.c_double,
+                                                       ctypes.POINTER(ctypes.c_int32),
+                                                       ctypes.POINTER(ctypes.c_double), _f64p]
+    lib.orc_grid_true_relres.restype = ctypes.c_double
+    lib.orc_grid_true_relres.argtypes = [ctypes.c_int32] * 3 + [_f64p, _f64p]
     lib.orc_batch_sizes.restype = None
     lib.orc_batch_sizes.argtypes = [ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p]
     _libs[name] = lib
@@ -139,6 +149,53 @@ def cg(A: Matrix, b, x0, max_iter: int, tolerance: float, omp: bool = False):
     _lib(omp).orc_cg(A.nrow, A.rowindex, A.colindex, A.values, np.ascontiguousarray(b, np.float64),
                      x, max_iter, tolerance, ctypes.byref(niters), ctypes.byref(normr), hist)
     return x, niters.value, normr.value, hist[: niters.value + 1].copy()
+
+
+def grid_spmv(nx: int, ny: int, nz: int, x, omp: bool = False):
+    """generate_matrix(nx,ny,nz)'s operator applied without a stored CSR; bit-identical to
+    spmv() on the generated CSR (same terms, same order)."""
+    y = np.empty(nx * ny * nz, np.float64)
+    _lib(omp).orc_grid_spmv(nx, ny, nz, np.ascontiguousarray(x, np.float64), y)
+    return y
+
+
+def cg_grid(nx: int, ny: int, nz: int, b, x0, max_iter: int, tolerance: float, omp: bool = False):
+    """cg() with the grid operator: same arithmetic, no host CSR.  Returns (x, niters, normr, hist)."""
+    x = np.ascontiguousarray(x0, np.float64).copy()
+    hist = np.zeros(max_iter + 1, np.float64)
+    niters = ctypes.c_int32(0)
+    normr = ctypes.c_double(0.0)
+    _lib(omp).orc_cg_grid(nx, ny, nz, np.ascontiguousarray(b, np.float64), x, max_iter, tolerance,
+                          ctypes.byref(niters), ctypes.byref(normr), hist)
+    return x, niters.value, normr.value, hist[: niters.value + 1].copy()
+
+
+def grid_true_relres(nx: int, ny: int, nz: int, b, x) -> float:
+    """||b - A x|| / ||b|| with the grid operator (sequential sums, as true_relres)."""
+    return _lib().orc_grid_true_relres(nx, ny, nz, np.ascontiguousarray(b, np.float64),
+                                       np.ascontiguousarray(x, np.float64))
+
+
+class CgWork:
+    """Work arrays (r, p, Ap) for repeated timed solves: allocated once and first-touched by
+    the same OpenMP static schedule the solve uses, so a timed solve neither allocates nor
+    faults pages in.  `solve` is cg() on them."""
+
+    def __init__(self, A: Matrix, omp: bool = False):
+        self.A, self.omp = A, omp
+        self.work = np.empty(3 * A.nrow, np.float64)
+        _lib(omp).orc_vcopy(3 * A.nrow, np.zeros(3 * A.nrow), self.work)
+        self.hist = np.zeros(100001, np.float64)
+
+    def solve(self, b, x, max_iter: int, tolerance: float):
+        """x (float64, contiguous) is updated in place.  Returns (niters, normr)."""
+        assert max_iter < len(self.hist)
+        niters = ctypes.c_int32(0)
+        normr = ctypes.c_double(0.0)
+        A = self.A
+        _lib(self.omp).orc_cg_work(A.nrow, A.rowindex, A.colindex, A.values, b, x, max_iter, tolerance,
+                                   ctypes.byref(niters), ctypes.byref(normr), self.hist, self.work)
+        return niters.value, normr.value
 
 
 class compensated_dots:

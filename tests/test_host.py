@@ -88,3 +88,20 @@ def test_host_generator_matches_oracle():
     assert np.array_equal(hp.uniform_pm1_host(1234, 1000), oracle.uniform_pm1(1234, 1000))
     assert np.array_equal(hp.uniform_pm1_host(9, 50, offset=0), oracle.uniform_pm1(9, 50))
     assert np.array_equal(hp.batch_sizes(7, 64, 16, 96).reshape(-1), np.asarray(oracle.batch_sizes(7, 64, 16, 96)).reshape(-1))
+
+
+def test_fortran_interfaces_bind_exported_symbols():
+    """The Fortran 90 host sources (not compiled: no Fortran compiler in this image) bind only
+    names the library exports and the header declares, and the drop-in `cg` keeps the
+    reference's argument list (MPI/src/numerics.F90:41-53)."""
+    drv = os.path.join(os.path.dirname(hp.LIB_PATH), "driver")
+    names = set()
+    for f in ("hpccg_gpu.F90", "numerics_gpu.F90", "main.F90"):
+        names |= set(re.findall(r'bind\(C,\s*name="(hpccg_\w+)"\)', open(os.path.join(drv, f)).read()))
+    assert {"hpccg_generate_matrix", "hpccg_gpu_create", "hpccg_gpu_cg", "hpccg_gpu_destroy"} <= names
+    assert names <= set(_declared_functions())
+    lib = ctypes.CDLL(hp.LIB_PATH)
+    for n in names:
+        assert hasattr(lib, n), n
+    src = open(os.path.join(drv, "numerics_gpu.F90")).read()
+    assert re.search(r"subroutine cg\(A, b, x, max_iter, tolerance, niters, normr\)", src)

@@ -126,3 +126,27 @@ def test_rng_counter_based():
     assert oracle.splitmix64_at(0, 0) == 0xE220A8397B1DCDAF  # splitmix64 from state 0: first output
     s = oracle.batch_sizes(7, 64, 16, 96)
     assert s.shape == (64, 3) and s.min() >= 16 and s.max() <= 96
+
+
+@pytest.mark.parametrize("nx,ny,nz", SIZES + [(33, 17, 5), (24, 24, 24)])
+def test_grid_operator_equals_csr_oracle(nx, ny, nz):
+    """The grid forms of spmv, cg and the true residual (used where a host CSR would be
+    gigabytes) repeat the CSR oracle's arithmetic bit for bit."""
+    A, x, b, xe = oracle.generate_matrix(nx, ny, nz)
+    v = oracle.uniform_pm1(99, A.nrow)
+    want = oracle.spmv(A, v)
+    assert np.array_equal(oracle.grid_spmv(nx, ny, nz, v), want)
+    assert np.array_equal(oracle.grid_spmv(nx, ny, nz, v, omp=True), want)
+    same = lambda u, w: np.array_equal(np.asarray(u), np.asarray(w), equal_nan=True)  # noqa: E731
+    r1 = oracle.cg(A, b, x, 40, 0.0)  # tiny grids converge exactly and then carry NaN, as the reference
+    r2 = oracle.cg_grid(nx, ny, nz, b, x, 40, 0.0)
+    r3 = oracle.cg_grid(nx, ny, nz, b, x, 40, 0.0, omp=True)
+    assert same(r1[0], r2[0]) and same(r1[3], r2[3]) and r1[1] == r2[1] and same(r1[2], r2[2])
+    with oracle.compensated_dots(omp=True), oracle.compensated_dots():
+        c1 = oracle.cg(A, b, x, 40, 0.0)
+        c3 = oracle.cg_grid(nx, ny, nz, b, x, 40, 0.0, omp=True)
+    assert same(c1[3], c3[3]) and same(c1[0], c3[0])
+    assert r3[1] == r1[1]
+    xs = oracle.uniform_pm1(5, A.nrow)
+    bs = oracle.spmv(A, xs)
+    assert oracle.grid_true_relres(nx, ny, nz, bs, v) == oracle.true_relres(A, bs, v)

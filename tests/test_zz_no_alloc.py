@@ -5,14 +5,17 @@ manager owns all device memory, or they may not allocate once set-up is over
 (cudaMalloc can synchronise the device and can fail on a fragmented heap).
 For them the library keeps the partial sums of this one dot product in a
 fixed array compiled into the library.  These tests call the entry point
-through the C-ABI and check it against the context-based hpccg_gpu_ddot,
-twice in a row, because successive calls share that array.  The file is
-named to run last; it also passes when run alone.
+through the C-ABI and check it against the context-based hpccg_gpu_ddot and
+the CPU oracle's ddot, twice in a row, because successive calls share that
+array, and check that calls leave the device's free memory unchanged.  The
+file is named to run last; it also passes when run alone.
 """
 import ctypes
 
 import numpy as np
 import pytest
+
+import oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -54,6 +57,25 @@ def test_noalloc_matches_ctx_ddot_twice(env, n):
         want = M.ddot(dx, dy)
         # both are reassociated sums of the same terms: the dot-product bound of the suite
         assert abs(got - want) <= 1e-15 * np.abs(x * y).sum(), (call, got, want)
+        ref = oracle.ddot(x, y)  # MPI/src/vector_operations.F90:40-71, sequential order
+        assert abs(got - ref) <= 1e-15 * np.abs(x * y).sum(), (call, got, ref)
+
+
+def test_noalloc_allocates_no_device_memory(env):
+    """After one warm-up call (which may load the library's kernels on the device), calls with
+    several sizes leave the device's free memory exactly as it was."""
+    torch, hp, fn, M = env
+    n_max = 3_000_001
+    x = torch.from_numpy(np.random.default_rng(5).uniform(-1, 1, n_max)).cuda()
+    y = torch.from_numpy(np.random.default_rng(6).uniform(-1, 1, n_max)).cuda()
+    assert _noalloc(torch, fn, x, y)[0] == hp.HPCCG_OK
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for n in (1, 777, 2048, 65537, 1 << 20, n_max):
+        assert _noalloc(torch, fn, x[:n], y[:n])[0] == hp.HPCCG_OK
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
 
 
 def test_noalloc_rejects_sizes_beyond_capacity(env):
