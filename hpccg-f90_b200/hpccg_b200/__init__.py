@@ -114,6 +114,26 @@ _SIGS = {
     "hpccg_gpu_mixed_fused": (_c.c_int, [_vp, _c.POINTER(_i32)]),
     "hpccg_gpu_mixed_pass": (_c.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _c.c_double, _c.c_double, _i32,
                                         _c.POINTER(_c.c_double)]),
+    "hpccg_generate_matrix_rank": (_c.c_int, [_i32, _i32, _i32, _i32, _i32, _i32p, _i32p, _f64p, _f64p, _f64p,
+                                              _f64p, _c.POINTER(_i64)]),
+    "hpccg_slab_plan_create": (_c.c_int, [_i32, _i64, _i32p, _i32p, _i32, _i32, _i32p, _i32, _c.POINTER(_vp)]),
+    "hpccg_slab_plan_destroy": (None, [_vp]),
+    "hpccg_slab_plan_info": (_c.c_int, [_vp, _c.POINTER(_i32), _c.POINTER(_i32), _c.POINTER(_i32),
+                                        _c.POINTER(_i32)]),
+    "hpccg_slab_plan_neighbors": (_c.c_int, [_vp, _vp, _vp]),
+    "hpccg_slab_plan_externals": (_c.c_int, [_vp, _vp, _vp]),
+    "hpccg_slab_plan_set_sends": (_c.c_int, [_vp, _vp, _vp]),
+    "hpccg_slab_plan_sends": (_c.c_int, [_vp, _vp, _vp]),
+    "hpccg_slab_plan_colindex": (_c.c_int, [_vp, _vp]),
+    "hpccg_slab_plan_blocks": (_c.c_int, [_vp, _vp, _vp]),
+    "hpccg_slab_create": (_c.c_int, [_vp, _f64p, _c.POINTER(_vp)]),
+    "hpccg_slab_destroy": (None, [_vp]),
+    "hpccg_slab_info": (_c.c_int, [_vp, _c.POINTER(_i32), _c.POINTER(_i32), _c.POINTER(_i32), _c.POINTER(_i32)]),
+    "hpccg_slab_spmv": (_c.c_int, [_vp, _vp, _vp]),
+    "hpccg_slab_pack": (_c.c_int, [_vp, _vp, _vp]),
+    "hpccg_slab_scatter_block": (_c.c_int, [_vp, _i32, _vp, _vp]),
+    "hpccg_slab_cg_step": (_c.c_int, [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hpccg_slab_group_cg": (_c.c_int, [_vp, _i32, _vp, _vp, _i32, _f64, _c.POINTER(_i32), _c.POINTER(_f64), _vp]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _fn = getattr(_lib, _name)

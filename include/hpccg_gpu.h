@@ -314,6 +314,108 @@ int hpccg_gpu_vcopy(hpccg_ctx *ctx, int32_t n, const double *d_x, double *d_y); 
  * host and device. */
 int hpccg_gpu_uniform_pm1(hpccg_ctx *ctx, uint64_t seed, int64_t offset, int64_t n, double *d_out);
 
+/* ---- several ranks: z slabs of the weak-scaled problem -------------------
+ *
+ * With nranks ranks the reference gives rank r the rows
+ * local_nrow*r+1 .. local_nrow*(r+1) of the nx x ny x (nz*nranks) grid
+ * (MPI/src/SparseMatrix.F90:68-185, start_row at :112), renumbers each rank's
+ * columns into its own rows followed by externals owned by other ranks
+ * (make_local_matrix, :235-627), fills p's externals before every SpMV
+ * (exchange_externals, :630-680) and sums each dot product over the ranks
+ * (MPI/src/vector_operations.F90:64-65, 96-97).  Two halo forms:
+ * HPCCG_HALO_MPI, externals grouped by owner and a send list per neighbour
+ * (the MPI variant); HPCCG_HALO_GET, externals in order of first appearance,
+ * each run of one owner filled from one contiguous range of the owner's
+ * vector (CAF-V2/src/SparseMatrix.F90:205-370).  Block lengths are the block
+ * sizes; the MPI variant's counting loop (:533-545) gives one more for every
+ * block but a rank's last, so with three or more ranks its middle ranks
+ * would read shifted halos. */
+#define HPCCG_HALO_MPI 0
+#define HPCCG_HALO_GET 1
+
+/* generate_matrix on rank `rank` of `nranks` (global 1-based columns, z
+ * truncated only at the global ends); hpccg_generate_matrix is rank 0 of 1. */
+int hpccg_generate_matrix_rank(int32_t nx, int32_t ny, int32_t nz, int32_t rank, int32_t nranks,
+                               int32_t *rowindex, int32_t *colindex, double *values, double *x, double *b,
+                               double *xexact, int64_t *nnz);
+
+/* The halo plan of one rank (host memory only; no GPU needed).  rowindex /
+ * colindex: the rank's rows in the reference layout with GLOBAL 1-based
+ * columns; first_rows[q] = first global row of rank q (1-based), q = 0..nranks,
+ * first_rows[nranks] = total rows + 1 (the reference's global_index_offsets,
+ * :318-324).  HPCCG_HALO_MPI plans need the neighbours' requests
+ * (hpccg_slab_plan_set_sends) before hpccg_slab_create; HPCCG_HALO_GET plans
+ * are complete at once. */
+typedef struct hpccg_slab_plan hpccg_slab_plan;
+int hpccg_slab_plan_create(int32_t nrow, int64_t nnz, const int32_t *rowindex, const int32_t *colindex,
+                           int32_t nranks, int32_t rank, const int32_t *first_rows, int32_t halo_mode,
+                           hpccg_slab_plan **plan);
+void hpccg_slab_plan_destroy(hpccg_slab_plan *plan);
+/* total_to_send is -1 until the sends are set (HPCCG_HALO_MPI). */
+int hpccg_slab_plan_info(const hpccg_slab_plan *plan, int32_t *num_external, int32_t *num_neighbors,
+                         int32_t *num_blocks, int32_t *total_to_send);
+/* HPCCG_HALO_MPI: neighbours in receive order and the externals each sends. */
+int hpccg_slab_plan_neighbors(const hpccg_slab_plan *plan, int32_t *neighbors, int32_t *recv_length);
+/* Global id and owning rank of each local external, in local order (for
+ * HPCCG_HALO_MPI the ids to send to each neighbour, block by block:
+ * make_local_matrix's new_external, :512-514). */
+int hpccg_slab_plan_externals(const hpccg_slab_plan *plan, int32_t *global_ids, int32_t *owners);
+/* HPCCG_HALO_MPI: what each neighbour (in this rank's neighbour order) asked
+ * for, as global ids, concatenated; stored as elements_to_send (local,
+ * :605-607).  Ids outside this rank's rows are rejected. */
+int hpccg_slab_plan_set_sends(hpccg_slab_plan *plan, const int32_t *send_length, const int32_t *global_ids);
+int hpccg_slab_plan_sends(const hpccg_slab_plan *plan, int32_t *send_length, int32_t *elements_to_send);
+/* The rank's columns renumbered: 1..nrow own rows, nrow+1.. externals. */
+int hpccg_slab_plan_colindex(const hpccg_slab_plan *plan, int32_t *colindex_local);
+/* HPCCG_HALO_GET: 4 per block (owner rank, first external (1-based), inmin,
+ * inmax in the owner's local rows) and each external's owner-local row. */
+int hpccg_slab_plan_blocks(const hpccg_slab_plan *plan, int32_t *blocks, int32_t *remote_index);
+
+/* The rank's device part on the current GPU: the local matrix (values in the
+ * CSR order of the plan's rowindex) as a column-major ELL over
+ * [own rows | externals], the send list or the block lists.  Vectors that
+ * SpMV reads (p) hold ncol = nrow + externals entries. */
+typedef struct hpccg_slab hpccg_slab;
+int hpccg_slab_create(const hpccg_slab_plan *plan, const double *values, hpccg_slab **slab);
+void hpccg_slab_destroy(hpccg_slab *slab);
+int hpccg_slab_info(const hpccg_slab *slab, int32_t *nrow, int32_t *ncol, int32_t *total_to_send,
+                    int32_t *num_blocks);
+/* y = A x (x: ncol entries), the reference's term order. */
+int hpccg_slab_spmv(hpccg_slab *slab, const double *d_x, double *d_y);
+/* HPCCG_HALO_MPI exchange: d_sendbuf[i] = x(elements_to_send(i)), neighbour
+ * after neighbour (:664-666); the receiver puts neighbour i's part at
+ * x + nrow + (recv_length of the neighbours before i). */
+int hpccg_slab_pack(hpccg_slab *slab, const double *d_x, double *d_sendbuf);
+/* HPCCG_HALO_GET exchange: d_range holds the owner's rows inmin..inmax of
+ * `block`; scatters them into the block's externals of x (:360-367). */
+int hpccg_slab_scatter_block(hpccg_slab *slab, int32_t block, const double *d_range, double *d_x);
+
+/* One rank's CG (MPI/src/numerics.F90:41-162) as steps between which the
+ * caller moves data: after START and BEGIN it fills p's externals, after
+ * PREPARE, SPMV and UPDATE it sets d_state[1] to the sum over ranks of every
+ * rank's d_state[0] (in rank order).  d_state: 8 doubles on the device,
+ * [0] local dot, [1] its sum over ranks, [2] rtrans, [3] normr, [4] alpha,
+ * [5] beta, [6] done (set by BEGIN once normr < tolerance; later steps do
+ * nothing), [7] tolerance (set by the caller).  Vectors: b, x, r, Ap nrow
+ * entries, p ncol.  d_hist (nullable): [0] and [k] as in hpccg_gpu_cg.
+ * Sequence: START; exchange p; PREPARE; sum; PREPARED; then for k = 1, 2, ..:
+ * BEGIN(k); exchange p; SPMV; sum; UPDATE; sum -- until done. */
+#define HPCCG_SLAB_START 0    /* p = x */
+#define HPCCG_SLAB_PREPARE 1  /* Ap = A p, r = b - Ap, [0] = local r.r */
+#define HPCCG_SLAB_PREPARED 2 /* rtrans = [1], normr = sqrt(rtrans) */
+#define HPCCG_SLAB_BEGIN 3    /* stop test; p = r (k = 1) or beta = [1]/rtrans, p = r + beta p */
+#define HPCCG_SLAB_SPMV 4     /* Ap = A p, [0] = local p.Ap */
+#define HPCCG_SLAB_UPDATE 5   /* alpha = rtrans/[1]; r -= alpha Ap; x += alpha p; [0] = local r.r */
+int hpccg_slab_cg_step(hpccg_slab *slab, int32_t step, int32_t k, const double *d_b, double *d_x, double *d_p,
+                       double *d_r, double *d_Ap, double *d_state, double *d_hist);
+
+/* All nslabs ranks in this process (slabs[q] is rank q, each on its own GPU
+ * or several on one): the whole CG with the exchange done by device copies
+ * and the sums folded in rank order.  d_b[q], d_x[q]: rank q's vectors on its
+ * GPU.  niters, normr and resid_hist as in hpccg_gpu_cg. */
+int hpccg_slab_group_cg(hpccg_slab *const *slabs, int32_t nslabs, const double *const *d_b, double *const *d_x,
+                        int32_t max_iter, double tolerance, int32_t *niters, double *normr, double *resid_hist);
+
 /* ---- allocation-free entry point ---------------------------------------- */
 
 /* Dot product x.y of two device arrays that allocates no device memory.  This

@@ -16,17 +16,20 @@
 #include <stdlib.h>
 #include <string.h>
 
-/* MPI/src/SparseMatrix.F90:68-185.  One rank: start_row = 1, total_nrow =
- * local_nrow, so the z truncation test curcol in [1,total_nrow] clips at the
- * first and last z-plane.  Loop nest iz -> iy -> ix (x fastest), stencil
- * sz -> sy -> sx, so columns ascend inside each row. */
-int64_t orc_generate_matrix(int32_t nx, int32_t ny, int32_t nz, int32_t *rowindex,
-                            int32_t *colindex, double *values, double *x, double *b,
-                            double *xexact)
+/* MPI/src/SparseMatrix.F90:68-185 on rank `rank` of `nranks` (weak scaling in
+ * z): local_nrow = nx*ny*nz (:108), total_nrow = local_nrow*nranks (:110),
+ * start_row = local_nrow*rank + 1 (:112); columns are global and 1-based, and
+ * the z truncation test curcol in [1,total_nrow] (:153) clips only at the
+ * first plane of rank 0 and the last plane of the last rank.  Loop nest
+ * iz -> iy -> ix (x fastest), stencil sz -> sy -> sx, so columns ascend
+ * inside each row. */
+int64_t orc_generate_matrix_rank(int32_t nx, int32_t ny, int32_t nz, int32_t rank, int32_t nranks,
+                                 int32_t *rowindex, int32_t *colindex, double *values, double *x,
+                                 double *b, double *xexact)
 {
     const int32_t local_nrow = nx * ny * nz;
-    const int32_t total_nrow = local_nrow;
-    const int32_t start_row = 1;
+    const int32_t total_nrow = local_nrow * nranks;
+    const int32_t start_row = local_nrow * rank + 1;
     int32_t cursor = 1, rowcursor = 1;
     for (int32_t iz = 1; iz <= nz; ++iz) {
         for (int32_t iy = 1; iy <= ny; ++iy) {
@@ -58,6 +61,14 @@ int64_t orc_generate_matrix(int32_t nx, int32_t ny, int32_t nz, int32_t *rowinde
     }
     rowindex[rowcursor - 1] = cursor;
     return (int64_t)cursor - 1;
+}
+
+/* One rank: start_row = 1, total_nrow = local_nrow. */
+int64_t orc_generate_matrix(int32_t nx, int32_t ny, int32_t nz, int32_t *rowindex,
+                            int32_t *colindex, double *values, double *x, double *b,
+                            double *xexact)
+{
+    return orc_generate_matrix_rank(nx, ny, nz, 0, 1, rowindex, colindex, values, x, b, xexact);
 }
 
 /* MPI/src/SparseMatrix.F90:213-232: row sum from 0.0 in increasing k. */

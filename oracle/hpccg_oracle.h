@@ -87,6 +87,44 @@ double orc_compute_residual(int32_t n, const double *v1, const double *v2);
 double orc_true_relres(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
                        const double *values, const double *b, const double *x);
 
+/* MPI/src/SparseMatrix.F90:68-185 on rank `rank` of `nranks`: the rows
+ * local_nrow*rank+1 .. local_nrow*(rank+1) of the weak-scaled problem (the
+ * nx x ny x (nz*nranks) grid cut into z slabs), with global 1-based columns.
+ * orc_generate_matrix is rank 0 of 1. */
+int64_t orc_generate_matrix_rank(int32_t nx, int32_t ny, int32_t nz, int32_t rank, int32_t nranks,
+                                 int32_t *rowindex, int32_t *colindex, double *values, double *x,
+                                 double *b, double *xexact);
+
+/* The multi-rank halo set-up of every rank of an nranks communicator,
+ * simulated in one process (hpccg_oracle_slab.c): mode 0 follows the MPI
+ * variant's make_local_matrix (MPI/src/SparseMatrix.F90:235-627), mode 1 the
+ * CAF-V2 variant's (CAF-V2/src/SparseMatrix.F90:205-331). */
+typedef struct orc_slab_plan orc_slab_plan;
+orc_slab_plan *orc_slab_plan_create(int32_t nx, int32_t ny, int32_t nz, int32_t nranks, int32_t mode);
+void orc_slab_plan_destroy(orc_slab_plan *plan);
+/* Copies one of a rank's lists into out (nullable) and returns its length.
+ * Indices keep the reference's 1-based convention; ranks are 0-based. */
+enum {
+    ORC_SLAB_NNZ = 0,               /* (count only) stored nonzeros */
+    ORC_SLAB_COLINDEX = 1,          /* local column indices after renumbering */
+    ORC_SLAB_ROWINDEX = 2,
+    ORC_SLAB_EXTERNALS = 3,         /* global id of each local external, in local order */
+    ORC_SLAB_EXTERNAL_OWNERS = 4,   /* owning rank of each local external */
+    ORC_SLAB_NEIGHBORS = 5,         /* mode 0: neighbours in receive order */
+    ORC_SLAB_RECV_LENGTH = 6,       /* mode 0: block sizes */
+    ORC_SLAB_RECV_LENGTH_LITERAL = 7, /* mode 0: the reference loop's count */
+    ORC_SLAB_SEND_LENGTH = 8,       /* mode 0 */
+    ORC_SLAB_ELEMENTS_TO_SEND = 9,  /* mode 0: local indices, neighbour by neighbour */
+    ORC_SLAB_BLOCKS = 10,           /* mode 1: 4 per block: owner, start, inmin, inmax */
+    ORC_SLAB_REMOTE_INDEX = 11      /* mode 1: owner-local index of each external */
+};
+int32_t orc_slab_plan_get(const orc_slab_plan *plan, int32_t rank, int32_t what, int32_t *out);
+/* MPI/src/numerics.F90:41-162 on all ranks in step (exchange before each
+ * spmv, dot products summed over ranks in rank order).  b, x: the ranks'
+ * vectors one after another. */
+int orc_cg_slabs(const orc_slab_plan *plan, const double *b, double *x, int32_t max_iter,
+                 double tolerance, int32_t *niters, double *normr, double *hist);
+
 /* The project's counter-based generator (no reference counterpart): value i of
  * stream `seed` is splitmix64's finaliser applied to seed + (i+1)*golden;
  * uniform in [-1,1) is 2*((z>>11)*2^-53) - 1. */

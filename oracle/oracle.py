@@ -72,6 +72,17 @@ def _lib(omp: bool = False) -> ctypes.CDLL:
                                                        ctypes.POINTER(ctypes.c_double), _f64p]
     lib.orc_grid_true_relres.restype = ctypes.c_double
     lib.orc_grid_true_relres.argtypes = [ctypes.c_int32] * 3 + [_f64p, _f64p]
+    lib.orc_generate_matrix_rank.restype = ctypes.c_int64
+    lib.orc_generate_matrix_rank.argtypes = [ctypes.c_int32] * 5 + [_i32p, _i32p, _f64p, _f64p, _f64p, _f64p]
+    lib.orc_slab_plan_create.restype = ctypes.c_void_p
+    lib.orc_slab_plan_create.argtypes = [ctypes.c_int32] * 5
+    lib.orc_slab_plan_destroy.restype = None
+    lib.orc_slab_plan_destroy.argtypes = [ctypes.c_void_p]
+    lib.orc_slab_plan_get.restype = ctypes.c_int32
+    lib.orc_slab_plan_get.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
+    lib.orc_cg_slabs.restype = ctypes.c_int
+    lib.orc_cg_slabs.argtypes = [ctypes.c_void_p, _f64p, _f64p, ctypes.c_int32, ctypes.c_double,
+                                 ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double), _f64p]
     lib.orc_batch_sizes.restype = None
     lib.orc_batch_sizes.argtypes = [ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p]
     _libs[name] = lib
@@ -174,6 +185,62 @@ def grid_true_relres(nx: int, ny: int, nz: int, b, x) -> float:
     """||b - A x|| / ||b|| with the grid operator (sequential sums, as true_relres)."""
     return _lib().orc_grid_true_relres(nx, ny, nz, np.ascontiguousarray(b, np.float64),
                                        np.ascontiguousarray(x, np.float64))
+
+
+def generate_matrix_rank(nx: int, ny: int, nz: int, rank: int, nranks: int):
+    """MPI/src/SparseMatrix.F90:68-185 on rank `rank` of `nranks` (z slabs of the
+    nx x ny x nz*nranks grid; global 1-based columns).  Returns (A, x, b, xexact)."""
+    n = nx * ny * nz
+    rowindex = np.zeros(n + 1, np.int32)
+    colindex = np.zeros(27 * n, np.int32)
+    values = np.zeros(27 * n, np.float64)
+    x, b, xexact = np.empty(n), np.empty(n), np.empty(n)
+    nnz = _lib().orc_generate_matrix_rank(nx, ny, nz, rank, nranks, rowindex, colindex, values, x, b, xexact)
+    A = Matrix(nx, ny, nz, rowindex, colindex[:nnz].copy(), values[:nnz].copy(), int(nnz))
+    return A, x, b, xexact
+
+
+HALO_MPI, HALO_GET = 0, 1
+
+
+class SlabPlan:
+    """Every rank's halo set-up for nranks z slabs of nx x ny x nz, simulated in one process:
+    mode HALO_MPI follows MPI/src/SparseMatrix.F90:235-627 (make_local_matrix), HALO_GET
+    CAF-V2/src/SparseMatrix.F90:205-331.  Indices keep the reference's 1-based convention;
+    ranks are 0-based."""
+
+    FIELDS = {"nnz": 0, "colindex": 1, "rowindex": 2, "externals": 3, "external_owners": 4, "neighbors": 5,
+              "recv_length": 6, "recv_length_literal": 7, "send_length": 8, "elements_to_send": 9,
+              "blocks": 10, "remote_index": 11}
+
+    def __init__(self, nx: int, ny: int, nz: int, nranks: int, mode: int = HALO_MPI):
+        self.nx, self.ny, self.nz, self.nranks, self.mode = nx, ny, nz, nranks, mode
+        self.local_nrow = nx * ny * nz
+        self._h = _lib().orc_slab_plan_create(nx, ny, nz, nranks, mode)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib().orc_slab_plan_destroy(self._h)
+            self._h = None
+
+    def get(self, rank: int, what: str):
+        code = self.FIELDS[what]
+        n = _lib().orc_slab_plan_get(self._h, rank, code, None)
+        if what == "nnz":
+            return int(n)
+        out = np.zeros(max(1, 4 * n if what == "blocks" else n), np.int32)
+        _lib().orc_slab_plan_get(self._h, rank, code, out.ctypes.data)
+        return out[:4 * n].reshape(n, 4) if what == "blocks" else out[:n]
+
+    def cg(self, b, x0, max_iter: int, tolerance: float):
+        """MPI/src/numerics.F90:41-162 on all ranks in step.  b, x0: the ranks' vectors one after
+        another.  Returns (x, niters, normr, hist[0..niters])."""
+        x = np.ascontiguousarray(x0, np.float64).copy()
+        hist = np.zeros(max_iter + 1, np.float64)
+        niters, normr = ctypes.c_int32(0), ctypes.c_double(0.0)
+        _lib().orc_cg_slabs(self._h, np.ascontiguousarray(b, np.float64), x, max_iter, tolerance,
+                            ctypes.byref(niters), ctypes.byref(normr), hist)
+        return x, niters.value, normr.value, hist[: niters.value + 1].copy()
 
 
 class CgWork:

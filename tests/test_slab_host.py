@@ -1,0 +1,191 @@
+"""Several ranks over z slabs: the host half, on the CPU.
+
+- The rank generator (MPI/src/SparseMatrix.F90:68-185 with start_row, :112)
+  matches the oracle's, and the ranks' rows stacked are the single-rank
+  matrix of the nx x ny x (nz*P) grid.
+- Every rank's halo plan (make_local_matrix, MPI/src/SparseMatrix.F90:235-627;
+  CAF-V2/src/SparseMatrix.F90:205-331) matches the oracle's restatement list
+  by list: renumbered columns, externals and owners, neighbours, block
+  lengths, send lists; blocks and owner-local rows in the GET form.  Built in
+  one process, and on gloo ranks (world sizes 2 and 3) whose plans exchange
+  their requests through torch.distributed as the reference's ranks do
+  through MPI.
+- The oracle's multi-rank CG against its single-rank CG on the stacked grid.
+- The reference's block-length count (:533-545), restated literally, is one
+  too large for every block but the last: right for two ranks, off by one for
+  the middle ranks of three -- the reason the plans use the block sizes.
+
+Integer and index results are compared exactly.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+import hpccg_b200 as hp
+import oracle
+from hpccg_b200 import zslab
+
+CASES = [(4, 3, 2, 2), (4, 3, 2, 3), (5, 4, 3, 4), (3, 3, 1, 3), (1, 1, 4, 2), (6, 2, 1, 2), (2, 5, 3, 1)]
+
+
+def _plans(nx, ny, nz, P, mode):
+    plans = []
+    for r in range(P):
+        rows, cols, vals, *_ = zslab.generate_matrix_rank(nx, ny, nz, r, P)
+        plans.append(zslab.SlabPlan(rows, cols, P, r, zslab.first_rows_equal(nx * ny * nz, P), mode))
+    zslab.exchange_plans_local(plans)
+    return plans
+
+
+def _compare(plan, ref, r, mode):
+    np.testing.assert_array_equal(plan.colindex_local(), ref.get(r, "colindex"))
+    ids, owners = plan.externals()
+    np.testing.assert_array_equal(ids, ref.get(r, "externals"))
+    np.testing.assert_array_equal(owners, ref.get(r, "external_owners"))
+    if mode == zslab.HALO_MPI:
+        nb, rl = plan.neighbors()
+        np.testing.assert_array_equal(nb, ref.get(r, "neighbors"))
+        np.testing.assert_array_equal(rl, ref.get(r, "recv_length"))
+        sl, ets = plan.sends()
+        np.testing.assert_array_equal(sl, ref.get(r, "send_length"))
+        np.testing.assert_array_equal(ets, ref.get(r, "elements_to_send"))
+    else:
+        blk, rem = plan.blocks()
+        np.testing.assert_array_equal(blk, ref.get(r, "blocks"))
+        np.testing.assert_array_equal(rem, ref.get(r, "remote_index"))
+
+
+@pytest.mark.parametrize("nx,ny,nz,P", CASES)
+def test_rank_generator_matches_oracle_and_stacks(nx, ny, nz, P):
+    G, _, bg, _ = oracle.generate_matrix(nx, ny, nz * P)
+    cols, vals, bs, rows_off = [], [], [], 0
+    for r in range(P):
+        rows, c, v, x, b, xe = zslab.generate_matrix_rank(nx, ny, nz, r, P)
+        A, ox, ob, oxe = oracle.generate_matrix_rank(nx, ny, nz, r, P)
+        np.testing.assert_array_equal(rows, A.rowindex)
+        np.testing.assert_array_equal(c, A.colindex)
+        np.testing.assert_array_equal(v, A.values)
+        np.testing.assert_array_equal(b, ob)
+        assert np.all(x == 0) and np.all(xe == 1)
+        cols.append(c), vals.append(v), bs.append(b)
+    np.testing.assert_array_equal(np.concatenate(cols), G.colindex)
+    np.testing.assert_array_equal(np.concatenate(vals), G.values)
+    np.testing.assert_array_equal(np.concatenate(bs), bg)
+
+
+@pytest.mark.parametrize("mode", [zslab.HALO_MPI, zslab.HALO_GET])
+@pytest.mark.parametrize("nx,ny,nz,P", CASES)
+def test_plans_match_oracle(nx, ny, nz, P, mode):
+    ref = oracle.SlabPlan(nx, ny, nz, P, mode)
+    for r, plan in enumerate(_plans(nx, ny, nz, P, mode)):
+        _compare(plan, ref, r, mode)
+
+
+def test_reference_block_length_count():
+    """The literal count of MPI/src/SparseMatrix.F90:533-545 against the block sizes."""
+    two = oracle.SlabPlan(4, 3, 2, 2, oracle.HALO_MPI)
+    for r in range(2):
+        np.testing.assert_array_equal(two.get(r, "recv_length_literal"), two.get(r, "recv_length"))
+    three = oracle.SlabPlan(4, 3, 2, 3, oracle.HALO_MPI)
+    np.testing.assert_array_equal(three.get(1, "recv_length"), [12, 12])
+    np.testing.assert_array_equal(three.get(1, "recv_length_literal"), [13, 12])  # first block one too long
+    for r in (0, 2):
+        np.testing.assert_array_equal(three.get(r, "recv_length_literal"), three.get(r, "recv_length"))
+
+
+def test_plan_rejects_bad_input():
+    rows, cols, vals, *_ = zslab.generate_matrix_rank(3, 3, 2, 0, 2)
+    fr = zslab.first_rows_equal(18, 2)
+    bad = cols.copy()
+    bad[0] = 37  # beyond the 36 rows of two slabs
+    with pytest.raises(hp.HpccgError):
+        zslab.SlabPlan(rows, bad, 2, 0, fr)
+    plan = zslab.SlabPlan(rows, cols, 2, 0, fr)
+    with pytest.raises(hp.HpccgError):
+        plan.set_sends({1: np.array([19], np.int32)})  # rank 0 owns rows 1..18 only
+
+
+@pytest.mark.parametrize("nx,ny,nz,P", [(4, 3, 2, 2), (4, 3, 2, 3), (3, 3, 1, 4), (5, 2, 3, 1)])
+def test_oracle_slab_cg_matches_single_rank(nx, ny, nz, P):
+    G, x0, b, _ = oracle.generate_matrix(nx, ny, nz * P)
+    _, it1, nr1, h1 = oracle.cg(G, b, x0, 30, 0.0)
+    runs = []
+    for mode in (oracle.HALO_MPI, oracle.HALO_GET):
+        x, it, nr, h = oracle.SlabPlan(nx, ny, nz, P, mode).cg(b, x0, 30, 0.0)
+        runs.append((x, h))
+        assert it == it1
+        r0 = h1[0]
+        for k in range(len(h1)):  # only the dot products' association differs
+            bound = 1e-12 * (h1[k] if h1[k] >= 1e-8 * r0 else r0)
+            assert abs(h[k] - h1[k]) <= bound or (np.isnan(h[k]) and np.isnan(h1[k])), (mode, k)
+        if P == 1:
+            np.testing.assert_array_equal(h, h1)
+    # the two halo forms fetch the same values: identical iterates
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    np.testing.assert_array_equal(runs[0][1], runs[1][1])
+
+
+# ---- gloo ranks ----------------------------------------------------------------
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, P, port, nx, ny, nz, mode, out_dir):
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=P,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        rows, cols, vals, *_ = zslab.generate_matrix_rank(nx, ny, nz, rank, P)
+        # global_index_offsets by an allreduce of each rank's first row (:318-324)
+        import torch
+
+        t = torch.zeros(P, dtype=torch.int64)
+        t[rank] = nx * ny * nz * rank + 1
+        dist.all_reduce(t)
+        fr = np.append(t.numpy(), nx * ny * nz * P + 1).astype(np.int32)
+        plan = zslab.SlabPlan(rows, cols, P, rank, fr, mode)
+        ranges = zslab.exchange_plans_dist(plan)
+        res = {"colindex": plan.colindex_local(), "externals": plan.externals()[0],
+               "owners": plan.externals()[1]}
+        if mode == zslab.HALO_MPI:
+            res["neighbors"], res["recv_length"] = plan.neighbors()
+            res["send_length"], res["elements_to_send"] = plan.sends()
+        else:
+            res["blocks"], res["remote_index"] = plan.blocks()
+            served = sorted((q, lo, hi) for q, rr in ranges.items() for lo, hi in rr)
+            res["served"] = np.array(served, np.int32).reshape(-1, 3)
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), **res)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("mode", [zslab.HALO_MPI, zslab.HALO_GET])
+@pytest.mark.parametrize("nx,ny,nz,P", [(4, 3, 2, 2), (3, 2, 2, 3), (3, 3, 1, 3)])
+def test_plans_over_gloo_ranks(tmp_path, nx, ny, nz, P, mode):
+    mp.start_processes(_rank_main, args=(P, _free_port(), nx, ny, nz, mode, str(tmp_path)), nprocs=P,
+                       join=True, start_method="spawn")
+    ref = oracle.SlabPlan(nx, ny, nz, P, mode)
+    for r in range(P):
+        got = np.load(tmp_path / f"rank{r}.npz")
+        np.testing.assert_array_equal(got["colindex"], ref.get(r, "colindex"))
+        np.testing.assert_array_equal(got["externals"], ref.get(r, "externals"))
+        np.testing.assert_array_equal(got["owners"], ref.get(r, "external_owners"))
+        if mode == zslab.HALO_MPI:
+            for k in ("neighbors", "recv_length", "send_length", "elements_to_send"):
+                np.testing.assert_array_equal(got[k], ref.get(r, k))
+        else:
+            np.testing.assert_array_equal(got["blocks"], ref.get(r, "blocks"))
+            np.testing.assert_array_equal(got["remote_index"], ref.get(r, "remote_index"))
+            # each rank serves exactly the ranges the other ranks' blocks name
+            want = sorted((q, int(lo), int(hi)) for q in range(P) for own, _s, lo, hi in ref.get(q, "blocks")
+                          if own == r)
+            np.testing.assert_array_equal(got["served"], np.array(want, np.int32).reshape(-1, 3))
