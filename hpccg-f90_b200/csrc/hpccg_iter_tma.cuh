@@ -21,15 +21,21 @@
 // alpha_k^2 Ap'.Ap', which the next pass needs before it can build p_{k+1}.
 // r and p are double-buffered (the halo of a tile is another tile's rows).
 //
-// A CTA owns a 32 x 64 tile of grid columns (4 x 2 per thread) and a chunk of
-// z planes.  Step s receives by TMA plane s of p (box 40 x 68 from
-// (x0-4, y0-2)), plane s-1 of r (box 40 x 66 from (x0-4, y0-1)) and plane s-1
-// of d (box 32 x 64) into a ring of kItStages slots; zeros arrive outside the
+// A CTA of 512 threads owns a 64 x 64 tile of grid columns (4 x 2 per thread)
+// and a chunk of z planes, one CTA per SM (128 registers a thread, 199 KB of
+// shared memory).  Step s receives by TMA plane s of p (box 72 x 68 from
+// (x0-4, y0-2)), plane s-1 of r (box 72 x 66 from (x0-4, y0-1)) and plane s-1
+// of d (box 64 x 64) into a ring of kItStages slots; zeros arrive outside the
 // grid.  Phase A of step s forms p'(s-1) on the tile and its one-wide ring (the
-// ring by 196 threads, one position each) into a shared p' plane, and stores
+// ring by 260 threads, one position each) into a shared p' plane, and stores
 // r', p' and d of the tile's own rows; phase B forms Ap'(s-3) from the shared
 // p' planes s-4 .. s-2 and accumulates the dots.  The loop is unrolled by two
 // so that values kept for one or two steps alternate between two register sets.
+// Against 32 x 64 tiles of 256 threads, two CTAs per SM, the 64 x 64 tile
+// recomputes fewer ring positions and halo lines per row (260 ring positions
+// per 4096 rows instead of 196 per 2048; p box 1.20 instead of 1.33 floats per
+// row) and passes half as many CTA barriers per row: 0.079 against 0.087 ms a
+// pass at 256^3, same iterates.
 //
 // Every stencil sum has one association, fixed by the position: a 3-point line
 // sum at even x is x[x-1] + (x[x] + x[x+1]) and at odd x (x[x-1] + x[x]) +
@@ -46,22 +52,24 @@
 
 namespace hpccg {
 
-constexpr int kItTileX = kTmaTileX, kItTileY = kTmaTileY;    // 32 x 64 columns per CTA
-constexpr int kItBoxX = kItTileX + 8;                         // x0-4 .. x0+35
+constexpr int kItTileX = 64, kItTileY = 64;                   // 64 x 64 columns per CTA
+constexpr int kItBlock = 512;                                 // threads per CTA
+constexpr int kItTX = kItTileX / 4;                           // threads along x
+constexpr int kItBoxX = kItTileX + 8;                         // x0-4 .. x0+67
 constexpr int kItPBoxY = kItTileY + 4;                        // p box: y0-2 .. y0+65
 constexpr int kItRBoxY = kItTileY + 2;                        // r box, p' plane: y0-1 .. y0+64
-constexpr uint32_t kItPBytes = kItBoxX * kItPBoxY * 4;        // 10880
-constexpr uint32_t kItRBytes = kItBoxX * kItRBoxY * 4;        // 10560
-constexpr uint32_t kItDBytes = kItTileX * kItTileY * 4;       // 8192
-constexpr int kItRSlot = ((kItRBytes + 127) / 128) * 128;     // 10624
-constexpr int kItStageBytes = kItPBytes + kItRSlot + kItDBytes;  // 29696
+constexpr uint32_t kItPBytes = kItBoxX * kItPBoxY * 4;        // 19584
+constexpr uint32_t kItRBytes = kItBoxX * kItRBoxY * 4;        // 19008
+constexpr uint32_t kItDBytes = kItTileX * kItTileY * 4;       // 16384
+constexpr int kItRSlot = ((kItRBytes + 127) / 128) * 128;     // 19072
+constexpr int kItStageBytes = kItPBytes + kItRSlot + kItDBytes;  // 55040
 constexpr int kItStages = 3;
 constexpr int kItNFloats = kItRSlot / 4;                      // one shared p' plane
-constexpr int kItHalo = 2 * kItRBoxY + 2 * kItTileX;          // ring positions of a p' plane (196)
+constexpr int kItHalo = 2 * kItRBoxY + 2 * kItTileX;          // ring positions of a p' plane (260)
 constexpr int kItSmemBytes = kItStages * kItStageBytes + 2 * kItRSlot;  // dynamic shared memory
 constexpr int kItMaxGrid = (kMaxPartials - 1) / 4;           // four partials per CTA
-static_assert(kItPBytes % 128 == 0 && kItDBytes % 128 == 0 && kItHalo <= kBlock, "layout");
-static_assert(kBlock == (kItTileX / 4) * (kItTileY / 2), "one thread per 4 x 2 columns");
+static_assert(kItPBytes % 128 == 0 && kItDBytes % 128 == 0 && kItHalo <= kItBlock, "layout");
+static_assert(kItBlock == (kItTileX / 4) * (kItTileY / 2), "one thread per 4 x 2 columns");
 
 struct IterScalars {
   float alpha, nalpha, beta;
@@ -261,7 +269,7 @@ __device__ __forceinline__ void iter_rows_tma(const TmaTile &t, const CUtensorMa
                                               const IterScalars &sc, double dots[4], int *status) {
   extern __shared__ __align__(128) unsigned char it_smem[];  // kItSmemBytes
   __shared__ uint64_t full[kItStages];
-  const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
+  const int tid = threadIdx.x, tx = tid % kItTX, ty = tid / kItTX;
   const int per_plane = t.tiles_x * t.tiles_y;
   const int q = blockIdx.x / per_plane, tile = blockIdx.x - q * per_plane;
   const int x0 = (tile % t.tiles_x) * kItTileX, y0 = (tile / t.tiles_x) * kItTileY;
@@ -286,7 +294,7 @@ __device__ __forceinline__ void iter_rows_tma(const TmaTile &t, const CUtensorMa
   if (tid < kItRBoxY) {
     hbx = 3, hby = tid;  // column x0-1
   } else if (tid < 2 * kItRBoxY) {
-    hbx = kItBoxX - 4, hby = tid - kItRBoxY;  // column x0+32
+    hbx = kItBoxX - 4, hby = tid - kItRBoxY;  // column x0+kItTileX
   } else if (tid < 2 * kItRBoxY + kItTileX) {
     hbx = 4 + tid - 2 * kItRBoxY, hby = 0;  // row y0-1
   } else {
@@ -363,6 +371,7 @@ __device__ __forceinline__ void iter_rows_tma(const TmaTile &t, const CUtensorMa
 }
 
 // Sums v[0..3] over the block (fixed order); valid in thread 0.
+template <int BLOCK>
 __device__ __forceinline__ void block_sum4(double v[4], double *smem /* [4 * 32] */) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -373,7 +382,7 @@ __device__ __forceinline__ void block_sum4(double v[4], double *smem /* [4 * 32]
   __syncthreads();
   if (wid == 0) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] = warp_sum(lane < kBlock / 32 ? smem[k * 32 + lane] : 0.0);
+    for (int k = 0; k < 4; ++k) v[k] = warp_sum(lane < BLOCK / 32 ? smem[k * 32 + lane] : 0.0);
   }
   __syncthreads();
 }
@@ -381,9 +390,10 @@ __device__ __forceinline__ void block_sum4(double v[4], double *smem /* [4 * 32]
 // Four partials per block at partials[k * gridDim.x + block]; true in every
 // thread of the last block to arrive, whose thread 0 then holds the totals
 // summed in block order.
+template <int BLOCK>
 __device__ __forceinline__ bool reduce4_last(const Reduction &red, double v[4], double *smem) {
   __shared__ bool s_last;
-  block_sum4(v, smem);
+  block_sum4<BLOCK>(v, smem);
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) red.partials[k * gridDim.x + blockIdx.x] = v[k];
@@ -396,11 +406,11 @@ __device__ __forceinline__ bool reduce4_last(const Reduction &red, double v[4], 
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     double a = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += kBlock)
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += BLOCK)
       a = __dadd_rn(a, ((volatile double *)red.partials)[k * gridDim.x + i]);
     v[k] = a;
   }
-  block_sum4(v, smem);
+  block_sum4<BLOCK>(v, smem);
   if (threadIdx.x == 0) *red.counter = 0u;
   return true;
 }

@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_residual_f(SpmvArg
   EpiResidualF epi{g.b, g.r, 0.0};
   double v[4] = {S::rows(a, g.x, epi), 0.0, 0.0, 0.0};
   v[1] = epi.bb;
-  if (reduce4_last(g.red, v, smem) && threadIdx.x == 0) {
+  if (reduce4_last<kBlock>(g.red, v, smem) && threadIdx.x == 0) {
     MixedState &st = *g.st;
     if (FIRST) {
       st.bb = v[1];
@@ -360,12 +360,12 @@ __global__ void __launch_bounds__(kBlock) k_mp_end_inner(MixedArgs g) {
 
 // One fused pass of the matrix-free inner CG (hpccg_iter_tma.cuh).  Pass k
 // reads r and p from buffers k & 1 and writes buffers (k + 1) & 1; p0, p1
-// (box 40 x 68), r0, r1 (box 40 x 66) and dm (box 32 x 64, of g.d) are the
+// (box 72 x 68), r0, r1 (box 72 x 66) and dm (box 64 x 64, of g.d) are the
 // tensor maps of the buffers.
 struct IterBufs {
   float *r[2], *p[2];
 };
-__global__ void __launch_bounds__(kBlock, 2) k_mp_iter_tma(MixedArgs g, TmaTile t, IterBufs b,
+__global__ void __launch_bounds__(kItBlock, 1) k_mp_iter_tma(MixedArgs g, TmaTile t, IterBufs b,
                                                           const __grid_constant__ CUtensorMap p0,
                                                           const __grid_constant__ CUtensorMap p1,
                                                           const __grid_constant__ CUtensorMap r0,
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_mp_iter_tma(MixedArgs g, TmaTile 
   else
     iter_rows_tma<false>(t, par ? &p1 : &p0, par ? &r1 : &r0, &dm, b.r[par ^ 1], b.p[par ^ 1], g.d, sc, v,
                          &st->status);
-  if (reduce4_last(g.red, v, smem) && threadIdx.x == 0) {
+  if (reduce4_last<kItBlock>(g.red, v, smem) && threadIdx.x == 0) {
     const double pAp = v[0], rAp = v[1], ApAp = v[2], rr = v[3];
     st->pAp = pAp;
     st->rAp = rAp;
@@ -494,12 +494,12 @@ static TmaTile iter_plan(const hpccg_ctx *c) {
     return none;
   }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_iter_tma, kBlock, kItSmemBytes) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mp_iter_tma, kItBlock, kItSmemBytes) != cudaSuccess ||
       per_sm < 1) {
     cudaGetLastError();
     return none;
   }
-  const TmaTile t = tma_tile_plan(c->gx, c->gy, c->gz, c->num_sms * per_sm);
+  const TmaTile t = tma_tile_plan(c->gx, c->gy, c->gz, c->num_sms * per_sm, kItTileX, kItTileY);
   // the refinement residual of the fused path reduces four values per block too
   const PlaneMap q = boxw_map(4, c->gx, c->gy, c->gz, (int64_t)c->num_sms * StratStencilBox64::kMinBlocks * kBlock);
   if (q.plane <= 0 || plane_grid(q) > kItMaxGrid) return none;
@@ -659,10 +659,10 @@ static int mixed_res(hpccg_ctx *c, int precision, MixedRes **out) {
         HPCCG_CUDA(cudaMalloc(&m->p2, vec));
         HPCCG_CUDA(cudaMemsetAsync(m->p2, 0, vec, c->stream));
       }
-      m->iter = make_stencil_tmap(&m->itmap[0], m->p, c->gx, c->gy, c->gz, kItPBoxY) == HPCCG_OK &&
-                make_stencil_tmap(&m->itmap[1], m->p2, c->gx, c->gy, c->gz, kItPBoxY) == HPCCG_OK &&
-                make_stencil_tmap(&m->itmap[2], m->r, c->gx, c->gy, c->gz, kItRBoxY) == HPCCG_OK &&
-                make_stencil_tmap(&m->itmap[3], m->r2, c->gx, c->gy, c->gz, kItRBoxY) == HPCCG_OK &&
+      m->iter = make_stencil_tmap(&m->itmap[0], m->p, c->gx, c->gy, c->gz, kItPBoxY, kItBoxX) == HPCCG_OK &&
+                make_stencil_tmap(&m->itmap[1], m->p2, c->gx, c->gy, c->gz, kItPBoxY, kItBoxX) == HPCCG_OK &&
+                make_stencil_tmap(&m->itmap[2], m->r, c->gx, c->gy, c->gz, kItRBoxY, kItBoxX) == HPCCG_OK &&
+                make_stencil_tmap(&m->itmap[3], m->r2, c->gx, c->gy, c->gz, kItRBoxY, kItBoxX) == HPCCG_OK &&
                 make_stencil_tmap(&m->itmap[4], m->d, c->gx, c->gy, c->gz, kItTileY, kItTileX) == HPCCG_OK;
     }
     m->tma_gx = c->gx;
@@ -678,7 +678,7 @@ static bool use_iter(const hpccg_ctx *c, const MixedRes *m) {
 
 static void launch_iter(hpccg_ctx *c, MixedRes *m, const MixedArgs &g, cudaStream_t s) {
   const IterBufs b{{m->r, m->r2}, {m->p, m->p2}};
-  k_mp_iter_tma<<<tma_tile_grid(m->itile), kBlock, kItSmemBytes, s>>>(g, m->itile, b, m->itmap[0], m->itmap[1],
+  k_mp_iter_tma<<<tma_tile_grid(m->itile), kItBlock, kItSmemBytes, s>>>(g, m->itile, b, m->itmap[0], m->itmap[1],
                                                                       m->itmap[2], m->itmap[3], m->itmap[4]);
 }
 
@@ -1102,8 +1102,8 @@ extern "C" int hpccg_gpu_mixed_pass(hpccg_ctx *c, const float *d_r, const float 
   if (rc) return rc;
   if (!uses_stencil(c) || !m->iter) return HPCCG_ERR_UNSUPPORTED;
   CUtensorMap pm, rm, dm;
-  if (make_stencil_tmap(&pm, d_p, c->gx, c->gy, c->gz, kItPBoxY) != HPCCG_OK ||
-      make_stencil_tmap(&rm, d_r, c->gx, c->gy, c->gz, kItRBoxY) != HPCCG_OK ||
+  if (make_stencil_tmap(&pm, d_p, c->gx, c->gy, c->gz, kItPBoxY, kItBoxX) != HPCCG_OK ||
+      make_stencil_tmap(&rm, d_r, c->gx, c->gy, c->gz, kItRBoxY, kItBoxX) != HPCCG_OK ||
       make_stencil_tmap(&dm, d_d, c->gx, c->gy, c->gz, kItTileY, kItTileX) != HPCCG_OK)
     return HPCCG_ERR_UNSUPPORTED;
   MixedState h0 = {};
@@ -1118,7 +1118,7 @@ extern "C" int hpccg_gpu_mixed_pass(hpccg_ctx *c, const float *d_r, const float 
   g.use_cond = 0;
   g.d = d_d;
   const IterBufs b{{const_cast<float *>(d_r), d_r_out}, {const_cast<float *>(d_p), d_p_out}};
-  k_mp_iter_tma<<<tma_tile_grid(m->itile), kBlock, kItSmemBytes, c->stream>>>(g, m->itile, b, pm, pm, rm, rm, dm);
+  k_mp_iter_tma<<<tma_tile_grid(m->itile), kItBlock, kItSmemBytes, c->stream>>>(g, m->itile, b, pm, pm, rm, rm, dm);
   HPCCG_CUDA(cudaGetLastError());
   MixedState hs;
   HPCCG_CUDA(cudaMemcpyAsync(&hs, m->st, sizeof(MixedState), cudaMemcpyDeviceToHost, c->stream));

@@ -38,11 +38,12 @@ struct TmaTile {
 
 // Host: tiles and z chunks for one wave of `resident_ctas` CTAs; nzc = 0 when
 // the grid does not allow the tensor map (nx not a multiple of 4).
-inline TmaTile tma_tile_plan(int nx, int ny, int nz, int resident_ctas) {
+inline TmaTile tma_tile_plan(int nx, int ny, int nz, int resident_ctas, int tile_x = kTmaTileX,
+                             int tile_y = kTmaTileY) {
   TmaTile t{nx, ny, nz, 0, 0, 0, 0};
   if (nx < 4 || ny < 1 || nz < 1 || nx % 4) return t;
-  t.tiles_x = (nx + kTmaTileX - 1) / kTmaTileX;
-  t.tiles_y = (ny + kTmaTileY - 1) / kTmaTileY;
+  t.tiles_x = (nx + tile_x - 1) / tile_x;
+  t.tiles_y = (ny + tile_y - 1) / tile_y;
   const int per_plane = t.tiles_x * t.tiles_y;
   int k = resident_ctas / per_plane;
   k = k < 1 ? 1 : (k > nz ? nz : k);

@@ -92,27 +92,32 @@ def test_slab_spmv_pack_scatter(torch, zs, nx, ny, nz, P, mode):
 
 
 @pytest.mark.parametrize("mode", [0, 1])
-@pytest.mark.parametrize("nx,ny,nz,P", [(8, 6, 4, 2), (6, 5, 4, 3), (5, 4, 2, 4), (4, 4, 1, 3)])
-def test_group_cg_matches_oracle(torch, zs, nx, ny, nz, P, mode):
+@pytest.mark.parametrize("nx,ny,nz,P,iters", [(8, 6, 4, 2, 60), (6, 5, 4, 3, 60), (5, 4, 2, 4, 60),
+                                              (6, 5, 1, 3, 40)])
+def test_group_cg_matches_oracle(torch, zs, nx, ny, nz, P, iters, mode):
+    """(6, 5, 1, 3): one plane per rank, so every row reaches both neighbours and the two
+    halo forms order the externals differently; 40 iterations stay clear of the exact
+    convergence of so small a system (after it the reference divides 0/0)."""
     plans, slabs = _build(zs, nx, ny, nz, P, mode)
     G, x0, bg, _ = oracle.generate_matrix(nx, ny, nz * P)
     n = nx * ny * nz
     ref = oracle.SlabPlan(nx, ny, nz, P, mode)
-    rx, rit, rnr, rh = ref.cg(bg, x0, 150, 0.0)
+    rx, rit, rnr, rh = ref.cg(bg, x0, iters, 0.0)
+    assert np.all(np.isfinite(rh)) and rh[-1] > 0
     d_b = [torch.from_numpy(bg[r * n:(r + 1) * n].copy()).cuda() for r in range(P)]
     d_x = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(P)]
-    it, nr, h, st = zs.group_cg(slabs, d_b, d_x, 150, 0.0)
+    it, nr, h, st = zs.group_cg(slabs, d_b, d_x, iters, 0.0)
     assert it == rit
     assert_history_parity(h, rh)
     x = np.concatenate([t.cpu().numpy() for t in d_x])
     assert np.abs(x - rx).max() <= 1e-10 and np.abs(x - 1.0).max() <= 1e-10
     # a tolerance stop (the reference's normr < tolerance at the top of an iteration)
     tol = 1e-8 * np.linalg.norm(bg)
-    rx, rit, rnr, rh = ref.cg(bg, x0, 150, tol)
+    rx, rit, rnr, rh = ref.cg(bg, x0, iters, tol)
     for t in d_x:
         t.zero_()
-    it, nr, h, st = zs.group_cg(slabs, d_b, d_x, 150, tol)
-    assert it == rit and it < 150
+    it, nr, h, st = zs.group_cg(slabs, d_b, d_x, iters, tol)
+    assert it == rit and it < iters
     assert_history_parity(h, rh)
     assert nr == pytest.approx(rnr, rel=1e-12)
     for s in slabs:
@@ -126,9 +131,9 @@ def test_group_cg_one_rank_equals_single_context(torch, zs):
     plans, slabs = _build(zs, 7, 6, 5, 1, 0)
     A, x0, b, _ = oracle.generate_matrix(7, 6, 5)
     M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
-    gx, it1, nr1, h1, _ = M.cg(b, x0.copy(), 80, 0.0)
+    gx, it1, nr1, h1, _ = M.cg(b, x0.copy(), 50, 0.0)
     d_b, d_x = [torch.from_numpy(b).cuda()], [torch.zeros(len(b), dtype=torch.float64, device="cuda")]
-    it, nr, h, st = zs.group_cg(slabs, d_b, d_x, 80, 0.0)
+    it, nr, h, st = zs.group_cg(slabs, d_b, d_x, 50, 0.0)
     assert it == it1
     assert_history_parity(h, h1)
     assert np.abs(d_x[0].cpu().numpy() - gx).max() <= 1e-12
