@@ -64,6 +64,29 @@ def _peaks():
     return 6650.0, 1590.0, "fallback"
 
 
+def _bf16_sustained():
+    """(burst, sustained, source) BF16 dense TFLOP/s from MEASURED_PEAKS.json, else the fallback figures."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        burst = float(d.get("bf16_tflops", 1590.0))
+        return burst, float(d.get("bf16_tflops_sustained", burst)), "measured"
+    return 1590.0, 1400.0, "fallback"
+
+
+# The U-Net's 3x3x3 convolutions as (input channels, level): level l runs on the grid coarsened
+# 2^l times per axis (csrc/unet.cu, kLayers), each layer 16 output channels; plus the 16 -> 1
+# projection at level 0.
+UNET_CONVS = [(1, 0), (16, 0), (16, 1), (16, 1), (16, 2), (16, 2), (16, 3), (16, 3), (32, 2), (16, 2),
+              (32, 1), (16, 1), (32, 0)]
+
+
+def unet_forward_flop(nx: int, ny: int, nz: int) -> float:
+    """Multiply-add FLOPs (2 per MAC) of one U-Net forward pass on an nx x ny x nz grid."""
+    vox = nx * ny * nz
+    return float(sum(2 * 27 * cin * 16 * vox / 8 ** lvl for cin, lvl in UNET_CONVS) + 2 * 16 * vox)
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -275,6 +298,8 @@ def batch_workload(hp, torch, args):
                         .abs().max()) for s in range(B.nsys))
         out[name] = {"ms": float(np.median(times)), "status": int(rc), "max_relres": float(relres.max()),
                      "iters_min_max": [int(iters.min()), int(iters.max())], "max_abs_err_vs_xstar": err}
+        if name == "fp64":
+            fp64_iters = iters.copy()
     out["schedule"] = list(B.get_schedule())
     B.set_spmv(hp.SPMV_STENCIL)  # matrix-free rows, same iterates in FP64
     for name, prec in (("fp64_stencil", hp.PREC_FP64), ("fp32_ir_stencil", hp.PREC_FP32)):
@@ -284,8 +309,13 @@ def batch_workload(hp, torch, args):
             iters, relres, outer, rc = B.solve(d_b, d_x, prec, REL_TOL)
             if rep >= args.warmup:
                 times.append(B.last_solve_ms())
+        err = max(float((d_x[B.offsets[s]:B.offsets[s] + B.nrows[s]] - d_xs[B.offsets[s]:B.offsets[s] + B.nrows[s]])
+                        .abs().max()) for s in range(B.nsys))
         out[name] = {"ms": float(np.median(times)), "status": int(rc), "max_relres": float(relres.max()),
-                     "iters_min_max": [int(iters.min()), int(iters.max())]}
+                     "iters_min_max": [int(iters.min()), int(iters.max())], "max_abs_err_vs_xstar": err}
+        if name == "fp64_stencil":  # the matrix-free rows repeat the stored rows' sums: same iterations
+            out[name]["iters_equal_stored"] = bool(np.array_equal(iters, fp64_iters))
+            assert out[name]["iters_equal_stored"], "matrix-free FP64 batch took other iteration counts"
     out["schedule_stencil"] = list(B.get_schedule())
     seq = 0.0
     for s, (nx, ny, nz) in enumerate(sizes):
@@ -377,8 +407,17 @@ def run_ours(args):
             return ({"iterations": info.iters, "nn_applies": info.nn_applies, "fallback": info.fallback},
                     4 + 25 * info.iters)
 
+        def learned_mixed():
+            info, st = learned.solve_mixed_fcg(M, net, (n, n, nz), d_b, d_x, REL_TOL)
+            assert st == hp.HPCCG_OK, st
+            return ({"outer": info.outer_iters, "inner": info.inner_iters, "nn_applies": info.nn_applies,
+                     "fallback": info.fallback}, 3 + 6 * info.inner_iters + 3 * info.outer_iters)
+
         methods.append(("learned_fcg", "flexible PCG (FP64, matrix-free stencil SpMV) with the trained U-Net "
                         "preconditioner (BF16 tensor cores)", learned_fcg, STENCIL))
+        methods.append(("learned_mixed_fcg", "FP64 iterative refinement (FP64 stencil residual) around the "
+                        "U-Net-preconditioned flexible CG in FP32 vectors (matrix-free FP32 operator)",
+                        learned_mixed, STENCIL))
     results = {}
     clk_summary = None
     if args.methods:
@@ -421,6 +460,17 @@ def run_ours(args):
         learned_info.update({"grf_rhs": {"plain_fp64_cg_iters": it_plain, "plain_fp64_cg_ms": plain_grf_ms,
                                          "learned_fcg_iters": info.iters, "learned_fcg_ms": M.last_solve_ms(),
                                          "relres": info.relres, "fallback": info.fallback}})
+        grf_mixed = {}
+        for name, nn in (("plain_fp32_ir", None), ("learned_mixed_fcg", net)):
+            d_x.zero_()
+            mi, _ = learned.solve_mixed_fcg(M, nn, n, grf, d_x, REL_TOL)
+            grf_mixed[name] = {"ms": M.last_solve_ms(), "outer": mi.outer_iters, "inner": mi.inner_iters,
+                               "nn_applies": mi.nn_applies, "relres": mi.relres, "fallback": mi.fallback}
+        d_x.zero_()
+        mi, _ = M.solve_mixed_device(grf, d_x, hp.PREC_FP32, REL_TOL)
+        grf_mixed["fp32_ir_stencil"] = {"ms": M.last_solve_ms(), "outer": mi.outer_iters,
+                                        "inner": mi.inner_iters, "relres": mi.relres}
+        learned_info["grf_rhs"]["mixed"] = grf_mixed
         d_in = torch.randn(N, dtype=torch.float32, device=dev)
         d_out = torch.empty_like(d_in)
         learned_info["unet_forward_ms"] = net.time_forward(d_in, d_out, n, n, n, 3)
@@ -428,7 +478,7 @@ def run_ours(args):
     ok = {k: v for k, v in results.items() if v["true_relres"] <= REL_TOL}
     head = min(ok, key=lambda k: ok[k]["ms"])
     plain_ms = results["fp64_cg"]["ms"]
-    head_kind = STENCIL if head.endswith("_stencil") or head == "learned_fcg" else ELL
+    head_kind = STENCIL if head.endswith("_stencil") or head.startswith("learned") else ELL
 
     # end to end through the host-array C-ABI call of the headline solver, pinned host buffers
     h_b = torch.empty(N, dtype=torch.float64, pin_memory=True)
@@ -442,10 +492,13 @@ def run_ours(args):
         t0 = time.perf_counter()
         if head.startswith("fp64_cg"):
             M.cg(bb, xb, max_iter, tol, history=False)
-        elif head == "learned_fcg":
+        elif head.startswith("learned"):
             h_bd = torch.from_numpy(bb).to(dev)
             d_xe = torch.zeros_like(h_bd)
-            learned.solve_fcg(M, net, n, h_bd, d_xe, REL_TOL, max_iter)
+            if head == "learned_fcg":
+                learned.solve_fcg(M, net, n, h_bd, d_xe, REL_TOL, max_iter)
+            else:
+                learned.solve_mixed_fcg(M, net, n, h_bd, d_xe, REL_TOL)
             xb[:] = d_xe.cpu().numpy()
         else:
             M.solve_mixed(bb, xb, hp.PREC_BF16 if head == "bf16_ir" else hp.PREC_FP32, REL_TOL)
@@ -501,7 +554,19 @@ def run_ours(args):
                                 "peak_source": peak_kind, "traffic": traffic if n == 256 and cubic else None,
                                 "inner_iteration_ms": sum(km)}
     roofs["fp32_ir_stencil"]["frac"] = roofs["fp32_ir_stencil"]["achieved"] / hbm
-    roofs["learned_fcg"] = roofs["fp64_cg_stencil"]
+    if learned_info is not None:
+        # the network's dominant work: the 3x3x3 convolutions on the tensor cores, against the
+        # sustained BF16 peak (the forward pass runs inside a seconds-long solve)
+        flop = unet_forward_flop(n, n, nz)
+        fms = learned_info["unet_forward_ms"]
+        _, bf16_sust, bf16_kind = _bf16_sustained()
+        conv = {"bound": "tensor", "kernel": "U-Net forward pass (k_conv3_row tcgen05 convolutions, BF16 in, "
+                "FP32 accumulate; plus the CUDA-core input layer, pooling and upsampling)",
+                "kernel_ms": fms, "flop_per_launch": flop, "achieved": flop / (fms * 1e-3) / 1e12,
+                "peak": bf16_sust, "unit": "TFLOP/s", "peak_source": bf16_kind, "traffic": None}
+        conv["frac"] = conv["achieved"] / bf16_sust
+        roofs["learned_fcg"] = conv
+        roofs["learned_mixed_fcg"] = conv
 
     if rank != 0:
         if ws > 1:
@@ -532,7 +597,8 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 16 * N, "d2h_bytes_per_step": 8 * N,
                 "call": "hpccg_gpu_cg" if head.startswith("fp64_cg") else
-                ("hpccg_gpu_solve_fcg" if head == "learned_fcg" else "hpccg_gpu_solve_mixed")},
+                ("hpccg_gpu_solve_fcg" if head == "learned_fcg" else
+                 "hpccg_gpu_solve_mixed_fcg" if head == "learned_mixed_fcg" else "hpccg_gpu_solve_mixed")},
         "gpu_launches": hr["gpu_launches"],
         "clocks": hr["clocks"],
     }

@@ -2,8 +2,9 @@
 
 Every numerical step runs in the library's own kernels through the C-ABI:
 the FP64 CG that generates residual->error pairs (hpccg_gpu_cg_device), the
-U-Net forward/backward/Adam (hpccg_unet_*), and the flexible PCG
-(hpccg_gpu_solve_fcg).  torch provides device memory and, for the synthetic
+U-Net forward/backward/Adam (hpccg_unet_*), and the flexible PCG in FP64
+(hpccg_gpu_solve_fcg) or in FP32 inside FP64 refinement
+(hpccg_gpu_solve_mixed_fcg).  torch provides device memory and, for the synthetic
 right-hand sides only, the FFT that shapes white noise into a Gaussian random
 field.
 """
@@ -27,6 +28,18 @@ _lib.hpccg_gpu_solve_fcg.restype = ctypes.c_int
 _lib.hpccg_gpu_solve_fcg.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_int32,
                                      ctypes.c_void_p]
+
+
+class MixedFcgInfo(ctypes.Structure):
+    _fields_ = [("outer_iters", ctypes.c_int32), ("inner_iters", ctypes.c_int32), ("nn_applies", ctypes.c_int32),
+                ("fallback", ctypes.c_int32), ("status", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("relres", ctypes.c_double)]
+
+
+_lib.hpccg_gpu_solve_mixed_fcg.restype = ctypes.c_int
+_lib.hpccg_gpu_solve_mixed_fcg.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                           ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                           ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
 
 
 def gaussian_random_field(M: Matrix, n: int, seed: int, torch):
@@ -165,6 +178,20 @@ def solve_fcg(M: Matrix, net: Unet | None, n: int, d_b, d_x, rel_tol: float = 1e
     rc = _lib.hpccg_gpu_solve_fcg(M.handle, None if net is None else net.handle, n, n, n, _dptr(d_b), _dptr(d_x),
                                   rel_tol, max_iter, ctypes.byref(info))
     _check(rc, "solve_fcg", allow=(HPCCG_OK, HPCCG_ERR_NOT_CONVERGED))
+    return info, rc
+
+
+def solve_mixed_fcg(M: Matrix, net: Unet | None, n, d_b, d_x, rel_tol: float = 1e-8, max_outer: int = 20,
+                    max_inner: int = 1000):
+    """FP64 iterative refinement around the network-preconditioned flexible CG in FP32
+    (hpccg_gpu_solve_mixed_fcg; net=None: plain FP32 CG).  n: the grid edge or (nx, ny, nz).
+    Returns (MixedFcgInfo, status)."""
+    nx, ny, nz = (n, n, n) if isinstance(n, int) else n
+    _sync_torch()
+    info = MixedFcgInfo()
+    rc = _lib.hpccg_gpu_solve_mixed_fcg(M.handle, None if net is None else net.handle, nx, ny, nz, _dptr(d_b),
+                                        _dptr(d_x), rel_tol, max_outer, max_inner, ctypes.byref(info))
+    _check(rc, "solve_mixed_fcg", allow=(HPCCG_OK, HPCCG_ERR_NOT_CONVERGED))
     return info, rc
 
 

@@ -290,6 +290,30 @@ typedef struct hpccg_fcg_info {
 int hpccg_gpu_solve_fcg(hpccg_ctx *ctx, hpccg_unet *unet, int32_t nx, int32_t ny, int32_t nz, const double *d_b,
                         double *d_x, double rel_tol, int32_t max_iter, hpccg_fcg_info *info);
 
+/* The learned preconditioner inside mixed precision: FP64 iterative
+ * refinement (r = b - A x with the context's FP64 SpMV, stop at
+ * ||r|| <= rel_tol ||b||, x += ||r|| d) around a flexible (Polak-Ribiere) CG
+ * with FP32 vectors, the FP32 matrix-free operator and z = s * net(r/s); the
+ * inner solve stops at max(1e-5, 0.5 rel_tol ||b|| / ||r||) relative, plain
+ * CG takes over as in hpccg_gpu_solve_fcg, unet = NULL runs plain FP32 CG.
+ * Needs the context's geometry (hpccg_gpu_set_geometry or a generated
+ * context) equal to nx, ny, nz (multiples of 8 with a network), else
+ * HPCCG_ERR_UNSUPPORTED.  Device arrays; x holds x0 on entry.  No reference
+ * counterpart: it replaces the whole cg call (MPI/src/numerics.F90:41-162)
+ * with a time-to-tolerance solve. */
+typedef struct hpccg_mixed_fcg_info {
+  int32_t outer_iters; /* FP64 refinement cycles          */
+  int32_t inner_iters; /* FP32 flexible-CG iterations     */
+  int32_t nn_applies;  /* network applications            */
+  int32_t fallback;    /* 1 if plain CG took over         */
+  int32_t status;
+  int32_t reserved;
+  double relres;       /* final FP64 ||b - A x|| / ||b||  */
+} hpccg_mixed_fcg_info;
+int hpccg_gpu_solve_mixed_fcg(hpccg_ctx *ctx, hpccg_unet *unet, int32_t nx, int32_t ny, int32_t nz,
+                              const double *d_b, double *d_x, double rel_tol, int32_t max_outer, int32_t max_inner,
+                              hpccg_mixed_fcg_info *info);
+
 /* ---- op-level drop-ins (device arrays), MPI/src/SparseMatrix.F90:213-232
  *      and MPI/src/vector_operations.F90:40-169 ------------------------------ */
 

@@ -409,7 +409,7 @@ int orc_cg_slabs(const orc_slab_plan *P, const double *b, double *x, int32_t max
     double **p = (double **)malloc(sizeof(double *) * (size_t)nr);
     double **r = (double **)malloc(sizeof(double *) * (size_t)nr);
     double **Ap = (double **)malloc(sizeof(double *) * (size_t)nr);
-    double *loc = (double *)malloc(sizeof(double) * (size_t)nr);
+    double *loc = (double *)calloc((size_t)nr, sizeof(double));
     for (int32_t q = 0; q < nr; ++q) {
         p[q] = (double *)calloc((size_t)P->r[q].local_ncol + 1, sizeof(double));
         r[q] = (double *)malloc(sizeof(double) * (size_t)n);

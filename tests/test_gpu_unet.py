@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 import unet_oracle as uo
+import oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -140,3 +141,18 @@ def test_trained_network_reduces_fcg_iterations(env):
             assert st0 == hp.HPCCG_OK and st1 == hp.HPCCG_OK
             assert fcg.relres <= 1e-8 and plain.relres <= 1e-8
             assert fcg.iters <= 0.6 * plain.iters, (n, sd, fcg.iters, plain.iters)
+            # the same network inside mixed precision: FP32 flexible CG in FP64 refinement,
+            # against plain FP32 CG through the same solver; the oracle judges the result
+            bh = b.cpu().numpy()
+            runs = {}
+            for name, nn in (("plain", None), ("learned", net)):
+                x.zero_()
+                info, st = learned.solve_mixed_fcg(M, nn, n, b, x)
+                assert st == hp.HPCCG_OK, name
+                rel = oracle.grid_true_relres(n, n, n, bh, x.cpu().numpy())
+                assert rel <= 1e-8 * (1 + 1e-6), (name, rel)
+                assert info.relres == pytest.approx(rel, rel=1e-6)
+                runs[name] = info
+            assert runs["learned"].nn_applies > 0
+            assert runs["learned"].inner_iters <= 0.6 * runs["plain"].inner_iters, (
+                n, sd, runs["learned"].inner_iters, runs["plain"].inner_iters)
