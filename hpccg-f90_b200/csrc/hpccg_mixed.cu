@@ -597,7 +597,8 @@ static bool uses_stencil(const hpccg_ctx *c) { return spmv_args(c).kind == HPCCG
 // wave of resident threads (StratLpStencil: 256 threads x 4 blocks per SM) when
 // nx allows it, else the context's plane map.
 static PlaneMap lp_map(const hpccg_ctx *c) {
-  const PlaneMap pm = spmv_args(c).pm;
+  // the FP32 one-column walk takes one line a thread
+  const PlaneMap pm = c->gx ? plane_map(c->gx, c->gy, c->gz, kMaxPartials) : spmv_args(c).pm;
   if (!uses_stencil(c) || pm.plane <= 0) return pm;
   const PlaneMap q = boxw_map(4, c->gx, c->gy, c->gz, (int64_t)c->num_sms * StratLpStencil::kMinBlocks * kBlock);
   return q.plane > 0 ? q : pm;

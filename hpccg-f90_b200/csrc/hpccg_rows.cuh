@@ -33,6 +33,13 @@ template <class Body>
 __device__ __forceinline__ void thread_rows(int n, const PlaneMap &m, Body &&body) {
   if (m.plane > 0) {
     const PlaneSpan sp = plane_span(m, n / m.plane);
+    if (m.ry == 2) {  // the column pair (x, y), (x, y+1), the order of stencil_column2
+      for (int z = sp.z0; z < sp.z1; ++z) {
+        body(sp.c + z * m.plane);
+        body(sp.c + m.nx + z * m.plane);
+      }
+      return;
+    }
     for (int z = sp.z0; z < sp.z1; ++z) body(sp.c + z * m.plane);
     return;
   }
@@ -228,7 +235,7 @@ struct StratCsr {
 };
 
 struct StratStencil {
-  static constexpr int kMinBlocks = 4;
+  static constexpr int kMinBlocks = 3;
   static int grid(const SpmvArgs &a, int dflt) { return plane_or(a.pm, dflt); }
   template <class Epi>
   static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
@@ -298,7 +305,7 @@ inline SpmvArgs spmv_args(const hpccg_ctx *c) {
   a.ell_col = c->d_ell_col;
   a.ell_val = c->d_ell_val;
   a.geom = StencilGeom{c->gx, c->gy, c->gz};
-  a.pm = c->gx ? plane_map(c->gx, c->gy, c->gz, kMaxPartials) : PlaneMap{0, 0, 0, 1};
+  a.pm = c->gx ? plane_map(c->gx, c->gy, c->gz, kMaxPartials, 2) : PlaneMap{0, 0, 0, 1, 1, 0};
   return a;
 }
 
