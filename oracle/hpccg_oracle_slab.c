@@ -338,6 +338,8 @@ int32_t orc_slab_plan_get(const orc_slab_plan *P, int32_t rank, int32_t what, in
     case ORC_SLAB_SEND_LENGTH:
         return copy_out(out, R->send_length, R->num_neighbors);
     case ORC_SLAB_ELEMENTS_TO_SEND:
+        if (!R->elements_to_send)
+            return 0;                   /* the CAF-V2 form sends nothing */
         return copy_out(out, R->elements_to_send + 1, R->total_to_be_sent);
     case ORC_SLAB_BLOCKS:
         if (out)
@@ -349,6 +351,8 @@ int32_t orc_slab_plan_get(const orc_slab_plan *P, int32_t rank, int32_t what, in
             }
         return R->num_blocks;
     case ORC_SLAB_REMOTE_INDEX:
+        if (!R->remote_index)
+            return 0;                   /* the MPI form has no block gets */
         return copy_out(out, R->remote_index + 1, R->num_external);
     default:
         return -1;

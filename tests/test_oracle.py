@@ -150,3 +150,20 @@ def test_grid_operator_equals_csr_oracle(nx, ny, nz):
     xs = oracle.uniform_pm1(5, A.nrow)
     bs = oracle.spmv(A, xs)
     assert oracle.grid_true_relres(nx, ny, nz, bs, v) == oracle.true_relres(A, bs, v)
+
+
+@pytest.mark.parametrize("case", ["4x3x2x2", "4x3x2x3", "3x3x1x3"])
+@pytest.mark.parametrize("tag", ["mpi", "get"])
+def test_slab_oracle_against_fixtures(case, tag):
+    """The multi-rank oracle (make_local_matrix in both forms, the multi-rank CG) against the
+    committed fixtures, list by list."""
+    nx, ny, nz, P = map(int, case.split("x"))
+    gold = np.load(os.path.join(GOLDEN, f"slab_{case}_{tag}.npz"))
+    plan = oracle.SlabPlan(nx, ny, nz, P, oracle.HALO_MPI if tag == "mpi" else oracle.HALO_GET)
+    for key in gold.files:
+        if key == "hist":
+            continue
+        r, field = key.split("_", 1)
+        np.testing.assert_array_equal(plan.get(int(r[1:]), field), gold[key], err_msg=key)
+    G, x0, bg, _ = oracle.generate_matrix(nx, ny, nz * P)
+    np.testing.assert_array_equal(plan.cg(bg, x0, 30, 0.0)[3], gold["hist"])
