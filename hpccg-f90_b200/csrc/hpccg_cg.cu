@@ -38,7 +38,7 @@ __device__ __forceinline__ void set_condition(const CgArgs &g, int v) {
 
 // Prepare phase, MPI/src/numerics.F90:91-104 (vcopy x->p; spmv; waxpby; ddot1).
 template <class S>
-__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_cg_residual(SpmvArgs a, CgArgs g) {
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_cg_residual(const __grid_constant__ SpmvArgs a, CgArgs g) {
   __shared__ double smem[32];
   EpiResidual epi{g.b, g.r};
   const double part = S::rows(a, g.x, epi);
@@ -52,11 +52,11 @@ __global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_cg_residual(SpmvArgs 
       st.normr = sqrt(rr);
       st.k = 1;
       st.niters = 0;
-      st.status = HPCCG_OK;
+      if (st.status != HPCCG_ERR_TIMEOUT) st.status = HPCCG_OK;  // a TMA walk's expired wait stands
       st.x_pending = 0;
       if (g.hist_cap > 0) g.hist[0] = st.normr;
       // Top of iteration 1 (:109-126): stop test, then normr = sqrt(rtrans).
-      const int cont = (st.max_iter >= 1) && !(st.normr < st.tolerance);
+      const int cont = !st.status && (st.max_iter >= 1) && !(st.normr < st.tolerance);
       if (cont && g.hist_cap > 1) g.hist[1] = st.normr;
       set_condition(g, cont);
     }
@@ -106,9 +106,10 @@ __global__ void __launch_bounds__(kBlock) k_cg_update_p(CgArgs g) {
 
 // K_A: MPI/src/numerics.F90:133-138 (spmv; ddot; alpha = rtrans/alpha).
 template <class S>
-__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_cg_spmv_dot(SpmvArgs a, CgArgs g) {
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_cg_spmv_dot(const __grid_constant__ SpmvArgs a, CgArgs g) {
   __shared__ double smem[32];
-  if (g.st->status) return;
+  // block-uniform exit: a TMA walk's barriers need every thread of the block
+  if (__syncthreads_or(threadIdx.x == 0 && g.st->status)) return;
   EpiDot epi{g.p, g.Ap};
   const double part = S::rows(a, g.p, epi);
   const double tot = block_sum<kBlock>(part, smem);
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_finish(CgArgs g) {
 
 // Plain y = A x (op-level drop-in and timing).
 template <class S>
-__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_spmv(SpmvArgs a, const double *x, double *y) {
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_spmv(const __grid_constant__ SpmvArgs a, const double *x, double *y) {
   EpiStore epi{y};
   S::rows(a, x, epi);
 }
@@ -212,20 +213,26 @@ static CgArgs cg_args(hpccg_ctx *c, cudaGraphConditionalHandle h, int use_cond) 
 }
 
 static int launch_prepare(hpccg_ctx *c, const SpmvArgs &a, const CgArgs &g, cudaStream_t s) {
-  return dispatch_strategy(a, [&](auto strat) {
-    using St = decltype(strat);
-    k_cg_residual<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, g);
-    return (int)cudaGetLastError();
-  });
+  return dispatch_strategy(
+      a,
+      [&](auto strat) {
+        using St = decltype(strat);
+        k_cg_residual<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, g);
+        return (int)cudaGetLastError();
+      },
+      g.x);
 }
 
 static int launch_body(hpccg_ctx *c, const SpmvArgs &a, const CgArgs &g, cudaStream_t s) {
   k_cg_update_p<<<c->grid, kBlock, 0, s>>>(g);
-  int rc = dispatch_strategy(a, [&](auto strat) {
-    using St = decltype(strat);
-    k_cg_spmv_dot<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, g);
-    return (int)cudaGetLastError();
-  });
+  int rc = dispatch_strategy(
+      a,
+      [&](auto strat) {
+        using St = decltype(strat);
+        k_cg_spmv_dot<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, g);
+        return (int)cudaGetLastError();
+      },
+      g.p);
   if (rc) return rc;
   k_cg_update_r<<<c->grid, kBlock, 0, s>>>(g);
   return (int)cudaGetLastError();
@@ -233,11 +240,14 @@ static int launch_body(hpccg_ctx *c, const SpmvArgs &a, const CgArgs &g, cudaStr
 
 int launch_spmv(hpccg_ctx *c, const double *x, double *y, cudaStream_t s) {
   const SpmvArgs a = spmv_args(c);
-  return dispatch_strategy(a, [&](auto strat) {
-    using St = decltype(strat);
-    k_spmv<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, x, y);
-    return (int)cudaGetLastError();
-  });
+  return dispatch_strategy(
+      a,
+      [&](auto strat) {
+        using St = decltype(strat);
+        k_spmv<St><<<St::grid(a, c->grid), kBlock, 0, s>>>(a, x, y);
+        return (int)cudaGetLastError();
+      },
+      x);
 }
 
 static void drop_graph(hpccg_ctx *c) {
@@ -520,11 +530,14 @@ extern "C" int hpccg_gpu_time_cg_kernels(hpccg_ctx *c, int32_t reps, float *ms) 
       if (which == 0) {
         k_cg_update_p<<<c->grid, kBlock, 0, c->stream>>>(g);
       } else if (which == 1) {
-        rc = dispatch_strategy(a, [&](auto strat) {
-          using St = decltype(strat);
-          k_cg_spmv_dot<St><<<St::grid(a, c->grid), kBlock, 0, c->stream>>>(a, g);
-          return 0;
-        });
+        rc = dispatch_strategy(
+            a,
+            [&](auto strat) {
+              using St = decltype(strat);
+              k_cg_spmv_dot<St><<<St::grid(a, c->grid), kBlock, 0, c->stream>>>(a, g);
+              return 0;
+            },
+            g.p);
       } else {
         k_cg_update_r<<<c->grid, kBlock, 0, c->stream>>>(g);
       }

@@ -32,7 +32,7 @@ struct FcgArgs {
 };
 
 template <class S>
-__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_fcg_spmv_dot(SpmvArgs a, FcgArgs g) {
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_fcg_spmv_dot(const __grid_constant__ SpmvArgs a, FcgArgs g) {
   __shared__ double smem[32];
   EpiDot epi{g.p, g.Ap};
   const double part = S::rows(a, g.p, epi);
@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_fcg_spmv_dot(SpmvArgs
 }
 
 template <class S>
-__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_fcg_residual(SpmvArgs a, FcgArgs g) {
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_fcg_residual(const __grid_constant__ SpmvArgs a, FcgArgs g) {
   __shared__ double smem[32];
   EpiResidual epi{g.b, g.r};
   const double part = S::rows(a, g.x, epi);

@@ -10,6 +10,7 @@
 //         counter, the CG scalar state and the residual history.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -69,6 +70,9 @@ struct hpccg_ctx {
   int grid = 0;  // blocks for streaming kernels (multiple of the SM count)
   // grid of generate_matrix the CSR was checked against (0: unknown)
   int32_t gx = 0, gy = 0, gz = 0;
+  // tensor maps of d_p and d_x for the FP64 TMA walk (tmaps_ok false: plain loads)
+  CUtensorMap tmaps[2];
+  bool tmaps_ok = false;
   // SpMV selection
   int spmv_kind = HPCCG_SPMV_AUTO;
   int spmv_param = 0;

@@ -9,7 +9,7 @@
 #include <algorithm>
 #include <vector>
 
-#include "hpccg_internal.cuh"
+#include "hpccg_rows.cuh"
 
 namespace hpccg {
 
@@ -373,6 +373,12 @@ extern "C" int hpccg_gpu_set_geometry(hpccg_ctx *c, int32_t nx, int32_t ny, int3
   c->gx = nx;
   c->gy = ny;
   c->gz = nz;
+  // the FP64 TMA walk under the tile map reads p and x through these maps;
+  // without them (a map the driver refuses) the same walk runs on plain loads
+  c->tmaps_ok = fp64_map(nx, ny, nz, c->num_sms).tiles_x > 0 &&
+                make_stencil_tmap64(&c->tmaps[0], c->d_p, nx, ny, nz, kR64BoxX, kR64BoxY) == HPCCG_OK &&
+                make_stencil_tmap64(&c->tmaps[1], c->d_x, nx, ny, nz, kR64BoxX, kR64BoxY) == HPCCG_OK;
+  c->cg_graph_kind = -1;  // a graph captured before holds the old map
   return HPCCG_OK;
 }
 

@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(kBlock) k_mp_bnorm(MixedArgs g) {
 
 // r64 = b - A x64 (FP64, reference order) and the outer decision.
 template <class S>
-__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_residual64(SpmvArgs a, MixedArgs g) {
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_residual64(const __grid_constant__ SpmvArgs a, MixedArgs g) {
   __shared__ double smem[32];
   EpiResidual epi{g.b, g.r64};
   const double part = S::rows(a, g.x, epi);
@@ -125,35 +125,75 @@ struct EpiResidualF {
   }
   __device__ __forceinline__ double operator()(int i, double s, double) { return (*this)(i, s); }
 };
+// Four rows at once (i a multiple of 4): b by two 16-byte loads, r by one.
+template <bool FIRST>
+struct EpiResidualF4 {
+  const double *b;
+  float *r;
+  double bb;
+  __device__ __forceinline__ double store4(int i, const double y[4]) {
+    const double2 b01 = __ldcs(reinterpret_cast<const double2 *>(b + i));
+    const double2 b23 = __ldcs(reinterpret_cast<const double2 *>(b + i) + 1);
+    const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+    float4 ro;
+    double rr = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (FIRST) bb = __dadd_rn(bb, __dmul_rn(bv[k], bv[k]));
+      const double rk = __dsub_rn(bv[k], y[k]);
+      reinterpret_cast<float *>(&ro)[k] = (float)rk;
+      rr = __dadd_rn(rr, __dmul_rn(rk, rk));
+    }
+    *reinterpret_cast<float4 *>(r + i) = ro;
+    return rr;
+  }
+};
+
+// The outer decision of the fused refinement from v[0] = r.r (and v[1] = b.b
+// on the first call); thread 0 of the last block.
+template <bool FIRST>
+__device__ __forceinline__ void residual_decision(const MixedArgs &g, const double v[4]) {
+  MixedState &st = *g.st;
+  if (FIRST) {
+    st.bb = v[1];
+    st.outer = 0;
+    st.inner_total = 0;
+    if (st.status != HPCCG_ERR_TIMEOUT) st.status = HPCCG_OK;  // a TMA walk's expired wait stands
+  }
+  const double rr = v[0];
+  st.rr64 = rr;
+  st.relres = st.bb > 0.0 ? sqrt(rr / st.bb) : 0.0;
+  int cont = !st.status && (st.relres > st.rel_tol) && (st.outer < st.max_outer);
+  if (!isfinite(st.relres)) {
+    st.status = HPCCG_ERR_BREAKDOWN;
+    cont = 0;
+  }
+  if (cont) {
+    st.scale = sqrt(rr);
+    st.target = st.inner_rtol > 0.0 ? st.inner_rtol : fmax(st.inner_floor, 0.5 * st.rel_tol / st.relres);
+    st.outer += 1;
+  }
+  set_outer(g, cont);
+}
+
 template <class S, bool FIRST>
-__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_residual_f(SpmvArgs a, MixedArgs g) {
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_residual_f(const __grid_constant__ SpmvArgs a, MixedArgs g) {
   __shared__ double smem[4 * 32];
   EpiResidualF epi{g.b, g.r, 0.0};
   double v[4] = {S::rows(a, g.x, epi), 0.0, 0.0, 0.0};
   v[1] = epi.bb;
-  if (reduce4_last<kBlock>(g.red, v, smem) && threadIdx.x == 0) {
-    MixedState &st = *g.st;
-    if (FIRST) {
-      st.bb = v[1];
-      st.outer = 0;
-      st.inner_total = 0;
-      st.status = HPCCG_OK;
-    }
-    const double rr = v[0];
-    st.rr64 = rr;
-    st.relres = st.bb > 0.0 ? sqrt(rr / st.bb) : 0.0;
-    int cont = (st.relres > st.rel_tol) && (st.outer < st.max_outer);
-    if (!isfinite(st.relres)) {
-      st.status = HPCCG_ERR_BREAKDOWN;
-      cont = 0;
-    }
-    if (cont) {
-      st.scale = sqrt(rr);
-      st.target = st.inner_rtol > 0.0 ? st.inner_rtol : fmax(st.inner_floor, 0.5 * st.rel_tol / st.relres);
-      st.outer += 1;
-    }
-    set_outer(g, cont);
-  }
+  if (reduce4_last<kBlock>(g.red, v, smem) && threadIdx.x == 0) residual_decision<FIRST>(g, v);
+}
+
+// The same with x streamed by TMA (stencil_rows_tma64box; t: 32 x 64 tiles).
+template <bool FIRST>
+__global__ void __launch_bounds__(kBlock, 2) k_mp_residual_tma(MixedArgs g, TmaTile t,
+                                                               const __grid_constant__ CUtensorMap xmap) {
+  __shared__ double smem[4 * 32];
+  EpiResidualF4<FIRST> epi{g.b, g.r, 0.0};
+  double v[4] = {stencil_rows_tma64box(t, &xmap, epi, &g.st->status), 0.0, 0.0, 0.0};
+  v[1] = epi.bb;
+  if (reduce4_last<kBlock>(g.red, v, smem) && threadIdx.x == 0) residual_decision<FIRST>(g, v);
 }
 
 // Start of an inner solve of the fused iteration: scalar state only (the
@@ -444,7 +484,10 @@ __global__ void __launch_bounds__(kBlock) k_spmv_lp_tma(TmaTile t, const __grid_
 static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 static std::mutex g_encode_mu;
 
-int make_stencil_tmap(CUtensorMap *map, const float *base, int nx, int ny, int nz, int box_y, int box_x) {
+// A 3D tensor map over a grid vector of `esize`-byte elements, box box_x x box_y x 1;
+// out-of-grid elements of a box read as zeros.
+static int encode_grid_tmap(CUtensorMap *map, CUtensorMapDataType type, int esize, const void *base, int nx, int ny,
+                            int nz, int box_x, int box_y) {
   {
     std::lock_guard<std::mutex> lk(g_encode_mu);
     if (!g_encode) {
@@ -457,15 +500,25 @@ int make_stencil_tmap(CUtensorMap *map, const float *base, int nx, int ny, int n
       g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
     }
   }
-  if ((reinterpret_cast<uintptr_t>(base) & 15) || nx % 4) return HPCCG_ERR_UNSUPPORTED;
+  // 16-byte base, row and plane strides; 16-byte inner box extent
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || ((int64_t)nx * esize) % 16 || ((int64_t)box_x * esize) % 16)
+    return HPCCG_ERR_UNSUPPORTED;
   const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
-  const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)nx * ny * 4};
+  const cuuint64_t strides[2] = {(cuuint64_t)nx * esize, (cuuint64_t)nx * ny * esize};
   const cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_y, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
-  const CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims, strides, box,
-                              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+  const CUresult r = g_encode(map, type, 3, const_cast<void *>(base), dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? HPCCG_OK : HPCCG_ERR_UNSUPPORTED;
+}
+
+int make_stencil_tmap(CUtensorMap *map, const float *base, int nx, int ny, int nz, int box_y, int box_x) {
+  return encode_grid_tmap(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, nx, ny, nz, box_x, box_y);
+}
+
+int make_stencil_tmap64(CUtensorMap *map, const double *base, int nx, int ny, int nz, int box_x, int box_y) {
+  return encode_grid_tmap(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, base, nx, ny, nz, box_x, box_y);
 }
 
 // Plan of the TMA SpMV for a context (nzc = 0: not usable).
@@ -504,6 +557,21 @@ static TmaTile iter_plan(const hpccg_ctx *c) {
   const PlaneMap q = boxw_map(4, c->gx, c->gy, c->gz, (int64_t)c->num_sms * StratStencilBox64::kMinBlocks * kBlock);
   if (q.plane <= 0 || plane_grid(q) > kItMaxGrid) return none;
   return tma_tile_grid(t) <= kItMaxGrid ? t : none;
+}
+
+// Plan of the TMA refinement residual (nzc = 0: not usable): 32 x 64 tiles,
+// two CTAs per SM in one wave.
+static TmaTile residual_plan(const hpccg_ctx *c) {
+  if (cudaFuncSetAttribute(k_mp_residual_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kB64RingBytes) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_mp_residual_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kB64RingBytes) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return TmaTile{c->gx, c->gy, c->gz, 0, 0, 0, 0};
+  }
+  TmaTile t = tma_tile_plan(c->gx, c->gy, c->gz, 2 * c->num_sms, kB64TileX, kB64TileY);
+  if (tma_tile_grid(t) > kItMaxGrid) t.nzc = 0;  // four partials per CTA
+  return t;
 }
 
 __global__ void k_to_lp(const double *src, float *f32, __nv_bfloat16 *b16, size_t count) {
@@ -558,6 +626,10 @@ struct MixedRes {
   CUtensorMap itmap[5];  // p0, p1, r0, r1 and d
   TmaTile itile{};
   bool iter = false;
+  // the FP64 refinement residual of the fused iteration with x by TMA
+  CUtensorMap xmap64;
+  TmaTile rtile{};
+  bool res_tma = false;
   bool exec_fused[3] = {false, false, false};
 };
 
@@ -666,6 +738,9 @@ static int mixed_res(hpccg_ctx *c, int precision, MixedRes **out) {
                 make_stencil_tmap(&m->itmap[3], m->r2, c->gx, c->gy, c->gz, kItRBoxY, kItBoxX) == HPCCG_OK &&
                 make_stencil_tmap(&m->itmap[4], m->d, c->gx, c->gy, c->gz, kItTileY, kItTileX) == HPCCG_OK;
     }
+    m->rtile = residual_plan(c);
+    m->res_tma = m->rtile.nzc > 0 && make_stencil_tmap64(&m->xmap64, c->d_x, c->gx, c->gy, c->gz, kB64BoxX,
+                                                         kB64BoxY) == HPCCG_OK;
     m->tma_gx = c->gx;
   }
   *out = m;
@@ -726,7 +801,14 @@ static int launch_inner_body(hpccg_ctx *c, MixedRes *m, int precision, const Mix
 }
 
 // The refinement residual of the fused iteration (FIRST: also b.b).
-static int launch_residual_f(hpccg_ctx *c, const MixedArgs &g, cudaStream_t s, bool first) {
+static int launch_residual_f(hpccg_ctx *c, const MixedRes *m, const MixedArgs &g, cudaStream_t s, bool first) {
+  if (m->res_tma && g.x == c->d_x) {
+    if (first)
+      k_mp_residual_tma<true><<<tma_tile_grid(m->rtile), kBlock, kB64RingBytes, s>>>(g, m->rtile, m->xmap64);
+    else
+      k_mp_residual_tma<false><<<tma_tile_grid(m->rtile), kBlock, kB64RingBytes, s>>>(g, m->rtile, m->xmap64);
+    return (int)cudaGetLastError();
+  }
   SpmvArgs a = spmv_args(c);
   auto go = [&](auto strat) {
     using St = decltype(strat);
@@ -813,7 +895,7 @@ static int build_mixed_graph(hpccg_ctx *c, MixedRes *m, int precision) {
   const bool fused = use_iter(c, m);
   if (e == cudaSuccess) {
     if (fused) {
-      e = (cudaError_t)launch_residual_f(c, ga, s, true);
+      e = (cudaError_t)launch_residual_f(c, m, ga, s, true);
     } else {
       k_mp_bnorm<<<c->grid, kBlock, 0, s>>>(ga);
       e = (cudaError_t)launch_residual64(c, ga, s);
@@ -840,7 +922,7 @@ static int build_mixed_graph(hpccg_ctx *c, MixedRes *m, int precision) {
         ee = cudaGetLastError();
       }
       if (ee == cudaSuccess)
-        ee = (cudaError_t)(fused ? launch_residual_f(c, gi, os, false) : launch_residual64(c, gi, os));
+        ee = (cudaError_t)(fused ? launch_residual_f(c, m, gi, os, false) : launch_residual64(c, gi, os));
       return ee;
     });
   cudaGraph_t out = nullptr;
@@ -864,7 +946,7 @@ static int run_mixed_eager(hpccg_ctx *c, MixedRes *m, int precision) {
   const bool fused = use_iter(c, m);
   int rc;
   if (fused) {
-    rc = launch_residual_f(c, g, c->stream, true);
+    rc = launch_residual_f(c, m, g, c->stream, true);
   } else {
     k_mp_bnorm<<<c->grid, kBlock, 0, c->stream>>>(g);
     rc = launch_residual64(c, g, c->stream);
@@ -888,7 +970,7 @@ static int run_mixed_eager(hpccg_ctx *c, MixedRes *m, int precision) {
       if (rc) return set_cuda_error((cudaError_t)rc, "inner", __FILE__, __LINE__);
     }
     k_mp_end_inner<<<c->grid, kBlock, 0, c->stream>>>(g);
-    rc = fused ? launch_residual_f(c, g, c->stream, false) : launch_residual64(c, g, c->stream);
+    rc = fused ? launch_residual_f(c, m, g, c->stream, false) : launch_residual64(c, g, c->stream);
     if (rc) return set_cuda_error((cudaError_t)rc, "residual64", __FILE__, __LINE__);
   }
   return HPCCG_OK;

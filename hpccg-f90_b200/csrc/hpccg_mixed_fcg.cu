@@ -51,7 +51,7 @@ struct MfcgArgs {
 
 // FP64 r = b - A x and r.r with the context's FP64 strategy.
 template <class S>
-__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mfcg_residual(SpmvArgs a, MfcgArgs g) {
+__global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mfcg_residual(const __grid_constant__ SpmvArgs a, MfcgArgs g) {
   __shared__ double smem[32];
   EpiResidual epi{g.b, g.r64};
   const double part = S::rows(a, g.x, epi);

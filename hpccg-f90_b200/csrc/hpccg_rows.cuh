@@ -20,6 +20,14 @@
 #pragma once
 #include "hpccg_internal.cuh"
 #include "hpccg_stencil.cuh"
+#include "hpccg_stencil_tma64.cuh"
+
+// z planes per block of the FP64 tile map: at most this many while the grid
+// gives every SM four blocks or more, down to 8 on small grids; more when the
+// blocks would exceed the reduction scratch.
+#ifndef HPCCG_TILE_ZC
+#define HPCCG_TILE_ZC 16
+#endif
 
 namespace hpccg {
 
@@ -31,6 +39,15 @@ __device__ __forceinline__ double mul_add(double s, double v, double x) {
 // it is in use (hpccg_stencil.cuh), else grid-stride rows.
 template <class Body>
 __device__ __forceinline__ void thread_rows(int n, const PlaneMap &m, Body &&body) {
+  if (m.tiles_x > 0) {  // the column pair of a tile, the order of stencil_rows_tma64ref
+    const TileSpan sp = tile_span(m, n / m.plane);
+    if (!sp.rows) return;
+    for (int z = sp.z0; z < sp.z1; ++z) {
+      body(sp.c + z * m.plane);
+      body(sp.c + m.nx + z * m.plane);
+    }
+    return;
+  }
   if (m.plane > 0) {
     const PlaneSpan sp = plane_span(m, n / m.plane);
     if (m.ry == 2) {  // the column pair (x, y), (x, y+1), the order of stencil_column2
@@ -185,6 +202,14 @@ struct SpmvArgs {
   const double *val, *ell_val;
   StencilGeom geom;  // grid of generate_matrix (STENCIL only)
   PlaneMap pm;       // row map of ELL (one row per thread) and STENCIL when the grid is known
+  // STENCIL under the tile map: tensor maps of the two vectors tma_vec[0..1],
+  // whose SpMVs read x by TMA (tma_ok); other vectors use plain loads.  The
+  // kernels take SpmvArgs as a __grid_constant__ parameter, so the TMA reads
+  // the maps from parameter space.
+  CUtensorMap tmap[2];
+  const double *tma_vec[2];
+  int tma_ok;
+  int *status;  // where a TMA walk records HPCCG_ERR_TIMEOUT
 };
 
 // Launch grid of a strategy that follows the plane map when it is in use.
@@ -235,11 +260,21 @@ struct StratCsr {
 };
 
 struct StratStencil {
-  static constexpr int kMinBlocks = 3;
+  static constexpr int kMinBlocks = 4;
   static int grid(const SpmvArgs &a, int dflt) { return plane_or(a.pm, dflt); }
   template <class Epi>
   static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
     return stencil_rows<double>(a.n, a.geom, a.pm, x, e);
+  }
+};
+// The same rows and sums with x streamed by TMA (tile map; the host selects it
+// only for x = tma_vec[0] or tma_vec[1], whose tensor maps a.tmap holds).
+struct StratStencilTma {
+  static constexpr int kMinBlocks = 4;
+  static int grid(const SpmvArgs &a, int dflt) { return plane_or(a.pm, dflt); }
+  template <class Epi>
+  static __device__ __forceinline__ double rows(const SpmvArgs &a, const double *x, Epi &e) {
+    return stencil_rows_tma64ref(a.geom, a.pm, &a.tmap[x == a.tma_vec[0] ? 0 : 1], e, a.status);
   }
 };
 
@@ -258,10 +293,14 @@ struct StratStencilBox64 {
 // hpccg_gpu_set_spmv for HPCCG_SPMV_ELL / HPCCG_SPMV_ELL2).
 constexpr int kEllMinBlocks[4] = {2, 3, 4, 8};
 
-// Calls f(Strat{}) with the strategy the arguments select (host side).
+// Calls f(Strat{}) with the strategy the arguments select (host side); x, the
+// vector the SpMV reads, selects the TMA walk when its tensor map exists.
 template <class F>
-inline int dispatch_strategy(const SpmvArgs &a, F &&f) {
-  if (a.kind == HPCCG_SPMV_STENCIL) return f(StratStencil{});
+inline int dispatch_strategy(const SpmvArgs &a, F &&f, const double *x = nullptr) {
+  if (a.kind == HPCCG_SPMV_STENCIL) {
+    if (x && a.tma_ok && a.pm.tiles_x > 0 && (x == a.tma_vec[0] || x == a.tma_vec[1])) return f(StratStencilTma{});
+    return f(StratStencil{});
+  }
   if (a.kind == HPCCG_SPMV_CSR_VECTOR) {
     switch (a.param) {
       case 4: return f(StratCsr<4>{});
@@ -287,6 +326,20 @@ inline int dispatch_strategy(const SpmvArgs &a, F &&f) {
   }
 }
 
+// Row map of the FP64 kernels of a context whose grid is known: the tile map
+// when nx and ny are even (nx even: the TMA walk's tensor map), else the
+// two-line plane map.
+inline PlaneMap fp64_map(int nx, int ny, int nz, int num_sms) {
+  if (nx % 2 == 0) {
+    int zc = HPCCG_TILE_ZC;
+    const int64_t per_plane = (int64_t)((nx + kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY);
+    while (zc > 8 && per_plane * ((nz + zc - 1) / zc) < 4 * (int64_t)num_sms) zc /= 2;
+    const PlaneMap t = tile_map(nx, ny, nz, kMaxPartials, zc);
+    if (t.plane > 0) return t;
+  }
+  return plane_map(nx, ny, nz, kMaxPartials, 2);
+}
+
 inline SpmvArgs spmv_args(const hpccg_ctx *c) {
   SpmvArgs a;
   a.kind = c->spmv_kind == HPCCG_SPMV_AUTO ? HPCCG_SPMV_ELL : c->spmv_kind;
@@ -305,7 +358,15 @@ inline SpmvArgs spmv_args(const hpccg_ctx *c) {
   a.ell_col = c->d_ell_col;
   a.ell_val = c->d_ell_val;
   a.geom = StencilGeom{c->gx, c->gy, c->gz};
-  a.pm = c->gx ? plane_map(c->gx, c->gy, c->gz, kMaxPartials, 2) : PlaneMap{0, 0, 0, 1, 1, 0};
+  a.pm = c->gx ? fp64_map(c->gx, c->gy, c->gz, c->num_sms) : PlaneMap{0, 0, 0, 1, 1, 0};
+  a.tma_ok = a.pm.tiles_x > 0 && c->tmaps_ok;
+  if (a.tma_ok) {
+    a.tmap[0] = c->tmaps[0];
+    a.tmap[1] = c->tmaps[1];
+  }
+  a.tma_vec[0] = c->d_p;
+  a.tma_vec[1] = c->d_x;
+  a.status = &c->d_state->status;
   return a;
 }
 

@@ -20,8 +20,11 @@
 // use the two-line form (ry = 2): thread t owns the columns (x, y) and
 // (x, y+1) of an even line y, so twelve loads a plane serve two rows (6 a
 // row); at 256^3 the matrix-free FP64 SpMV went 0.109 -> 0.095 ms with it.
-// The ELL kernel uses the same map for the same context, so fused dot
-// products -- and whole CG runs -- are bit-identical between the two.
+// With nx and ny even the FP64 kernels use the tile map below instead (32 x
+// 16 columns a block, the same column pairs), whose rectangles a TMA box can
+// feed (hpccg_stencil_tma64.cuh).  The ELL kernel uses the same map for the
+// same context, so fused dot products -- and whole CG runs -- are
+// bit-identical between the two.
 #pragma once
 #include <algorithm>
 
@@ -40,7 +43,16 @@ struct PlaneMap {
   int cols;   // consecutive grid columns per thread (0 or 1: one; 4: the FP32 box walk)
   int ry;     // plane map: grid lines per thread (0 or 1: one; 2: lines y and y+1, y even)
   int nx;     // plane map with ry = 2: the grid's nx
+  int tiles_x, tiles_y;  // > 0: tile map (below), tiles per plane
 };
+
+// Tile map of the FP64 walks (ry = 2): block b owns the kTileX x kTileY
+// columns of tile b mod (tiles_x*tiles_y) and planes [q*zc, (q+1)*zc) of
+// chunk q = b div (tiles_x*tiles_y); thread t owns column x = x0 + t mod
+// kTileX of the even line y = y0 + 2 (t div kTileX) and of line y+1.  A warp
+// is one 32-column line pair, so loads stay coalesced, and a block's columns
+// form the rectangle that one TMA box (plus halo) covers.
+constexpr int kTileX = 32, kTileY = 2 * (kBlock / kTileX);
 
 // Host: the plane map for a grid, with at most `max_blocks` blocks of kBlock
 // threads (the reduction scratch holds one partial per block).  Chunks of at
@@ -63,11 +75,33 @@ inline PlaneMap plane_map(int nx, int ny, int nz, int max_blocks, int ry_max = 1
     if (zc >= nz) return m;  // one plane alone needs too many threads
   }
 }
+// Host: the tile map for a grid with an even ny, z chunks of zc planes (more
+// when the blocks would outnumber max_blocks); plane = 0 when no tile map fits.
+inline PlaneMap tile_map(int nx, int ny, int nz, int max_blocks, int zc) {
+  PlaneMap m{0, 0, 0, 1, 1, nx, 0, 0};
+  if (nx < 1 || ny < 2 || ny % 2 || nz < 1 || zc < 1) return m;
+  const int64_t tx = (nx + kTileX - 1) / kTileX, ty = (ny + kTileY - 1) / kTileY;
+  for (zc = std::min(zc, nz);; zc = std::min(2 * zc, nz)) {
+    const int64_t nzc = (nz + zc - 1) / zc;
+    if (tx * ty * nzc <= max_blocks) {
+      m.plane = nx * ny;
+      m.zc = zc;
+      m.nzc = (int)nzc;
+      m.ry = 2;
+      m.tiles_x = (int)tx;
+      m.tiles_y = (int)ty;
+      return m;
+    }
+    if (zc >= nz) return m;
+  }
+}
+
 // Threads of one z chunk: one per column (or column group), or per column pair in y.
 __host__ __device__ __forceinline__ int64_t plane_threads(const PlaneMap &m) {
   return m.ry == 2 ? m.plane / 2 : m.plane;
 }
 inline int plane_grid(const PlaneMap &m) {
+  if (m.tiles_x > 0) return m.tiles_x * m.tiles_y * m.nzc;
   return (int)((plane_threads(m) * m.nzc + kBlock - 1) / kBlock);
 }
 
@@ -84,6 +118,27 @@ __device__ __forceinline__ PlaneSpan plane_span(const PlaneMap &m, int nz) {
   const int u = (int)(t - (int64_t)q * tpc);
   // ry = 2: consecutive threads own consecutive x of one even line y (and line y+1)
   s.c = m.ry == 2 ? (u / m.nx) * 2 * m.nx + u % m.nx : u;
+  s.z0 = q * m.zc;
+  s.z1 = min(nz, s.z0 + m.zc);
+  return s;
+}
+
+// The calling thread's rows under a tile map: columns c and c + nx (c at an
+// even line y), planes [z0, z1); rows = false for a thread whose column lies
+// outside the grid (a partial tile at the x or y face).  x0, y0: the tile.
+struct TileSpan {
+  int c, z0, z1, x0, y0;
+  bool rows;
+};
+__device__ __forceinline__ TileSpan tile_span(const PlaneMap &m, int nz) {
+  TileSpan s;
+  const int per = m.tiles_x * m.tiles_y;
+  const int q = blockIdx.x / per, tile = blockIdx.x - q * per;
+  s.x0 = (tile % m.tiles_x) * kTileX;
+  s.y0 = (tile / m.tiles_x) * kTileY;
+  const int x = s.x0 + (int)threadIdx.x % kTileX, y = s.y0 + 2 * ((int)threadIdx.x / kTileX);
+  s.rows = x < m.nx && y < m.plane / m.nx;  // ny even: line y+1 is inside too
+  s.c = y * m.nx + x;
   s.z0 = q * m.zc;
   s.z1 = min(nz, s.z0 + m.zc);
   return s;
@@ -189,6 +244,32 @@ __device__ __forceinline__ Real stencil_lead(const Real *a) {
       s = __dsub_rn(s, a[j]);
     else
       s -= a[j];
+  }
+  return s;
+}
+// The tail split at the plane boundary: mid = s followed by the nine terms of
+// plane z (27 x_i at the centre), end = s followed by those of plane z+1;
+// stencil_end(stencil_mid(s, b), c) is stencil_tail(s, b, c), operation for
+// operation.
+template <typename Real>
+__device__ __forceinline__ Real stencil_mid(Real s, const Real *b) {
+  if constexpr (sizeof(Real) == 8) {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s = j == 4 ? __dadd_rn(s, __dmul_rn(27.0, b[j])) : __dsub_rn(s, b[j]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s = j == 4 ? fmaf(27.f, b[j], s) : s - b[j];
+  }
+  return s;
+}
+template <typename Real>
+__device__ __forceinline__ Real stencil_end(Real s, const Real *c) {
+  if constexpr (sizeof(Real) == 8) {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s = __dsub_rn(s, c[j]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s -= c[j];
   }
   return s;
 }
@@ -518,32 +599,61 @@ __device__ __forceinline__ unsigned stencil_mask4(const StencilGeom &g, int ix, 
 }
 // The z walk of a column pair (x, y) and (x, y+1): per plane twelve loads serve
 // both rows (nine a row otherwise).  Each row's sum is the single-line walk's,
-// term for term: lead (plane z-1) then planes z and z+1, lines in sy order;
-// row y's lines are v[0..8], row y+1's v[3..11].  Rows go to epi in the order
-// (z, y), (z, y+1), z ascending -- the order thread_rows gives the ELL kernels.
+// term for term: plane z-1 (lead), plane z (mid), plane z+1 (end), lines in sy
+// order; row y's lines are v[0..8], row y+1's v[3..11].  The three pieces are
+// pipelined across planes (ColumnPair2): when plane z+1 arrives it ends the
+// rows of plane z, takes the rows of plane z+1 through their mid and starts
+// the leads of plane z+2 -- six independent 9-term chains a step instead of
+// two 18-term ones, and one plane of values held instead of two.  Rows go to
+// epi in the order (z, y), (z, y+1), z ascending -- the order thread_rows
+// gives the ELL kernels.
+template <typename Real>
+struct ColumnPair2 {
+  Real lead0, lead1;  // rows of the next plane: their first nine terms
+  Real mid0, mid1;    // rows of the current plane: through their plane's terms
+  Real x0, x1;        // x of the current plane's two rows
+  // plane z-1 of the walk's first row
+  __device__ __forceinline__ void first(const Real *v) {
+    lead0 = stencil_lead<Real>(v);
+    lead1 = stencil_lead<Real>(v + 3);
+  }
+  // plane p: the rows of plane p through their mid, the leads of plane p+1
+  __device__ __forceinline__ void middle(const Real *v) {
+    mid0 = stencil_mid<Real>(lead0, v);
+    mid1 = stencil_mid<Real>(lead1, v + 3);
+    x0 = v[4];
+    x1 = v[7];
+    lead0 = stencil_lead<Real>(v);
+    lead1 = stencil_lead<Real>(v + 3);
+  }
+  // plane p+1 ends the rows of plane p: s0, s1 (then middle(v) moves on)
+  __device__ __forceinline__ void end(const Real *v, Real &s0, Real &s1) const {
+    s0 = stencil_end<Real>(mid0, v);
+    s1 = stencil_end<Real>(mid1, v + 3);
+  }
+};
 template <typename Real, bool FULL, class Epi>
 __device__ __forceinline__ double stencil_column2(const PlaneSpan &sp, const StencilGeom &g, const PlaneMap &m,
                                                   unsigned mask, const Real *__restrict__ pc, Epi &epi) {
   double part = 0.0;
-  Real b[12], c[12];
-  stencil_plane4<Real, FULL>(pc + (int64_t)(sp.z0 - 1) * m.plane, g.nx, mask, sp.z0 > 0, c);
-  Real lead0 = stencil_lead<Real>(c), lead1 = stencil_lead<Real>(c + 3);
-  stencil_plane4<Real, FULL>(pc + (int64_t)sp.z0 * m.plane, g.nx, mask, true, b);
+  Real v[12];
+  ColumnPair2<Real> w;
+  stencil_plane4<Real, FULL>(pc + (int64_t)(sp.z0 - 1) * m.plane, g.nx, mask, sp.z0 > 0, v);
+  w.first(v);
+  stencil_plane4<Real, FULL>(pc + (int64_t)sp.z0 * m.plane, g.nx, mask, true, v);
+  w.middle(v);
   for (int z = sp.z0; z < sp.z1; ++z) {
-    stencil_plane4<Real, FULL>(pc + (int64_t)(z + 1) * m.plane, g.nx, mask, z + 1 < g.nz, c);
-    const Real s0 = stencil_tail<Real>(lead0, b, c);
-    const Real s1 = stencil_tail<Real>(lead1, b + 3, c + 3);
+    stencil_plane4<Real, FULL>(pc + (int64_t)(z + 1) * m.plane, g.nx, mask, z + 1 < g.nz, v);
+    Real s0, s1;
+    w.end(v, s0, s1);
     if constexpr (sizeof(Real) == 8) {
-      part = __dadd_rn(part, epi(sp.c + z * m.plane, s0, b[4]));
-      part = __dadd_rn(part, epi(sp.c + g.nx + z * m.plane, s1, b[7]));
+      part = __dadd_rn(part, epi(sp.c + z * m.plane, s0, w.x0));
+      part = __dadd_rn(part, epi(sp.c + g.nx + z * m.plane, s1, w.x1));
     } else {
-      part += epi(sp.c + z * m.plane, s0, b[4]);
-      part += epi(sp.c + g.nx + z * m.plane, s1, b[7]);
+      part += epi(sp.c + z * m.plane, s0, w.x0);
+      part += epi(sp.c + g.nx + z * m.plane, s1, w.x1);
     }
-    lead0 = stencil_lead<Real>(b);
-    lead1 = stencil_lead<Real>(b + 3);
-#pragma unroll
-    for (int j = 0; j < 12; ++j) b[j] = c[j];
+    w.middle(v);
   }
   return part;
 }
@@ -554,7 +664,14 @@ __device__ __forceinline__ double stencil_rows(int n, const StencilGeom &g, cons
                                                const Real *__restrict__ x, Epi &epi) {
   double part = 0.0;
   if (m.plane > 0) {
-    const PlaneSpan sp = plane_span(m, g.nz);
+    PlaneSpan sp;
+    if (m.tiles_x > 0) {
+      const TileSpan ts = tile_span(m, g.nz);
+      if (!ts.rows) return part;
+      sp = PlaneSpan{ts.c, ts.z0, ts.z1};
+    } else {
+      sp = plane_span(m, g.nz);
+    }
     if (sp.z0 >= sp.z1) return part;
     const int iy = sp.c / g.nx, ix = sp.c - iy * g.nx;
     if (m.ry == 2) {
