@@ -50,6 +50,7 @@ struct MixedArgs {
   PlaneMap pm;
   cudaGraphConditionalHandle cond_outer, cond_inner;
   int use_cond;
+  int skip_done;  // fused pass: return at once when the inner solve has ended
 };
 
 __device__ __forceinline__ void set_outer(const MixedArgs &g, int v) {
@@ -125,15 +126,14 @@ struct EpiResidualF {
   }
   __device__ __forceinline__ double operator()(int i, double s, double) { return (*this)(i, s); }
 };
-// Four rows at once (i a multiple of 4): b by two 16-byte loads, r by one.
+// Four rows at once (i a multiple of 4): b from shared memory, r by one 16-byte store.
 template <bool FIRST>
 struct EpiResidualF4 {
-  const double *b;
   float *r;
   double bb;
-  __device__ __forceinline__ double store4(int i, const double y[4]) {
-    const double2 b01 = __ldcs(reinterpret_cast<const double2 *>(b + i));
-    const double2 b23 = __ldcs(reinterpret_cast<const double2 *>(b + i) + 1);
+  __device__ __forceinline__ double store4(int i, const double y[4], const double *b4) {
+    const double2 b01 = *reinterpret_cast<const double2 *>(b4);
+    const double2 b23 = *reinterpret_cast<const double2 *>(b4 + 2);
     const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
     float4 ro;
     double rr = 0.0;
@@ -188,10 +188,11 @@ __global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_residual_f(const _
 // The same with x streamed by TMA (stencil_rows_tma64box; t: 32 x 64 tiles).
 template <bool FIRST>
 __global__ void __launch_bounds__(kBlock, 2) k_mp_residual_tma(MixedArgs g, TmaTile t,
-                                                               const __grid_constant__ CUtensorMap xmap) {
+                                                               const __grid_constant__ CUtensorMap xmap,
+                                                               const __grid_constant__ CUtensorMap bmap) {
   __shared__ double smem[4 * 32];
-  EpiResidualF4<FIRST> epi{g.b, g.r, 0.0};
-  double v[4] = {stencil_rows_tma64box(t, &xmap, epi, &g.st->status), 0.0, 0.0, 0.0};
+  EpiResidualF4<FIRST> epi{g.r, 0.0};
+  double v[4] = {stencil_rows_tma64box(t, &xmap, &bmap, epi, &g.st->status), 0.0, 0.0, 0.0};
   v[1] = epi.bb;
   if (reduce4_last<kBlock>(g.red, v, smem) && threadIdx.x == 0) residual_decision<FIRST>(g, v);
 }
@@ -413,6 +414,9 @@ __global__ void __launch_bounds__(kItBlock, 1) k_mp_iter_tma(MixedArgs g, TmaTil
                                                           const __grid_constant__ CUtensorMap dm) {
   __shared__ double smem[4 * 32];
   MixedState *st = g.st;
+  // a pass of an unrolled loop body after the inner solve has ended does nothing
+  // (cont_inner changes only in the last block of a pass, after every block has read it)
+  if (g.skip_done && !st->cont_inner) return;
   const int par = st->passes & 1;
   const bool first = st->passes == 0;
   IterScalars sc;
@@ -626,8 +630,8 @@ struct MixedRes {
   CUtensorMap itmap[5];  // p0, p1, r0, r1 and d
   TmaTile itile{};
   bool iter = false;
-  // the FP64 refinement residual of the fused iteration with x by TMA
-  CUtensorMap xmap64;
+  // the FP64 refinement residual of the fused iteration with x and b by TMA
+  CUtensorMap xmap64, bmap64;
   TmaTile rtile{};
   bool res_tma = false;
   bool exec_fused[3] = {false, false, false};
@@ -739,8 +743,9 @@ static int mixed_res(hpccg_ctx *c, int precision, MixedRes **out) {
                 make_stencil_tmap(&m->itmap[4], m->d, c->gx, c->gy, c->gz, kItTileY, kItTileX) == HPCCG_OK;
     }
     m->rtile = residual_plan(c);
-    m->res_tma = m->rtile.nzc > 0 && make_stencil_tmap64(&m->xmap64, c->d_x, c->gx, c->gy, c->gz, kB64BoxX,
-                                                         kB64BoxY) == HPCCG_OK;
+    m->res_tma = m->rtile.nzc > 0 &&
+                 make_stencil_tmap64(&m->xmap64, c->d_x, c->gx, c->gy, c->gz, kB64BoxX, kB64BoxY) == HPCCG_OK &&
+                 make_stencil_tmap64(&m->bmap64, c->d_b, c->gx, c->gy, c->gz, kB64TileX, kB64TileY) == HPCCG_OK;
     m->tma_gx = c->gx;
   }
   *out = m;
@@ -778,9 +783,18 @@ static MixedArgs mixed_args(hpccg_ctx *c, MixedRes *m, int precision) {
   return g;
 }
 
+// Fused passes per inner-loop body: the while node's per-iteration cost is paid
+// once per kInnerUnroll passes; passes after the solve has ended return at once.
+#ifndef HPCCG_INNER_UNROLL
+#define HPCCG_INNER_UNROLL 4
+#endif
+constexpr int kInnerUnroll = HPCCG_INNER_UNROLL;
+
 static int launch_inner_body(hpccg_ctx *c, MixedRes *m, int precision, const MixedArgs &g, cudaStream_t s) {
   if (use_iter(c, m)) {
-    launch_iter(c, m, g, s);
+    MixedArgs gs = g;
+    gs.skip_done = 1;
+    for (int k = 0; k < kInnerUnroll; ++k) launch_iter(c, m, k ? gs : g, s);
     return (int)cudaGetLastError();
   }
   k_mp_update_p<<<c->grid, kBlock, 0, s>>>(g);
@@ -802,11 +816,12 @@ static int launch_inner_body(hpccg_ctx *c, MixedRes *m, int precision, const Mix
 
 // The refinement residual of the fused iteration (FIRST: also b.b).
 static int launch_residual_f(hpccg_ctx *c, const MixedRes *m, const MixedArgs &g, cudaStream_t s, bool first) {
-  if (m->res_tma && g.x == c->d_x) {
+  if (m->res_tma && g.x == c->d_x && g.b == c->d_b) {
+    const int grid = tma_tile_grid(m->rtile);
     if (first)
-      k_mp_residual_tma<true><<<tma_tile_grid(m->rtile), kBlock, kB64RingBytes, s>>>(g, m->rtile, m->xmap64);
+      k_mp_residual_tma<true><<<grid, kBlock, kB64RingBytes, s>>>(g, m->rtile, m->xmap64, m->bmap64);
     else
-      k_mp_residual_tma<false><<<tma_tile_grid(m->rtile), kBlock, kB64RingBytes, s>>>(g, m->rtile, m->xmap64);
+      k_mp_residual_tma<false><<<grid, kBlock, kB64RingBytes, s>>>(g, m->rtile, m->xmap64, m->bmap64);
     return (int)cudaGetLastError();
   }
   SpmvArgs a = spmv_args(c);

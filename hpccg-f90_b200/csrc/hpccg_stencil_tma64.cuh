@@ -13,7 +13,7 @@
 //    the reassociated FP64 sum of stencil_rows_box64x4 (3-point line sums, 3x3
 //    box sums, y = 28 x - (box(z-1) + box(z) + box(z+1))), the same value bit
 //    for bit up to the sign of a zero.  The refinement residual of the mixed
-//    solvers.
+//    solvers; b arrives by TMA in the same slots.
 //  * stencil_rows_tma64ref: 32 x 16 columns per CTA, the column pair (x, y),
 //    (x, y+1) of an even line y a thread, the reference's term order
 //    (stencil_column2), so the row sums are bit-identical to the ELL kernels'.
@@ -37,6 +37,8 @@ int make_stencil_tmap64(CUtensorMap *map, const double *base, int nx, int ny, in
 // A ring of STAGES shared-memory slots, each receiving one z plane of the
 // CTA's box.  Planes lo .. hi load in order; thread 0 issues them, STAGES
 // ahead of the plane being read.
+// A slot can also take a companion box: plane p + 1 of map2 for p + 1 in
+// [lo2, hi2], at byte offset off2 of the slot (the same mbarrier covers both).
 template <int STAGES>
 struct PlaneRing {
   unsigned char *slots;
@@ -48,14 +50,19 @@ struct PlaneRing {
   int lo, hi;
   int next;      // thread 0: the next plane to issue
   int consumed;  // the last plane every thread has released
+  const CUtensorMap *map2 = nullptr;
+  int bx2 = 0, by2 = 0, off2 = 0, lo2 = 0, hi2 = -1;
+  uint32_t bytes2 = 0;
 
   __device__ __forceinline__ int slot(int p) const { return (p - lo) % STAGES; }
   __device__ __forceinline__ uint32_t parity(int p) const { return (uint32_t)((p - lo) / STAGES) & 1u; }
   __device__ __forceinline__ const unsigned char *data(int p) const { return slots + (size_t)slot(p) * slot_bytes; }
   __device__ __forceinline__ void issue() {  // thread 0
     const int k = slot(next);
-    tc::mbar_expect_tx(&full[k], bytes);
+    const bool two = map2 && next - 1 >= lo2 && next - 1 <= hi2;
+    tc::mbar_expect_tx(&full[k], bytes + (two ? bytes2 : 0u));
     tma_load_3d(slots + (size_t)k * slot_bytes, map, &full[k], bx, by, next);
+    if (two) tma_load_3d(slots + (size_t)k * slot_bytes + off2, map2, &full[k], bx2, by2, next - 1);
     ++next;
   }
   // Thread 0 initialises the barriers; a CTA barrier must follow, then prime().
@@ -103,17 +110,21 @@ constexpr int kB64TileX = 32, kB64TileY = 64;                  // columns per CT
 constexpr int kB64BoxX = kB64TileX + 4;                        // x0-2 .. x0+33
 constexpr int kB64BoxY = kB64TileY + 2;                        // y0-1 .. y0+64
 constexpr uint32_t kB64BoxBytes = kB64BoxX * kB64BoxY * 8;     // 19008
-constexpr int kB64Slot = ((kB64BoxBytes + 127) / 128) * 128;   // 19072
-constexpr int kB64Stages = 4;
-constexpr int kB64RingBytes = kB64Stages * kB64Slot;           // dynamic shared memory
+constexpr int kB64XSlot = ((kB64BoxBytes + 127) / 128) * 128;  // 19072
+constexpr uint32_t kB64TileBytes = kB64TileX * kB64TileY * 8;   // 16384: the companion tile (b)
+constexpr int kB64Slot = kB64XSlot + kB64TileBytes;             // 35456
+constexpr int kB64Stages = 3;
+constexpr int kB64RingBytes = kB64Stages * kB64Slot;           // dynamic shared memory (two CTAs a SM)
 static_assert(kBlock == (kB64TileX / 4) * (kB64TileY / 2), "one thread per 4 x 2 columns");
 
-// Rows of the calling CTA (tile plan with kB64TileX x kB64TileY tiles);
-// epi.store4(i, y[4]) stores rows i .. i+3 and returns their dot term.  Every
-// thread of the CTA must call it (it has barriers).
+// Rows of the calling CTA (tile plan with kB64TileX x kB64TileY tiles).  With
+// the slot of plane z+1 arrives the tile of plane z of a second vector (bmap,
+// no halo); epi.store4(i, y[4], b4) stores rows i .. i+3 and returns their
+// dot term, b4 = that vector's four values of the rows (shared memory).
+// Every thread of the CTA must call it (it has barriers).
 template <class Epi>
-__device__ __forceinline__ double stencil_rows_tma64box(const TmaTile &t, const CUtensorMap *map, Epi &epi,
-                                                        int *status) {
+__device__ __forceinline__ double stencil_rows_tma64box(const TmaTile &t, const CUtensorMap *map,
+                                                        const CUtensorMap *bmap, Epi &epi, int *status) {
   extern __shared__ __align__(128) unsigned char b64_ring[];  // kB64RingBytes
   __shared__ uint64_t full[kB64Stages];
   double part = 0.0;
@@ -125,6 +136,13 @@ __device__ __forceinline__ double stencil_rows_tma64box(const TmaTile &t, const 
   const int xc = x0 + 4 * tx, yc = y0 + 2 * ty;
   const int64_t plane = (int64_t)t.nx * t.ny;
   PlaneRing<kB64Stages> ring{b64_ring, kB64Slot, full, map, x0 - 2, y0 - 1, kB64BoxBytes, z0 - 1, z1, 0, 0};
+  ring.map2 = bmap;  // b(z) rides with x(z+1), z in [z0, z1)
+  ring.bx2 = x0;
+  ring.by2 = y0;
+  ring.off2 = kB64XSlot;
+  ring.bytes2 = kB64TileBytes;
+  ring.lo2 = z0;
+  ring.hi2 = z1 - 1;
   ring.init();
   __syncthreads();
   ring.prime();
@@ -161,22 +179,29 @@ __device__ __forceinline__ double stencil_rows_tma64box(const TmaTile &t, const 
     if (ring.release(z0, ok)) {
       for (int z = z0; z < z1; ++z) {
         ok = consume(z + 1, bp, vp);
+        if (ok) {  // rows of plane z, before the slot that holds b(z) is released
+          const double *bt = reinterpret_cast<const double *>(ring.data(z + 1) + kB64XSlot) +
+                             (2 * ty) * kB64TileX + 4 * tx;
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            if (xc < t.nx && yc + j < t.ny) {
+              double y[4];
+#pragma unroll
+              for (int i = 0; i < 4; ++i) y[i] = fma(28.0, v0[j][i], -((bm[j][i] + b0[j][i]) + bp[j][i]));
+              part = __dadd_rn(part, epi.store4((int)(z * plane + (int64_t)(yc + j) * t.nx + xc), y,
+                                                bt + j * kB64TileX));
+            }
+          }
+        }
         if (!ring.release(z + 1, ok)) break;
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          if (xc < t.nx && yc + j < t.ny) {
-            double y[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) y[i] = fma(28.0, v0[j][i], -((bm[j][i] + b0[j][i]) + bp[j][i]));
-            part = __dadd_rn(part, epi.store4((int)(z * plane + (int64_t)(yc + j) * t.nx + xc), y));
-          }
+        for (int j = 0; j < 2; ++j)
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             bm[j][i] = b0[j][i];
             b0[j][i] = bp[j][i];
             v0[j][i] = vp[j][i];
           }
-        }
       }
     }
   }
