@@ -374,7 +374,7 @@ class Matrix:
         _check(_lib.hpccg_gpu_set_mixed_rows_per_thread(self._h, precision, rpt), "set_mixed_rows_per_thread")
 
     def time_mixed_kernels(self, precision: int, reps: int = 10):
-        """[p update, SpMV + p.Ap, r update] ms; [0, pass, 0] with the fused iteration."""
+        """[p update, SpMV + p.Ap, r update] ms; [FP64 residual, pass, 0] with the fused iteration."""
         ms = (_c.c_float * 3)()
         _check(_lib.hpccg_gpu_time_mixed_kernels(self._h, precision, reps, ms), "time_mixed_kernels")
         return [ms[0], ms[1], ms[2]]

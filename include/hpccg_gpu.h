@@ -158,8 +158,8 @@ int hpccg_gpu_set_mixed_rows_per_thread(hpccg_ctx *ctx, int32_t precision, int32
 
 /* Average ms of the inner-CG kernels (p update, low-precision SpMV + p.Ap,
  * r update + r.r), each launched `reps` times back to back.  When the inner
- * iteration is one fused pass (hpccg_gpu_mixed_fused), ms[1] is that pass and
- * ms[0] = ms[2] = 0. */
+ * iteration is one fused pass (hpccg_gpu_mixed_fused), ms[1] is that pass,
+ * ms[0] the FP64 refinement residual of an outer cycle and ms[2] = 0. */
 int hpccg_gpu_time_mixed_kernels(hpccg_ctx *ctx, int32_t precision, int32_t reps, float *ms);
 
 /* The fused inner iteration of the matrix-free solve (HPCCG_SPMV_STENCIL

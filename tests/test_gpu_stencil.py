@@ -229,7 +229,7 @@ def test_fused_inner_solve_matches_three_kernel(hp, torch, n):
     M.set_spmv(hp.SPMV_STENCIL)
     assert M.mixed_fused()
     ms = M.time_mixed_kernels(hp.PREC_FP32, 3)
-    assert ms[0] == 0.0 and ms[2] == 0.0 and ms[1] > 0.0
+    assert ms[0] > 0.0 and ms[2] == 0.0 and ms[1] > 0.0  # FP64 refinement residual, fused pass
     info_f, rc_f = M.solve_mixed_device(db, dx, hp.PREC_FP32, rel_tol=1e-8)
     assert rc_f == hp.HPCCG_OK and info_f.relres <= 1e-8
     r = torch.empty_like(dx)
