@@ -233,8 +233,10 @@ __device__ __forceinline__ void stencil_plane(const Real *__restrict__ p, int nx
   }
 }
 
-// The same sum split at plane boundaries: lead = the first 9 terms (plane
-// z-1) from 0, tail = lead followed by planes z and z+1.
+// The row sum split at the plane boundaries, term for term the reference's
+// order: lead = the nine terms of plane z-1 from 0, mid = s followed by the
+// nine of plane z (27 x_i at the centre), end = s followed by the nine of
+// plane z+1; a row is stencil_end(stencil_mid(stencil_lead(a), b), c).
 template <typename Real>
 __device__ __forceinline__ Real stencil_lead(const Real *a) {
   Real s = Real(0);
@@ -247,10 +249,6 @@ __device__ __forceinline__ Real stencil_lead(const Real *a) {
   }
   return s;
 }
-// The tail split at the plane boundary: mid = s followed by the nine terms of
-// plane z (27 x_i at the centre), end = s followed by those of plane z+1;
-// stencil_end(stencil_mid(s, b), c) is stencil_tail(s, b, c), operation for
-// operation.
 template <typename Real>
 __device__ __forceinline__ Real stencil_mid(Real s, const Real *b) {
   if constexpr (sizeof(Real) == 8) {
@@ -268,21 +266,6 @@ __device__ __forceinline__ Real stencil_end(Real s, const Real *c) {
 #pragma unroll
     for (int j = 0; j < 9; ++j) s = __dsub_rn(s, c[j]);
   } else {
-#pragma unroll
-    for (int j = 0; j < 9; ++j) s -= c[j];
-  }
-  return s;
-}
-template <typename Real>
-__device__ __forceinline__ Real stencil_tail(Real s, const Real *b, const Real *c) {
-  if constexpr (sizeof(Real) == 8) {
-#pragma unroll
-    for (int j = 0; j < 9; ++j) s = j == 4 ? __dadd_rn(s, __dmul_rn(27.0, b[j])) : __dsub_rn(s, b[j]);
-#pragma unroll
-    for (int j = 0; j < 9; ++j) s = __dsub_rn(s, c[j]);
-  } else {
-#pragma unroll
-    for (int j = 0; j < 9; ++j) s = j == 4 ? fmaf(27.f, b[j], s) : s - b[j];
 #pragma unroll
     for (int j = 0; j < 9; ++j) s -= c[j];
   }
@@ -483,28 +466,47 @@ __device__ __forceinline__ double stencil_rows_box64x4(const StencilGeom &g, con
   return part;
 }
 
-// The z walk of one column (plane map): the row sum starts with the 9 terms
-// of plane z-1 added to 0 in order; that prefix depends on plane z-1 alone,
-// so it is formed once per plane (lead) and the window keeps only planes z
-// and z+1 in full.  epi(i, rowsum, x_i) stores and returns a dot term.
+// The pipelined row sums of one column (the single-line form of ColumnPair2
+// below): a row's 27 terms in the reference's order, split at the plane
+// boundaries.  When plane p arrives, end() finishes the row of plane p-1 with
+// p's nine values and middle() carries the row of plane p through its own
+// plane and starts the nine-term prefix of the row of plane p+1 -- three
+// independent 9-term chains a step instead of one 18-term chain.
+template <typename Real>
+struct ColumnLine {
+  Real lead;  // the next plane's row: its first nine terms
+  Real mid;   // the current plane's row: through its own plane
+  Real x;     // x of the current plane's row
+  __device__ __forceinline__ void first(const Real *v) { lead = stencil_lead<Real>(v); }
+  __device__ __forceinline__ void middle(const Real *v) {
+    mid = stencil_mid<Real>(lead, v);
+    x = v[4];
+    lead = stencil_lead<Real>(v);
+  }
+  __device__ __forceinline__ Real end(const Real *v) const { return stencil_end<Real>(mid, v); }
+};
+
+// The z walk of one column (plane map): planes z0-1 .. z1 of the column's 3x3
+// neighbourhood, one plane a step.  epi(i, rowsum, x_i) stores and returns a
+// dot term.
 template <typename Real, class Epi>
 __device__ __forceinline__ double stencil_column(const PlaneSpan &sp, const StencilGeom &g, const PlaneMap &m,
                                                  unsigned mask, const Real *__restrict__ pc, Epi &epi) {
   double part = 0.0;
-  Real b[9], c[9];
-  stencil_plane<Real>(pc + (int64_t)(sp.z0 - 1) * m.plane, g.nx, mask, sp.z0 > 0, c);
-  Real lead = stencil_lead<Real>(c);
-  stencil_plane<Real>(pc + (int64_t)sp.z0 * m.plane, g.nx, mask, true, b);
+  Real v[9];
+  ColumnLine<Real> w;
+  stencil_plane<Real>(pc + (int64_t)(sp.z0 - 1) * m.plane, g.nx, mask, sp.z0 > 0, v);
+  w.first(v);
+  stencil_plane<Real>(pc + (int64_t)sp.z0 * m.plane, g.nx, mask, true, v);
+  w.middle(v);
   for (int z = sp.z0; z < sp.z1; ++z) {
-    stencil_plane<Real>(pc + (int64_t)(z + 1) * m.plane, g.nx, mask, z + 1 < g.nz, c);
-    const Real s = stencil_tail<Real>(lead, b, c);
+    stencil_plane<Real>(pc + (int64_t)(z + 1) * m.plane, g.nx, mask, z + 1 < g.nz, v);
+    const Real s = w.end(v);
     if constexpr (sizeof(Real) == 8)
-      part = __dadd_rn(part, epi(sp.c + z * m.plane, s, b[4]));
+      part = __dadd_rn(part, epi(sp.c + z * m.plane, s, w.x));
     else
-      part += epi(sp.c + z * m.plane, s, b[4]);
-    lead = stencil_lead<Real>(b);
-#pragma unroll
-    for (int j = 0; j < 9; ++j) b[j] = c[j];
+      part += epi(sp.c + z * m.plane, s, w.x);
+    w.middle(v);
   }
   return part;
 }
@@ -518,58 +520,46 @@ __device__ __forceinline__ void stencil_plane3(const Real *__restrict__ p, int n
   v[3] = __ldg(p - 1), v[4] = __ldg(p), v[5] = __ldg(p + 1);
   v[6] = __ldg(r2 - 1), v[7] = __ldg(r2), v[8] = __ldg(r2 + 1);
 }
-// Row z from the lead (its plane z-1 prefix), plane z (b) and plane z+1 (c);
-// then the lead of row z+1.
-template <typename Real, class Epi>
-__device__ __forceinline__ void stencil_step(int i, Real &lead, const Real *b, const Real *c, double &part,
-                                             Epi &epi) {
-  const Real s = stencil_tail<Real>(lead, b, c);
-  if constexpr (sizeof(Real) == 8)
-    part = __dadd_rn(part, epi(i, s, b[4]));
-  else
-    part += epi(i, s, b[4]);
-  lead = stencil_lead<Real>(b);
-}
 // stencil_column for a column whose nine neighbours lie inside the grid in x
-// and y: the planes inside the grid load without selects (the last plane of
-// the grid is peeled off), and the loop runs two planes per trip so the
-// window's two halves trade roles instead of being copied.  Same sums.
+// and y: the planes inside the grid load without selects (the plane above the
+// grid's last one is zeros).  Same sums.
 template <typename Real, class Epi>
 __device__ __forceinline__ double stencil_column_interior(const PlaneSpan &sp, const StencilGeom &g,
                                                           const PlaneMap &m, const Real *__restrict__ pc,
                                                           Epi &epi) {
   double part = 0.0;
-  Real b[9], c[9];
+  Real v[9];
+  ColumnLine<Real> w;
   const int64_t pl = m.plane;
   if (sp.z0 > 0) {
-    stencil_plane3<Real>(pc + (sp.z0 - 1) * pl, g.nx, c);
+    stencil_plane3<Real>(pc + (sp.z0 - 1) * pl, g.nx, v);
   } else {
 #pragma unroll
-    for (int j = 0; j < 9; ++j) c[j] = Real(0);
+    for (int j = 0; j < 9; ++j) v[j] = Real(0);
   }
-  Real lead = stencil_lead<Real>(c);
-  stencil_plane3<Real>(pc + sp.z0 * pl, g.nx, b);
+  w.first(v);
+  stencil_plane3<Real>(pc + sp.z0 * pl, g.nx, v);
+  w.middle(v);
   const int zi = min(sp.z1, g.nz - 1);  // rows whose plane z+1 lies inside the grid
   const Real *p = pc + (sp.z0 + 1) * pl;
   int z = sp.z0;
-  for (; z + 1 < zi; z += 2) {
-    stencil_plane3<Real>(p, g.nx, c);
-    stencil_step<Real>(sp.c + z * m.plane, lead, b, c, part, epi);
-    stencil_plane3<Real>(p + pl, g.nx, b);
-    stencil_step<Real>(sp.c + (z + 1) * m.plane, lead, c, b, part, epi);
-    p += 2 * pl;
-  }
-  if (z < zi) {
-    stencil_plane3<Real>(p, g.nx, c);
-    stencil_step<Real>(sp.c + z * m.plane, lead, b, c, part, epi);
-#pragma unroll
-    for (int j = 0; j < 9; ++j) b[j] = c[j];
-    ++z;
+  for (; z < zi; ++z, p += pl) {
+    stencil_plane3<Real>(p, g.nx, v);
+    const Real s = w.end(v);
+    if constexpr (sizeof(Real) == 8)
+      part = __dadd_rn(part, epi(sp.c + z * m.plane, s, w.x));
+    else
+      part += epi(sp.c + z * m.plane, s, w.x);
+    w.middle(v);
   }
   if (z < sp.z1) {  // z = nz - 1: no plane above
 #pragma unroll
-    for (int j = 0; j < 9; ++j) c[j] = Real(0);
-    stencil_step<Real>(sp.c + z * m.plane, lead, b, c, part, epi);
+    for (int j = 0; j < 9; ++j) v[j] = Real(0);
+    const Real s = w.end(v);
+    if constexpr (sizeof(Real) == 8)
+      part = __dadd_rn(part, epi(sp.c + z * m.plane, s, w.x));
+    else
+      part += epi(sp.c + z * m.plane, s, w.x);
   }
   return part;
 }
