@@ -137,8 +137,8 @@ struct PhInit64 {  // r = b - A x, p = r, rtrans = r.r
     y.rtrans = t;
     y.k = 0;
     y.active = (t > y.tol2) && (g.max_iter > 0);
-    y.converged = !(t > y.tol2);
-    y.relres = y.bb > 0.0 ? sqrt(t / y.bb) : 0.0;
+    y.converged = t <= y.tol2;  // false for a non-finite b, which then fails the final check
+    y.relres = rel_residual(t, y.bb);
   }
   static constexpr int kCond = 1;  // outer (the CG loop)
 };
@@ -205,7 +205,7 @@ struct PhResidual64 {  // final r = b - A x, relres (all systems)
   static __device__ double commit(const BatchArgs &g, int i, int s, const V2 &v) { return __dmul_rn(v.a, v.a); }
   static __device__ void finalize(const BatchArgs &g, int s, double t) {
     BatchSys &y = g.sys[s];
-    y.relres = y.bb > 0.0 ? sqrt(t / y.bb) : 0.0;
+    y.relres = rel_residual(t, y.bb);
     y.converged = y.relres <= g.rel_tol;
   }
   static constexpr int kCond = -1;
@@ -225,7 +225,7 @@ struct PhOuter64 {  // r64 = b - A x, relres, outer decision (systems still refi
   }
   static __device__ void finalize(const BatchArgs &g, int s, double t) {
     BatchSys &y = g.sys[s];
-    y.relres = y.bb > 0.0 ? sqrt(t / y.bb) : 0.0;
+    y.relres = rel_residual(t, y.bb);
     if (!isfinite(y.relres)) {
       y.status = HPCCG_ERR_BREAKDOWN;
       y.active = 0;
@@ -1281,9 +1281,12 @@ extern "C" int hpccg_batch_spmv(hpccg_batch *B, const double *d_x, double *d_y) 
   return HPCCG_OK;
 }
 
-extern "C" int hpccg_batch_solve(hpccg_batch *B, const double *d_b, double *d_x, int32_t precision,
-                                 double rel_tol, int32_t max_iter, int32_t *iters, double *relres,
-                                 int32_t *outer) {
+// The solve of hpccg_batch_solve; b and x are copied in with `in` and the
+// solution out with `out` (device-to-device for device vectors, host-to-device
+// and device-to-host for host arrays).
+static int batch_solve(hpccg_batch *B, const double *d_b, double *d_x, cudaMemcpyKind in, cudaMemcpyKind out,
+                       int32_t precision, double rel_tol, int32_t max_iter, int32_t *iters, double *relres,
+                       int32_t *outer) {
   if (!B || !d_b || !d_x || !(rel_tol >= 0.0) || max_iter < 0) return HPCCG_ERR_INVALID_ARG;
   if (precision != HPCCG_PREC_FP64 && precision != HPCCG_PREC_FP32 && precision != HPCCG_PREC_BF16)
     return HPCCG_ERR_INVALID_ARG;
@@ -1292,14 +1295,14 @@ extern "C" int hpccg_batch_solve(hpccg_batch *B, const double *d_b, double *d_x,
   if (precision != HPCCG_PREC_FP64 && B->spmv_kind != HPCCG_SPMV_STENCIL && (rc = ensure_lp(B, precision)))
     return rc;
   const size_t bytes = sizeof(double) * B->npad;
-  HPCCG_CUDA(cudaMemcpyAsync(B->b, d_b, bytes, cudaMemcpyDeviceToDevice, B->stream));
-  HPCCG_CUDA(cudaMemcpyAsync(B->x, d_x, bytes, cudaMemcpyDeviceToDevice, B->stream));
+  HPCCG_CUDA(cudaMemcpyAsync(B->b, d_b, bytes, in, B->stream));
+  HPCCG_CUDA(cudaMemcpyAsync(B->x, d_x, bytes, in, B->stream));
   HPCCG_CUDA(cudaEventRecord(B->ev0, B->stream));
   const bool eager = getenv("HPCCG_EAGER") && atoi(getenv("HPCCG_EAGER")) != 0;
   rc = run_batch(B, precision, eager, rel_tol, max_iter);
   if (rc) return rc;
   HPCCG_CUDA(cudaEventRecord(B->ev1, B->stream));
-  HPCCG_CUDA(cudaMemcpyAsync(d_x, B->x, bytes, cudaMemcpyDeviceToDevice, B->stream));
+  HPCCG_CUDA(cudaMemcpyAsync(d_x, B->x, bytes, out, B->stream));
   std::vector<BatchSys> hs(B->nsys);
   HPCCG_CUDA(cudaMemcpyAsync(hs.data(), B->sys, sizeof(BatchSys) * B->nsys, cudaMemcpyDeviceToHost, B->stream));
   HPCCG_CUDA(cudaStreamSynchronize(B->stream));
@@ -1313,6 +1316,20 @@ extern "C" int hpccg_batch_solve(hpccg_batch *B, const double *d_b, double *d_x,
     else if (!hs[s].converged && status == HPCCG_OK) status = HPCCG_ERR_NOT_CONVERGED;
   }
   return status;
+}
+
+extern "C" int hpccg_batch_solve(hpccg_batch *B, const double *d_b, double *d_x, int32_t precision,
+                                 double rel_tol, int32_t max_iter, int32_t *iters, double *relres,
+                                 int32_t *outer) {
+  return batch_solve(B, d_b, d_x, cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice, precision, rel_tol, max_iter,
+                     iters, relres, outer);
+}
+
+extern "C" int hpccg_batch_solve_host(hpccg_batch *B, const double *b, double *x, int32_t precision,
+                                      double rel_tol, int32_t max_iter, int32_t *iters, double *relres,
+                                      int32_t *outer) {
+  return batch_solve(B, b, x, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, precision, rel_tol, max_iter, iters,
+                     relres, outer);
 }
 
 extern "C" int hpccg_batch_last_solve_ms(const hpccg_batch *B, float *ms) {

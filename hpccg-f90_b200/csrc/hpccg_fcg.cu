@@ -285,7 +285,7 @@ extern "C" int hpccg_gpu_solve_fcg(hpccg_ctx *c, hpccg_unet *u, int32_t nx, int3
   if (!rc) {
     if ((rc = residual()) == 0) rc = read_state();
   }
-  relres = bnorm > 0 ? sqrt(h.rr) / bnorm : 0.0;
+  relres = rel_norm(sqrt(h.rr), bnorm);
   HPCCG_CUDA(cudaEventRecord(c->solve1, s));
   cudaMemcpyAsync(d_x, c->d_x, bytes, cudaMemcpyDeviceToDevice, s);
   cudaStreamSynchronize(s);

@@ -42,6 +42,20 @@ struct Reduction {
   unsigned *counter;  // arrival counter, reset by the last block
 };
 
+// ||r|| / ||b|| from the two norms.  A non-finite b (a NaN anywhere in it)
+// gives NaN, so a solver reports it instead of taking it for convergence; for
+// b = 0 the ratio is 0 when r = 0 too and the largest double otherwise (the
+// relative target can then never be met).
+__host__ __device__ __forceinline__ double rel_norm(double rnorm, double bnorm) {
+  if (bnorm > 0.0) return rnorm / bnorm;
+  if (bnorm == 0.0) return rnorm == 0.0 ? 0.0 : (rnorm > 0.0 ? 1.7976931348623157e308 : rnorm);
+  return bnorm;  // NaN
+}
+// The same from the squared norms r.r and b.b.
+__host__ __device__ __forceinline__ double rel_residual(double rr, double bb) {
+  return rel_norm(sqrt(rr), sqrt(bb));
+}
+
 }  // namespace hpccg
 
 struct hpccg_ctx {

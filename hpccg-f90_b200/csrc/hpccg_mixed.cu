@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kBlock, S::kMinBlocks) k_mp_residual64(const _
     if (threadIdx.x == 0) {
       MixedState &st = *g.st;
       st.rr64 = rr;
-      st.relres = st.bb > 0.0 ? sqrt(rr / st.bb) : 0.0;
+      st.relres = rel_residual(rr, st.bb);
       int cont = (st.relres > st.rel_tol) && (st.outer < st.max_outer);
       if (!isfinite(st.relres)) {
         st.status = HPCCG_ERR_BREAKDOWN;
@@ -162,7 +162,7 @@ __device__ __forceinline__ void residual_decision(const MixedArgs &g, const doub
   }
   const double rr = v[0];
   st.rr64 = rr;
-  st.relres = st.bb > 0.0 ? sqrt(rr / st.bb) : 0.0;
+  st.relres = rel_residual(rr, st.bb);
   int cont = !st.status && (st.relres > st.rel_tol) && (st.outer < st.max_outer);
   if (!isfinite(st.relres)) {
     st.status = HPCCG_ERR_BREAKDOWN;

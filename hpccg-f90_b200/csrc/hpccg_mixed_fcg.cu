@@ -331,7 +331,7 @@ extern "C" int hpccg_gpu_solve_mixed_fcg(hpccg_ctx *c, hpccg_unet *u, int32_t nx
   cudaEventElapsedTime(&c->last_solve_ms, c->solve0, c->solve1);
   cleanup();
   if (rc) return rc;
-  const double relres = bnorm > 0 ? rnorm / bnorm : 0.0;
+  const double relres = rel_norm(rnorm, bnorm);
   if (info) {
     info->outer_iters = outer;
     info->inner_iters = inner_total;

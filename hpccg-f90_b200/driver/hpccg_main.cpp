@@ -8,6 +8,17 @@
 //
 //   HPCCG-B200 nx ny nz [--max-iter N] [--tol T] [--device-generate]
 //                       [--spmv KIND[,PARAM]] [--timing-level L] [--quiet]
+//                       [--precision fp64|fp32|bf16] [--rel-tol R]
+//   HPCCG-B200 --batch SPEC [--precision ...] [--rel-tol R] [--max-iter N] [--spmv 4]
+//
+// --precision fp32 or bf16 replaces the reference's fixed-count CG by the
+// FP64 iterative refinement around a low-precision inner CG
+// (hpccg_gpu_solve_mixed), run to the FP64 relative residual --rel-tol
+// (default 1e-8); fp64 (the default) is the reference's CG.  --batch solves
+// many generate_matrix systems of the reference's problem (x0 = 0, b = A 1)
+// together (hpccg_batch_solve_host), each to --rel-tol; SPEC is a list
+// "nx,ny,nz/nx,ny,nz/..." or "random:COUNT,LO,HI,SEED" (each of nx, ny, nz
+// uniform in [LO, HI] from the project's generator, as the bench's batch).
 //
 // --timing-level follows the reference's TIMINGLEV (MPI/config.mk TIMER_LEVEL,
 // default 1; numerics.F90:100-156): 1 prints "TIMER: Total"; 2 adds one
@@ -61,32 +72,161 @@ static void check(int rc, const char *what) {
   }
 }
 
-int main(int argc, char **argv) {
-  if (argc < 4) {
-    printf(" USAGE: ./HPCCG <nx> <ny> <nz>\n");
-    return 0;
+// The project's counter-based generator (splitmix64 finaliser of
+// seed + (i+1) * 0x9E3779B97F4A7C15), the sequence hpccg_gpu_uniform_pm1 draws.
+static uint64_t splitmix64_at(uint64_t seed, uint64_t i) {
+  uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// Grid sizes of a --batch SPEC (see the header); false on a malformed spec.
+static bool batch_spec(const char *spec, std::vector<int32_t> *sizes) {
+  sizes->clear();
+  if (!strncmp(spec, "random:", 7)) {
+    long long count = 0, lo = 0, hi = 0, seed = 0;
+    if (sscanf(spec + 7, "%lld,%lld,%lld,%lld", &count, &lo, &hi, &seed) != 4 || count < 1 || lo < 1 || hi < lo)
+      return false;
+    for (long long i = 0; i < 3 * count; ++i)
+      sizes->push_back((int32_t)(lo + (long long)(splitmix64_at((uint64_t)seed, (uint64_t)i) % (uint64_t)(hi - lo + 1))));
+    return true;
   }
-  const int nx = atoi(argv[1]), ny = atoi(argv[2]), nz = atoi(argv[3]);
+  const char *q = spec;
+  while (*q) {
+    int a = 0, b = 0, c = 0, used = 0;
+    if (sscanf(q, "%d,%d,%d%n", &a, &b, &c, &used) != 3 || a < 1 || b < 1 || c < 1) return false;
+    sizes->push_back(a);
+    sizes->push_back(b);
+    sizes->push_back(c);
+    q += used;
+    if (*q == '/') ++q;
+    else if (*q) return false;
+  }
+  return !sizes->empty();
+}
+
+// b = 27 - (nnzrow - 1) of generate_matrix's row (SparseMatrix.F90:170-172),
+// nnzrow the row's kept neighbours; rows in the reference's order, x fastest.
+static void reference_rhs(int nx, int ny, int nz, double *b) {
+  auto kept = [](int i, int m) { return 1 + (i > 1) + (i < m); };
+  const int64_t n = (int64_t)nx * ny * nz;
+  for (int64_t r = 0; r < n; ++r) {
+    const int ix = (int)(r % nx) + 1, iy = (int)((r / nx) % ny) + 1, iz = (int)(r / ((int64_t)nx * ny)) + 1;
+    b[r] = 27.0 - (double)(kept(ix, nx) * kept(iy, ny) * kept(iz, nz) - 1);
+  }
+}
+
+static int precision_code(const char *name) {
+  if (!strcmp(name, "fp64")) return HPCCG_PREC_FP64;
+  if (!strcmp(name, "fp32")) return HPCCG_PREC_FP32;
+  if (!strcmp(name, "bf16")) return HPCCG_PREC_BF16;
+  return -1;
+}
+static const char *precision_name(int p) { return p == HPCCG_PREC_FP32 ? "FP32" : p == HPCCG_PREC_BF16 ? "BF16" : "FP64"; }
+
+// --batch: every system of the spec, solved together on the device.
+static int run_batch(const std::vector<int32_t> &sizes, int precision, double rel_tol, int max_iter, int spmv_kind,
+                     int timing_level) {
+  const int nsys = (int)(sizes.size() / 3);
+  hpccg_batch *B = nullptr;
+  check(hpccg_batch_create_generated(nsys, sizes.data(), &B), "batch_create_generated");
+  if (spmv_kind == HPCCG_SPMV_STENCIL) check(hpccg_batch_set_spmv(B, HPCCG_SPMV_STENCIL), "batch_set_spmv");
+  int32_t ns = 0;
+  int64_t rows = 0;
+  check(hpccg_batch_info(B, &ns, &rows, nullptr), "batch_info");
+  std::vector<int64_t> offs(2 * (size_t)nsys);
+  check(hpccg_batch_info(B, nullptr, nullptr, offs.data()), "batch_info");
+  std::vector<double> b((size_t)rows, 0.0), x((size_t)rows, 0.0);
+  int64_t total = 0;
+  for (int s = 0; s < nsys; ++s) {
+    reference_rhs(sizes[3 * s], sizes[3 * s + 1], sizes[3 * s + 2], b.data() + offs[2 * s]);
+    total += offs[2 * s + 1];
+  }
+  printf(" HPCCG Benchmark\n");
+  printf(" Using double precision\n");
+  printf(" Batch of %d systems, %lld rows in all\n", nsys, (long long)total);
+  printf(" Solver: %s\n", precision == HPCCG_PREC_FP64 ? "FP64 CG per system"
+                                                      : precision == HPCCG_PREC_FP32
+                                                            ? "FP64 iterative refinement, FP32 inner CG per system"
+                                                            : "FP64 iterative refinement, BF16-value inner CG per system");
+  std::vector<int32_t> iters(nsys), outer(nsys);
+  std::vector<double> relres(nsys);
+  const auto t0 = std::chrono::steady_clock::now();
+  const int rc = hpccg_batch_solve_host(B, b.data(), x.data(), precision, rel_tol, max_iter, iters.data(),
+                                        relres.data(), outer.data());
+  const auto t1 = std::chrono::steady_clock::now();
+  if (rc != HPCCG_OK && rc != HPCCG_ERR_NOT_CONVERGED) check(rc, "batch_solve_host");
+  for (int s = 0; s < nsys; ++s) {
+    double err = 0.0;
+    for (int64_t i = 0; i < offs[2 * s + 1]; ++i) err = std::fmax(err, std::fabs(x[offs[2 * s] + i] - 1.0));
+    printf(" System %d (%d x %d x %d): iterations %d, refinement cycles %d, FP64 rel-res %.6e, "
+           "max|x - xexact| %.3e\n",
+           s, sizes[3 * s], sizes[3 * s + 1], sizes[3 * s + 2], iters[s], outer[s], relres[s], err);
+  }
+  float ms = 0.f;
+  check(hpccg_batch_last_solve_ms(B, &ms), "batch_last_solve_ms");
+  if (timing_level > 0) {
+    printf(" TIMER: Total %15.7g sec\n", std::chrono::duration<double>(t1 - t0).count());
+    printf(" TIMER: Device %15.7g sec\n", 1e-3 * ms);
+  }
+  if (rc == HPCCG_ERR_NOT_CONVERGED) printf(" Not every system reached the target\n");
+  hpccg_batch_destroy(B);
+  return rc == HPCCG_OK ? 0 : 3;
+}
+
+int main(int argc, char **argv) {
   int max_iter = 150;    // main.F90:127
   double tolerance = 0;  // main.F90:128
+  double rel_tol = 1e-8;
   bool device_generate = false, quiet = false;
   int timing_level = 1;  // MPI/config.mk TIMER_LEVEL
   int spmv_kind = HPCCG_SPMV_AUTO, spmv_param = 0;
-  for (int i = 4; i < argc; ++i) {
+  int precision = HPCCG_PREC_FP64;
+  const char *batch = nullptr;
+  std::vector<int> pos;
+  for (int i = 1; i < argc; ++i) {
     if (!strcmp(argv[i], "--max-iter") && i + 1 < argc) max_iter = atoi(argv[++i]);
     else if (!strcmp(argv[i], "--tol") && i + 1 < argc) tolerance = atof(argv[++i]);
+    else if (!strcmp(argv[i], "--rel-tol") && i + 1 < argc) rel_tol = atof(argv[++i]);
     else if (!strcmp(argv[i], "--device-generate")) device_generate = true;
     else if (!strcmp(argv[i], "--quiet")) quiet = true;
     else if (!strcmp(argv[i], "--timing-level") && i + 1 < argc) timing_level = atoi(argv[++i]);
-    else if (!strcmp(argv[i], "--spmv") && i + 1 < argc) {
+    else if (!strcmp(argv[i], "--batch") && i + 1 < argc) batch = argv[++i];
+    else if (!strcmp(argv[i], "--precision") && i + 1 < argc) {
+      precision = precision_code(argv[++i]);
+      if (precision < 0) {
+        fprintf(stderr, "HPCCG-B200: --precision takes fp64, fp32 or bf16\n");
+        return 2;
+      }
+    } else if (!strcmp(argv[i], "--spmv") && i + 1 < argc) {
       spmv_kind = atoi(argv[++i]);
       const char *comma = strchr(argv[i], ',');
       if (comma) spmv_param = atoi(comma + 1);
+    } else if (argv[i][0] != '-' && pos.size() < 3) {
+      pos.push_back(atoi(argv[i]));
     } else {
       fprintf(stderr, "HPCCG-B200: unknown option %s\n", argv[i]);
       return 2;
     }
   }
+  if (!(rel_tol > 0.0)) {
+    fprintf(stderr, "HPCCG-B200: --rel-tol must be positive\n");
+    return 2;
+  }
+  if (batch) {
+    std::vector<int32_t> sizes;
+    if (!batch_spec(batch, &sizes)) {
+      fprintf(stderr, "HPCCG-B200: bad --batch spec %s\n", batch);
+      return 2;
+    }
+    return run_batch(sizes, precision, rel_tol, max_iter, spmv_kind, timing_level);
+  }
+  if (pos.size() < 3) {
+    printf(" USAGE: ./HPCCG <nx> <ny> <nz>\n");
+    return 0;
+  }
+  const int nx = pos[0], ny = pos[1], nz = pos[2];
   if (nx < 1 || ny < 1 || nz < 1) {
     fprintf(stderr, "HPCCG-B200: nx, ny, nz must be positive\n");
     return 2;
@@ -100,11 +240,9 @@ int main(int argc, char **argv) {
     // neighbour count, b = 27 - (nnzrow - 1) (SparseMatrix.F90:170-172).
     check(hpccg_gpu_create_generated(nx, ny, nz, nullptr, nullptr, nullptr, &ctx), "generate");
     check(hpccg_gpu_info(ctx, nullptr, &nnz, nullptr), "info");
-    auto kept = [](int i, int m) { return 1 + (i > 1) + (i < m); };
+    reference_rhs(nx, ny, nz, b.data());
     for (int64_t r = 0; r < n; ++r) {
-      const int ix = (int)(r % nx) + 1, iy = (int)((r / nx) % ny) + 1, iz = (int)(r / ((int64_t)nx * ny)) + 1;
       x[r] = 0.0;
-      b[r] = 27.0 - (double)(kept(ix, nx) * kept(iy, ny) * kept(iz, nz) - 1);
       xexact[r] = 1.0;
     }
   } else {
@@ -128,6 +266,31 @@ int main(int argc, char **argv) {
   printf(" MPI disabled.\n");
   printf(" OpenMP disabled.\n");
   printf(" GPU: sm_100a kernels, stored nonzeroes %lld\n", (long long)nnz);
+
+  if (precision != HPCCG_PREC_FP64) {
+    // FP64 iterative refinement around the low-precision inner CG, to rel_tol
+    printf(" Solver: FP64 iterative refinement, %s inner CG, FP64 rel-res target %g\n", precision_name(precision),
+           rel_tol);
+    hpccg_mixed_info info{};
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = hpccg_gpu_solve_mixed(ctx, b.data(), x.data(), precision, rel_tol, 30, max_iter, 0.0, &info);
+    const auto t1 = std::chrono::steady_clock::now();
+    if (rc != HPCCG_OK && rc != HPCCG_ERR_NOT_CONVERGED) check(rc, "solve_mixed");
+    printf(" Refinement cycles: %d  inner iterations: %d  FP64 rel-res: %.6e\n", info.outer_iters, info.inner_iters,
+           info.relres);
+    float solve_ms = 0.f;
+    check(hpccg_gpu_last_solve_ms(ctx, &solve_ms), "last_solve_ms");
+    if (timing_level > 0) {
+      printf(" TIMER: Total %15.7g sec\n", std::chrono::duration<double>(t1 - t0).count());
+      printf(" TIMER: Device %15.7g sec\n", 1e-3 * solve_ms);
+    }
+    double err = 0.0;
+    for (int64_t i = 0; i < n; ++i) err = std::fmax(err, std::fabs(x[i] - xexact[i]));
+    printf(" max|x - xexact|: %.3e\n", err);
+    if (rc == HPCCG_ERR_NOT_CONVERGED) printf(" Not converged in 30 refinement cycles\n");
+    hpccg_gpu_destroy(ctx);
+    return rc == HPCCG_OK ? 0 : 3;
+  }
 
   std::vector<double> hist(max_iter + 1);
   int32_t niters = 0;

@@ -93,6 +93,7 @@ _SIGS = {
     "hpccg_batch_get_schedule": (_c.c_int, [_vp, _c.POINTER(_i32), _c.POINTER(_i32)]),
     "hpccg_batch_spmv": (_c.c_int, [_vp, _vp, _vp]),
     "hpccg_batch_solve": (_c.c_int, [_vp, _vp, _vp, _i32, _f64, _i32, _vp, _vp, _vp]),
+    "hpccg_batch_solve_host": (_c.c_int, [_vp, _f64p, _f64p, _i32, _f64, _i32, _vp, _vp, _vp]),
     "hpccg_batch_last_solve_ms": (_c.c_int, [_vp, _c.POINTER(_c.c_float)]),
     "hpccg_unet_create": (_c.c_int, [_c.c_uint64, _c.POINTER(_vp)]),
     "hpccg_unet_destroy": (None, [_vp]),
@@ -500,6 +501,20 @@ class Batch:
         rc = _lib.hpccg_batch_solve(self._h, _dptr(d_b), _dptr(d_x), precision, rel_tol, max_iter,
                                     iters.ctypes.data, relres.ctypes.data, outer.ctypes.data)
         _check(rc, "batch_solve", allow=(HPCCG_OK, HPCCG_ERR_NOT_CONVERGED, HPCCG_ERR_BREAKDOWN))
+        return iters, relres, outer, rc
+
+    def solve_host(self, b, x, precision: int = PREC_FP64, rel_tol: float = 1e-8, max_iter: int = 1000):
+        """Stacked HOST arrays (float64, length stacked_rows); x is updated in place.
+        Returns (iters, relres, outer, status) per system."""
+        b = np.ascontiguousarray(b, np.float64)
+        if x.dtype != np.float64 or not x.flags.c_contiguous or b.shape != x.shape or b.size != self.stacked_rows:
+            raise ValueError("b and x must be contiguous float64 arrays of the stacked length")
+        iters = np.zeros(self.nsys, np.int32)
+        relres = np.zeros(self.nsys, np.float64)
+        outer = np.zeros(self.nsys, np.int32)
+        rc = _lib.hpccg_batch_solve_host(self._h, b, x, precision, rel_tol, max_iter, iters.ctypes.data,
+                                         relres.ctypes.data, outer.ctypes.data)
+        _check(rc, "batch_solve_host", allow=(HPCCG_OK, HPCCG_ERR_NOT_CONVERGED, HPCCG_ERR_BREAKDOWN))
         return iters, relres, outer, rc
 
     def last_solve_ms(self) -> float:

@@ -226,6 +226,12 @@ int hpccg_batch_spmv(hpccg_batch *batch, const double *d_x, double *d_y);
 int hpccg_batch_solve(hpccg_batch *batch, const double *d_b, double *d_x, int32_t precision,
                       double rel_tol, int32_t max_iter, int32_t *iters, double *relres,
                       int32_t *outer);
+/* The same with HOST arrays b and x (stacked layout, length stacked_rows):
+ * the library copies them in and the solution out.  The call a host driver
+ * makes, like hpccg_gpu_cg for one system. */
+int hpccg_batch_solve_host(hpccg_batch *batch, const double *b, double *x, int32_t precision,
+                           double rel_tol, int32_t max_iter, int32_t *iters, double *relres,
+                           int32_t *outer);
 /* Device ms of the last hpccg_batch_solve (events around the graph launch). */
 int hpccg_batch_last_solve_ms(const hpccg_batch *batch, float *ms);
 

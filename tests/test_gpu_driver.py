@@ -5,7 +5,10 @@ numerics.F90:103-156): printInfo lines with total_nnz = 27 N, the initial
 residual, the ITER lines at print_freq = clamp(max_iter/10, 1, 50) and at
 k + 1 = max_iter in e20.10, the TIMER lines of each timing level and
 MFLOPS SPARSEMV; the printed residuals equal the oracle's history to the 10
-digits printed; the matrix-free SpMV prints the identical history.
+digits printed; the matrix-free SpMV prints the identical history.  The
+options beyond the reference (--precision, --rel-tol, --batch) against the
+library's own calls and the oracle, the host-array batch call, and host-side
+fault injection (a NaN in b, a zero on the diagonal).
 """
 import os
 import re
@@ -68,3 +71,129 @@ def test_driver_stencil_prints_identical_history():
     assert _iters(st) and _iters(st) == _iters(gen)
     for k, v in _iters(base).items():
         assert _iters(st)[k] == pytest.approx(v, rel=1.1e-9)
+
+
+def _field(pattern, text, cast=float):
+    m = re.search(pattern, text, re.M)
+    assert m, (pattern, text[-2000:])
+    return cast(m.group(1))
+
+
+@pytest.mark.parametrize("extra", [(), ("--spmv", 4, "--device-generate")])
+def test_driver_mixed_precision_reaches_fp64_target(extra):
+    """--precision fp32: FP64 refinement around the FP32 inner CG on the reference's problem (b = A 1),
+    to the FP64 relative residual --rel-tol; the same cycles and inner iterations as the library call
+    on the same system, and the oracle's own residual of x = 1 bounds the error."""
+    import hpccg_b200 as hp
+
+    n = 24
+    out = _run(n, n, n, "--precision", "fp32", "--rel-tol", "1e-9", *extra)
+    relres = _field(r"FP64 rel-res: (\S+)$", out)
+    outer = _field(r"Refinement cycles: (\d+)", out, int)
+    inner = _field(r"inner iterations: (\d+)", out, int)
+    err = _field(r"max\|x - xexact\|: (\S+)$", out)
+    assert relres <= 1e-9 and err <= 1e-7, (relres, err)
+    A, x, b, xe = oracle.generate_matrix(n, n, n)
+    M = hp.Matrix.generated(n, n, n) if extra else hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    if extra:
+        M.set_spmv(hp.SPMV_STENCIL)
+    gx, info, st = M.solve_mixed(b, x.copy(), hp.PREC_FP32, 1e-9, 30, 150)
+    M.close()
+    assert st == hp.HPCCG_OK and (info.outer_iters, info.inner_iters) == (outer, inner)
+    assert oracle.true_relres(A, b, gx) <= 1e-9 * (1 + 1e-6)
+
+
+def test_driver_batch_random_spec_matches_oracle():
+    """--batch random:COUNT,LO,HI,SEED draws the sizes from the project's generator (the bench's batch
+    workload uses the same draw); every system of the reference's problem is solved in FP64 CG to
+    --rel-tol with the oracle CG's iteration count (one more or less for a stop on the border)."""
+    spec = (6, 6, 20, 7)
+    out = _run("--batch", "random:%d,%d,%d,%d" % spec)
+    sizes = oracle.batch_sizes(spec[3], spec[0], spec[1], spec[2])
+    lines = re.findall(r"^ System (\d+) \((\d+) x (\d+) x (\d+)\): iterations (\d+), refinement cycles (\d+), "
+                       r"FP64 rel-res (\S+), max\|x - xexact\| (\S+)$", out, re.M)
+    assert len(lines) == spec[0]
+    for s, (idx, nx, ny, nz, it, _, rel, err) in enumerate(lines):
+        assert int(idx) == s and [int(nx), int(ny), int(nz)] == list(sizes[s])
+        A, x, b, _ = oracle.generate_matrix(*sizes[s])
+        _, ref_it, _, _ = oracle.cg(A, b, x, 1000, 1e-8 * float(np.linalg.norm(b)))
+        assert abs(int(it) - ref_it) <= 1, (s, it, ref_it)
+        assert float(rel) <= 1e-8 and float(err) <= 1e-6
+    assert re.search(r"^ TIMER: Device\s+\S+ sec$", out, re.M)
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+def test_driver_batch_list_spec_mixed(prec):
+    """An explicit size list, FP64 refinement around the low-precision inner CG per system, with the
+    stored-matrix rows and the matrix-free ones."""
+    for extra in ((), ("--spmv", 4)):
+        out = _run("--batch", "5,6,7/16,16,16/1,1,40", "--precision", prec, *extra)
+        rel = [float(v) for v in re.findall(r"FP64 rel-res (\S+),", out)]
+        assert len(rel) == 3 and max(rel) <= 1e-8, (extra, rel)
+
+
+def test_batch_host_arrays_equal_device_vectors():
+    """hpccg_batch_solve_host (host arrays in and out) gives the device-vector call's iterates."""
+    import torch
+
+    import hpccg_b200 as hp
+
+    sizes = [(5, 6, 7), (12, 9, 8), (3, 3, 33)]
+    B = hp.Batch.generated(sizes)
+    xs = B.stack([oracle.uniform_pm1(3 + s, int(B.nrows[s])) for s in range(B.nsys)])
+    d_xs = torch.from_numpy(xs).cuda()
+    d_b = torch.empty_like(d_xs)
+    B.spmv(d_xs, d_b)
+    b = d_b.cpu().numpy()
+    for prec in (hp.PREC_FP64, hp.PREC_FP32):
+        d_x = torch.zeros_like(d_b)
+        it_d, rel_d, out_d, rc_d = B.solve(d_b, d_x, prec, 1e-9)
+        x = np.zeros_like(b)
+        it_h, rel_h, out_h, rc_h = B.solve_host(b, x, prec, 1e-9)
+        assert rc_d == rc_h == hp.HPCCG_OK
+        assert np.array_equal(it_d, it_h) and np.array_equal(out_d, out_h) and np.array_equal(rel_d, rel_h)
+        assert np.array_equal(d_x.cpu().numpy(), x)
+
+
+def test_nan_in_b_is_reported_not_hung():
+    """Fault injection on the host: a NaN in b makes the first alpha non-finite; the CG graph exits
+    and the call returns HPCCG_ERR_BREAKDOWN at once, and the mixed solver stops with a non-OK status
+    within its cycle cap; the context stays usable for the next solve."""
+    import hpccg_b200 as hp
+
+    A, x, b, xe = oracle.generate_matrix(8, 8, 8)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    bad = b.copy()
+    bad[17] = np.nan
+    _, it, normr, hist, st = M.cg(bad, x.copy(), 150, 0.0)
+    assert st == hp.HPCCG_ERR_BREAKDOWN and it < 150
+    _, info, mst = M.solve_mixed(bad, x.copy(), hp.PREC_FP32, 1e-8, 3, 50)
+    assert mst in (hp.HPCCG_ERR_BREAKDOWN, hp.HPCCG_ERR_NOT_CONVERGED)
+    gx, it, normr, hist, st = M.cg(b, x.copy(), 150, 0.0)  # the same context, a clean right-hand side
+    assert st == hp.HPCCG_OK and np.abs(gx - xe).max() <= 1e-10
+    M.close()
+
+
+def test_zero_diagonal_ends_within_caps():
+    """Fault injection on the host: a zero on the diagonal makes A indefinite.  The reference's CG has
+    no test for that and runs to max_iter; so does this one (or it stops with HPCCG_ERR_BREAKDOWN if a
+    scalar turns non-finite), the mixed solver ends within its cycle cap, and the next context solves
+    the intact matrix."""
+    import hpccg_b200 as hp
+
+    A, x, b, xe = oracle.generate_matrix(6, 5, 4)
+    vals = A.values.copy()
+    row = 37
+    for k in range(A.rowindex[row] - 1, A.rowindex[row + 1] - 1):
+        if A.colindex[k] - 1 == row:
+            vals[k] = 0.0
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, vals)
+    _, it, normr, hist, st = M.cg(b, x.copy(), 150, 0.0)
+    assert st in (hp.HPCCG_OK, hp.HPCCG_ERR_BREAKDOWN) and it <= 150
+    _, info, mst = M.solve_mixed(b, x.copy(), hp.PREC_FP32, 1e-8, 3, 50)
+    assert mst in (hp.HPCCG_OK, hp.HPCCG_ERR_NOT_CONVERGED, hp.HPCCG_ERR_BREAKDOWN) and info.outer_iters <= 3
+    M.close()
+    M2 = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    gx, it, normr, hist, st = M2.cg(b, x.copy(), 150, 0.0)
+    assert st in (hp.HPCCG_OK, hp.HPCCG_ERR_BREAKDOWN) and np.abs(gx - xe).max() <= 1e-10
+    M2.close()

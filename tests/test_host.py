@@ -79,6 +79,24 @@ def test_driver_built_and_prints_usage():
     assert out.returncode == 0 and "USAGE" in out.stdout
 
 
+@pytest.mark.parametrize("args,msg", [
+    (["--batch", "random:0,8,20,7"], "bad --batch spec"),
+    (["--batch", "4,4"], "bad --batch spec"),
+    (["--batch", "4,4,4/5,x,5"], "bad --batch spec"),
+    (["--batch", "random:3,9,8,1"], "bad --batch spec"),
+    (["8", "8", "8", "--precision", "fp16"], "--precision takes fp64, fp32 or bf16"),
+    (["8", "8", "8", "--rel-tol", "0"], "--rel-tol must be positive"),
+    (["8", "8", "8", "--frobnicate"], "unknown option"),
+])
+def test_driver_rejects_bad_options_before_any_device_work(args, msg):
+    """The driver's option errors exit with status 2 on the host (no GPU needed)."""
+    exe = os.path.join(PKG, "HPCCG-B200")
+    if not os.path.exists(exe):
+        subprocess.run(["make", "-s", "-C", PKG], check=True)
+    out = subprocess.run([exe, *args], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 2 and msg in out.stderr, (out.returncode, out.stderr)
+
+
 def test_host_generator_matches_oracle():
     """The package's host copy of the generator (workload synthesis in bench.py)
     draws the same numbers as the oracle's restatement."""
