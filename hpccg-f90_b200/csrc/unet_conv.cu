@@ -422,16 +422,20 @@ __global__ void __launch_bounds__(kConvThreads * row_pipes(NIN, RX), 1) k_conv3_
           uint64_t sd[3];
 #pragma unroll
           for (int j = 0; j < 3; ++j) sd[j] = smem_desc(sA + ((sc0 + i + j) % R) * kSlab, kSlabPlaneBytes, 128);
+          // taps in dy-major order: the nine of dy = -1 first, so slab y-1 (this
+          // tile is its last user) is released as soon as they complete and the
+          // producer refills its slot while the other 18 run
 #pragma unroll
           for (int ks = 0; ks < 27 * NIN; ++ks) {
-            const int tap = ks / NIN, in = ks % NIN;
-            const int dzp = tap / 9, dyp = (tap / 3) % 3, dxp = tap % 3;  // offsets + 1
+            const int t = ks / NIN, in = ks % NIN;
+            const int dyp = t / 9, dzp = (t / 3) % 3, dxp = t % 3;  // offsets + 1
+            const int tap = dzp * 9 + dyp * 3 + dxp;
             const uint64_t ad = sd[dyp] + (uint64_t)((in * 2 * kSlabPlaneBytes + (dzp * kRowVox + dxp) * 16) >> 4);
             const uint64_t bd = wd + (uint64_t)(((in * 27 + tap) * kWTapBytes) >> 4);
             mma_bf16(d, ad, bd, idesc, ks > 0 ? 1u : 0u);
+            if (ks == 9 * NIN - 1) mma_commit(&empty[(sc0 + i) % R]);  // slab y-1 is done for the unit
           }
           mma_commit(&acc_full[buf]);
-          mma_commit(&empty[(sc0 + i) % R]);  // slab y-1 of this tile is done for the unit
         }
         if (!ok) break;
         mma_commit(&empty[(sc0 + ntile) % R]);  // the unit's last two slabs
