@@ -197,3 +197,34 @@ def test_zero_diagonal_ends_within_caps():
     gx, it, normr, hist, st = M2.cg(b, x.copy(), 150, 0.0)
     assert st in (hp.HPCCG_OK, hp.HPCCG_ERR_BREAKDOWN) and np.abs(gx - xe).max() <= 1e-10
     M2.close()
+
+
+def test_zero_rhs_edge_cases():
+    """b = 0.  From x0 = 0 the mixed solver and the batch report convergence at once (r = 0 too); from
+    x0 != 0 the relative target ||r|| <= tol ||b|| = 0 cannot be met, so they stop at their caps with
+    HPCCG_ERR_NOT_CONVERGED (never a false success), having driven x towards 0.  The reference's CG
+    (tolerance 0) computes 0/0 on r = 0; the C-ABI stops there with HPCCG_ERR_BREAKDOWN and x0 unchanged."""
+    import torch
+
+    import hpccg_b200 as hp
+
+    A, x, b, xe = oracle.generate_matrix(6, 6, 6)
+    M = hp.Matrix.from_csr(A.rowindex, A.colindex, A.values)
+    zero = np.zeros_like(b)
+    _, info, st = M.solve_mixed(zero, zero.copy(), hp.PREC_FP32, 1e-8, 3, 50)
+    assert st == hp.HPCCG_OK and info.relres == 0.0
+    x1 = np.ones_like(b)
+    _, info, st = M.solve_mixed(zero, x1, hp.PREC_FP32, 1e-8, 3, 50)
+    assert st == hp.HPCCG_ERR_NOT_CONVERGED and info.outer_iters == 3 and np.abs(x1).max() < 1e-3
+    gx, it, normr, hist, st = M.cg(zero, zero.copy(), 150, 0.0)
+    assert st == hp.HPCCG_ERR_BREAKDOWN and normr == 0.0 and not np.any(gx)
+    M.close()
+    B = hp.Batch.generated([(6, 6, 6), (5, 4, 3)])
+    d_b = torch.zeros(B.stacked_rows, dtype=torch.float64, device="cuda")
+    for prec in (hp.PREC_FP64, hp.PREC_FP32):
+        d_x = torch.zeros_like(d_b)
+        iters, relres, outer, rc = B.solve(d_b, d_x, prec, 1e-8)
+        assert rc == hp.HPCCG_OK and not np.any(relres), (prec, relres)
+        d_x = torch.from_numpy(B.stack([np.ones(int(n)) for n in B.nrows])).cuda()  # zero gaps
+        iters, relres, outer, rc = B.solve(d_b, d_x, prec, 1e-8, 40)
+        assert rc == hp.HPCCG_ERR_NOT_CONVERGED and np.all(relres > 1e300), (prec, relres)
