@@ -311,13 +311,15 @@ __device__ __forceinline__ void iter_rows_tma(const TmaTile &t, const CUtensorMa
     tc::fence_mbar_init();
   }
   __syncthreads();
+  // The first pass of an inner solve reads r alone: p' = r' = r / ||r|| needs no
+  // p, and d is written as 0 without being read.
   auto issue = [&](int s) {  // thread 0
     const int k = (s - c.s_lo) % kItStages;
     unsigned char *st = it_smem + k * kItStageBytes;
-    tc::mbar_expect_tx(&full[k], kItPBytes + kItRBytes + kItDBytes);
-    tma_load_3d(st, pmap, &full[k], x0 - 4, y0 - 2, s);
+    tc::mbar_expect_tx(&full[k], FIRST ? kItRBytes : kItPBytes + kItRBytes + kItDBytes);
+    if (!FIRST) tma_load_3d(st, pmap, &full[k], x0 - 4, y0 - 2, s);
     tma_load_3d(st + kItPBytes, rmap, &full[k], x0 - 4, y0 - 1, s - 1);
-    tma_load_3d(st + kItPBytes + kItRSlot, dmap, &full[k], x0, y0, s - 1);
+    if (!FIRST) tma_load_3d(st + kItPBytes + kItRSlot, dmap, &full[k], x0, y0, s - 1);
   };
   int next = c.s_lo;  // next plane to load (thread 0's view)
   if (tid == 0)
