@@ -876,3 +876,42 @@ extern "C" int hpccg_slab_group_cg(hpccg_slab *const *slabs, int32_t nslabs, con
   cleanup();
   return rc;
 }
+
+extern "C" int hpccg_slab_group_cg_host(hpccg_slab *const *slabs, int32_t nslabs, const double *const *b,
+                                        double *const *x, int32_t max_iter, double tolerance, int32_t *niters,
+                                        double *normr, double *resid_hist) {
+  if (!slabs || nslabs < 1 || !b || !x) return HPCCG_ERR_INVALID_ARG;
+  for (int32_t q = 0; q < nslabs; ++q)
+    if (!slabs[q] || !b[q] || !x[q]) return HPCCG_ERR_INVALID_ARG;
+  std::vector<double *> db(nslabs, nullptr), dx(nslabs, nullptr);
+  int rc = HPCCG_OK;
+  for (int32_t q = 0; q < nslabs && !rc; ++q) {
+    DevGuard dg(slabs[q]->device);
+    const size_t bytes = (size_t)slabs[q]->nrow * sizeof(double);
+    if (cudaMalloc(&db[q], bytes) != cudaSuccess || cudaMalloc(&dx[q], bytes) != cudaSuccess) {
+      cudaGetLastError();
+      rc = HPCCG_ERR_OOM;
+    } else if (cudaMemcpy(db[q], b[q], bytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+               cudaMemcpy(dx[q], x[q], bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+      rc = set_cuda_error(cudaGetLastError(), "slab group upload", __FILE__, __LINE__);
+    }
+  }
+  if (!rc) {
+    rc = hpccg_slab_group_cg(slabs, nslabs, db.data(), dx.data(), max_iter, tolerance, niters, normr, resid_hist);
+    if (rc == HPCCG_OK || rc == HPCCG_ERR_BREAKDOWN)
+      for (int32_t q = 0; q < nslabs; ++q) {
+        DevGuard dg(slabs[q]->device);
+        if (cudaMemcpy(x[q], dx[q], (size_t)slabs[q]->nrow * sizeof(double), cudaMemcpyDeviceToHost) !=
+            cudaSuccess) {
+          rc = set_cuda_error(cudaGetLastError(), "slab group download", __FILE__, __LINE__);
+          break;
+        }
+      }
+  }
+  for (int32_t q = 0; q < nslabs; ++q) {
+    DevGuard dg(slabs[q]->device);
+    cudaFree(db[q]);
+    cudaFree(dx[q]);
+  }
+  return rc;
+}

@@ -10,6 +10,7 @@
 //                       [--spmv KIND[,PARAM]] [--timing-level L] [--quiet]
 //                       [--precision fp64|fp32|bf16] [--rel-tol R]
 //   HPCCG-B200 --batch SPEC [--precision ...] [--rel-tol R] [--max-iter N] [--spmv 4]
+//   HPCCG-B200 nx ny nz --ranks P [--halo mpi|get] [--max-iter N] [--tol T] [--quiet]
 //
 // --precision fp32 or bf16 replaces the reference's fixed-count CG by the
 // FP64 iterative refinement around a low-precision inner CG
@@ -19,6 +20,12 @@
 // together (hpccg_batch_solve_host), each to --rel-tol; SPEC is a list
 // "nx,ny,nz/nx,ny,nz/..." or "random:COUNT,LO,HI,SEED" (each of nx, ny, nz
 // uniform in [LO, HI] from the project's generator, as the bench's batch).
+// --ranks P runs the reference's multi-rank problem (what `mpirun -np P` runs):
+// rank q owns the z slab q of the nx x ny x (nz P) grid (SparseMatrix.F90:68-185),
+// make_local_matrix's halo plan in the MPI form or, with --halo get, the CAF-V2
+// block form, and the reference's CG with rank-order dot sums; all P ranks run
+// in this process on the current GPU (hpccg_slab_group_cg_host), with the
+// report lines of the reference's rank 0.
 //
 // --timing-level follows the reference's TIMINGLEV (MPI/config.mk TIMER_LEVEL,
 // default 1; numerics.F90:100-156): 1 prints "TIMER: Total"; 2 adds one
@@ -175,6 +182,109 @@ static int run_batch(const std::vector<int32_t> &sizes, int precision, double re
   return rc == HPCCG_OK ? 0 : 3;
 }
 
+// --ranks: the reference's P-rank run, all ranks in this process.
+static int run_ranks(int nx, int ny, int nz, int nranks, int halo, int max_iter, double tolerance, bool quiet,
+                     int timing_level) {
+  const int64_t local = (int64_t)nx * ny * nz;
+  std::vector<std::vector<int32_t>> rows(nranks), cols(nranks);
+  std::vector<std::vector<double>> vals(nranks), x(nranks), b(nranks), xe(nranks);
+  std::vector<int64_t> nnz(nranks);
+  std::vector<int32_t> first((size_t)nranks + 1);
+  for (int q = 0; q <= nranks; ++q) first[q] = (int32_t)(local * q + 1);
+  std::vector<hpccg_slab_plan *> plans(nranks, nullptr);
+  int64_t total_nnz = 0;
+  for (int q = 0; q < nranks; ++q) {
+    rows[q].resize(local + 1);
+    cols[q].resize(27 * local);
+    vals[q].resize(27 * local);
+    x[q].resize(local);
+    b[q].resize(local);
+    xe[q].resize(local);
+    check(hpccg_generate_matrix_rank(nx, ny, nz, q, nranks, rows[q].data(), cols[q].data(), vals[q].data(),
+                                     x[q].data(), b[q].data(), xe[q].data(), &nnz[q]),
+          "generate_matrix_rank");
+    total_nnz += nnz[q];
+    check(hpccg_slab_plan_create((int32_t)local, nnz[q], rows[q].data(), cols[q].data(), nranks, q, first.data(),
+                                 halo, &plans[q]),
+          "slab_plan_create");
+  }
+  if (halo == HPCCG_HALO_MPI) {
+    // make_local_matrix's messages (SparseMatrix.F90:563-604): each rank learns, from every
+    // neighbour, the global ids that neighbour needs from it, in the neighbour's order
+    std::vector<std::vector<int32_t>> nbr(nranks), ext(nranks), own(nranks);
+    for (int q = 0; q < nranks; ++q) {
+      int32_t ne = 0, nn = 0, nb = 0, ts = 0;
+      check(hpccg_slab_plan_info(plans[q], &ne, &nn, &nb, &ts), "slab_plan_info");
+      nbr[q].resize(nn);
+      std::vector<int32_t> rl(nn);
+      check(hpccg_slab_plan_neighbors(plans[q], nbr[q].data(), rl.data()), "slab_plan_neighbors");
+      ext[q].resize(ne);
+      own[q].resize(ne);
+      check(hpccg_slab_plan_externals(plans[q], ext[q].data(), own[q].data()), "slab_plan_externals");
+    }
+    for (int q = 0; q < nranks; ++q) {
+      std::vector<int32_t> lens, ids;
+      for (int32_t n : nbr[q]) {
+        int32_t cnt = 0;
+        for (size_t i = 0; i < ext[n].size(); ++i)
+          if (own[n][i] == q) {
+            ids.push_back(ext[n][i]);
+            ++cnt;
+          }
+        lens.push_back(cnt);
+      }
+      static const int32_t none = 0;  // a non-null pointer for an empty list
+      check(hpccg_slab_plan_set_sends(plans[q], lens.empty() ? &none : lens.data(), ids.empty() ? &none : ids.data()),
+            "slab_plan_set_sends");
+    }
+  }
+  std::vector<hpccg_slab *> slabs(nranks, nullptr);
+  for (int q = 0; q < nranks; ++q) check(hpccg_slab_create(plans[q], vals[q].data(), &slabs[q]), "slab_create");
+
+  // printInfo of the reference's rank 0 (main.F90:58-71): total_nrow = P local_nrow, total_nnz = 27 total_nrow
+  printf(" HPCCG Benchmark\n");
+  printf(" Using double precision\n");
+  printf(" Total size (N x N): %12lld\n", (long long)(local * nranks));
+  printf(" Total nonzeroes: %12lld\n", (long long)(27 * local * nranks));
+  printf(" Ranks: %d z slabs in one process (halo %s), stored nonzeroes %lld\n", nranks,
+         halo == HPCCG_HALO_MPI ? "MPI send lists" : "CAF-V2 block gets", (long long)total_nnz);
+  printf(" OpenMP disabled.\n");
+  std::vector<const double *> bp(nranks);
+  std::vector<double *> xp(nranks);
+  for (int q = 0; q < nranks; ++q) {
+    bp[q] = b[q].data();
+    xp[q] = x[q].data();
+  }
+  std::vector<double> hist((size_t)max_iter + 1);
+  int32_t niters = 0;
+  double normr = 0.0;
+  const auto t0 = std::chrono::steady_clock::now();
+  const int rc = hpccg_slab_group_cg_host(slabs.data(), nranks, bp.data(), xp.data(), max_iter, tolerance, &niters,
+                                          &normr, hist.data());
+  const auto t1 = std::chrono::steady_clock::now();
+  if (rc != HPCCG_OK && rc != HPCCG_ERR_BREAKDOWN) check(rc, "slab_group_cg");
+  printf(" Initial Residual = %25.17g\n", hist[0]);
+  if (!quiet) {
+    int print_freq = max_iter / 10;
+    if (print_freq > 50) print_freq = 50;
+    if (print_freq < 1) print_freq = 1;
+    for (int k = 1; k <= niters; ++k)
+      if (k % print_freq == 0 || k + 1 == max_iter)
+        printf("ITER%5d  Residual%s\n", k, fortran_e(hist[k]).c_str());
+  }
+  if (rc == HPCCG_ERR_BREAKDOWN) printf(" CG breakdown after %d iterations\n", niters);
+  if (timing_level > 0) printf(" TIMER: Total %15.7g sec\n", std::chrono::duration<double>(t1 - t0).count());
+  double err = 0.0;
+  for (int q = 0; q < nranks; ++q)
+    for (int64_t i = 0; i < local; ++i) err = std::fmax(err, std::fabs(x[q][i] - xe[q][i]));
+  printf(" Iterations: %d  final normr: %.17g  max|x - xexact|: %.3e\n", niters, normr, err);
+  for (int q = 0; q < nranks; ++q) {
+    hpccg_slab_destroy(slabs[q]);
+    hpccg_slab_plan_destroy(plans[q]);
+  }
+  return rc == HPCCG_OK ? 0 : 3;
+}
+
 int main(int argc, char **argv) {
   int max_iter = 150;    // main.F90:127
   double tolerance = 0;  // main.F90:128
@@ -183,6 +293,7 @@ int main(int argc, char **argv) {
   int timing_level = 1;  // MPI/config.mk TIMER_LEVEL
   int spmv_kind = HPCCG_SPMV_AUTO, spmv_param = 0;
   int precision = HPCCG_PREC_FP64;
+  int nranks = 0, halo = HPCCG_HALO_MPI;
   const char *batch = nullptr;
   std::vector<int> pos;
   for (int i = 1; i < argc; ++i) {
@@ -193,6 +304,21 @@ int main(int argc, char **argv) {
     else if (!strcmp(argv[i], "--quiet")) quiet = true;
     else if (!strcmp(argv[i], "--timing-level") && i + 1 < argc) timing_level = atoi(argv[++i]);
     else if (!strcmp(argv[i], "--batch") && i + 1 < argc) batch = argv[++i];
+    else if (!strcmp(argv[i], "--ranks") && i + 1 < argc) {
+      nranks = atoi(argv[++i]);
+      if (nranks < 1) {
+        fprintf(stderr, "HPCCG-B200: --ranks must be positive\n");
+        return 2;
+      }
+    } else if (!strcmp(argv[i], "--halo") && i + 1 < argc) {
+      ++i;
+      if (!strcmp(argv[i], "mpi")) halo = HPCCG_HALO_MPI;
+      else if (!strcmp(argv[i], "get")) halo = HPCCG_HALO_GET;
+      else {
+        fprintf(stderr, "HPCCG-B200: --halo takes mpi or get\n");
+        return 2;
+      }
+    }
     else if (!strcmp(argv[i], "--precision") && i + 1 < argc) {
       precision = precision_code(argv[++i]);
       if (precision < 0) {
@@ -231,6 +357,7 @@ int main(int argc, char **argv) {
     fprintf(stderr, "HPCCG-B200: nx, ny, nz must be positive\n");
     return 2;
   }
+  if (nranks > 0) return run_ranks(nx, ny, nz, nranks, halo, max_iter, tolerance, quiet, timing_level);
   const int64_t n = (int64_t)nx * ny * nz;
   std::vector<double> x(n), b(n), xexact(n);
   hpccg_ctx *ctx = nullptr;

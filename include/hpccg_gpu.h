@@ -445,6 +445,12 @@ int hpccg_slab_cg_step(hpccg_slab *slab, int32_t step, int32_t k, const double *
  * GPU.  niters, normr and resid_hist as in hpccg_gpu_cg. */
 int hpccg_slab_group_cg(hpccg_slab *const *slabs, int32_t nslabs, const double *const *d_b, double *const *d_x,
                         int32_t max_iter, double tolerance, int32_t *niters, double *normr, double *resid_hist);
+/* The same with HOST arrays: b[q] and x[q] (in: x0, out: x) hold rank q's
+ * nrow rows.  The library copies them to each rank's GPU and back, as
+ * hpccg_gpu_cg does for one rank; the call a host driver of all the ranks makes. */
+int hpccg_slab_group_cg_host(hpccg_slab *const *slabs, int32_t nslabs, const double *const *b, double *const *x,
+                             int32_t max_iter, double tolerance, int32_t *niters, double *normr,
+                             double *resid_hist);
 
 /* ---- allocation-free entry point ---------------------------------------- */
 

@@ -228,3 +228,24 @@ def test_zero_rhs_edge_cases():
         d_x = torch.from_numpy(B.stack([np.ones(int(n)) for n in B.nrows])).cuda()  # zero gaps
         iters, relres, outer, rc = B.solve(d_b, d_x, prec, 1e-8, 40)
         assert rc == hp.HPCCG_ERR_NOT_CONVERGED and np.all(relres > 1e300), (prec, relres)
+
+
+@pytest.mark.parametrize("halo,mode", [("mpi", 0), ("get", 1)])
+@pytest.mark.parametrize("nx,ny,nz,P", [(8, 6, 4, 2), (6, 5, 4, 3)])
+def test_driver_ranks_prints_the_oracle_multi_rank_history(halo, mode, nx, ny, nz, P):
+    """--ranks P: the reference's P-rank run (z slabs of nx x ny x nz*P, make_local_matrix's plan in
+    the MPI or CAF-V2 form, rank-order sums), all ranks in one process; the report's sizes are the
+    reference's totals and the printed residuals are the oracle's multi-rank CG history."""
+    iters = 60
+    out = _run(nx, ny, nz, "--ranks", P, "--halo", halo, "--max-iter", iters)
+    N = nx * ny * nz * P
+    assert re.search(r"Total size \(N x N\):\s+%d$" % N, out, re.M)
+    assert re.search(r"Total nonzeroes:\s+%d$" % (27 * N), out, re.M)
+    _, x0, bg, _ = oracle.generate_matrix(nx, ny, nz * P)
+    rx, rit, rnr, rh = oracle.SlabPlan(nx, ny, nz, P, mode).cg(bg, x0, iters, 0.0)
+    got = _iters(out)
+    assert sorted(got) == sorted(set(range(6, iters + 1, 6)) | {iters - 1})
+    for k, v in got.items():
+        assert v == pytest.approx(rh[k], rel=1e-9, abs=1e-12 * rh[0]), (k, v, rh[k])
+    assert _field(r"Iterations: (\d+)", out, int) == rit
+    assert _field(r"max\|x - xexact\|: (\S+)$", out) <= 1e-10

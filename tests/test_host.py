@@ -87,6 +87,8 @@ def test_driver_built_and_prints_usage():
     (["8", "8", "8", "--precision", "fp16"], "--precision takes fp64, fp32 or bf16"),
     (["8", "8", "8", "--rel-tol", "0"], "--rel-tol must be positive"),
     (["8", "8", "8", "--frobnicate"], "unknown option"),
+    (["8", "8", "8", "--ranks", "0"], "--ranks must be positive"),
+    (["8", "8", "8", "--ranks", "2", "--halo", "shmem"], "--halo takes mpi or get"),
 ])
 def test_driver_rejects_bad_options_before_any_device_work(args, msg):
     """The driver's option errors exit with status 2 on the host (no GPU needed)."""
