@@ -218,13 +218,13 @@ static int forward(hpccg_unet *u, const float *in, float *out, bool train) {
   k_pool<<<grid1d(u, L[3].nvox * 2), 256, 0, u->stream>>>(u->e3b, u->d3, L[2].nx, L[2].ny, L[2].nz, u->nb);
   UNET_TRY(conv(u, 6, 3, u->d3, nullptr, nullptr, kEpiBiasRelu, u->e4a));
   UNET_TRY(conv(u, 7, 3, u->e4a, nullptr, nullptr, kEpiBiasRelu, u->e4b));
-  k_upsample<<<grid1d(u, L[2].nvox * 2), 256, 0, u->stream>>>(u->e4b, u->u3, L[2].nx, L[2].ny, L[2].nz, u->nb);
+  k_upsample<<<grid1d(u, L[2].nvox / 4), 256, 0, u->stream>>>(u->e4b, u->u3, L[2].nx, L[2].ny, L[2].nz, u->nb);
   UNET_TRY(conv(u, 8, 2, u->e3b, u->u3, nullptr, kEpiBiasRelu, u->c3a));
   UNET_TRY(conv(u, 9, 2, u->c3a, nullptr, nullptr, kEpiBiasRelu, u->c3b));
-  k_upsample<<<grid1d(u, L[1].nvox * 2), 256, 0, u->stream>>>(u->c3b, u->u2, L[1].nx, L[1].ny, L[1].nz, u->nb);
+  k_upsample<<<grid1d(u, L[1].nvox / 4), 256, 0, u->stream>>>(u->c3b, u->u2, L[1].nx, L[1].ny, L[1].nz, u->nb);
   UNET_TRY(conv(u, 10, 1, u->e2b, u->u2, nullptr, kEpiBiasRelu, u->c2a));
   UNET_TRY(conv(u, 11, 1, u->c2a, nullptr, nullptr, kEpiBiasRelu, u->c2b));
-  k_upsample<<<grid1d(u, L[0].nvox * 2), 256, 0, u->stream>>>(u->c2b, u->u1, L[0].nx, L[0].ny, L[0].nz, u->nb);
+  k_upsample<<<grid1d(u, L[0].nvox / 4), 256, 0, u->stream>>>(u->c2b, u->u1, L[0].nx, L[0].ny, L[0].nz, u->nb);
   if (train) {
     UNET_TRY(conv(u, 12, 0, u->e1b, u->u1, nullptr, kEpiBiasRelu, u->c1));
     k_proj_fwd<<<grid1d(u, L[0].nvox), 256, 0, u->stream>>>(u->c1, u->params + u->off[kNumLayers], out, L[0].nvox,

@@ -111,32 +111,36 @@ __device__ __forceinline__ void conv3_in1_body(const float *in, const float *W, 
     for (int j = 0; j < V; ++j)
 #pragma unroll
       for (int c = 0; c < 16; ++c) acc[j][c] = sw[27 * 16 + c];
+    // the nine (dz, dy) lines in turn; line li+1 is loaded while line li is used
+    float s[2][V + 2];
+    auto load_line = [&](int li, float *dst) {
+      const int dz = li / 3 - 1, dy = li % 3 - 1;
+      const bool line = (unsigned)(y + dy) < (unsigned)ny && (unsigned)(z + dz) < (unsigned)nz;
+      const float *p = in + v0 + (int64_t)dy * nx + (int64_t)dz * nx * ny;
 #pragma unroll
-    for (int dz = -1; dz <= 1; ++dz) {
+      for (int k = 0; k < V + 2; ++k) {
+        const int xx = x0 + k - 1;
+        dst[k] = (line && (unsigned)xx < (unsigned)nx) ? __ldg(p + k - 1) : 0.f;
+      }
+    };
+    load_line(0, s[0]);
 #pragma unroll
-      for (int dy = -1; dy <= 1; ++dy) {
-        const bool line = (unsigned)(y + dy) < (unsigned)ny && (unsigned)(z + dz) < (unsigned)nz;
-        const float *p = in + v0 + (int64_t)dy * nx + (int64_t)dz * nx * ny;
-        float s[V + 2];
+    for (int li = 0; li < 9; ++li) {
+      if (li + 1 < 9) load_line(li + 1, s[(li + 1) & 1]);
+      const float *sl = s[li & 1];
 #pragma unroll
-        for (int k = 0; k < V + 2; ++k) {
-          const int xx = x0 + k - 1;
-          s[k] = (line && (unsigned)xx < (unsigned)nx) ? __ldg(p + k - 1) : 0.f;
-        }
+      for (int dx = -1; dx <= 1; ++dx) {
+        const float4 *w4 = reinterpret_cast<const float4 *>(sw + (li * 3 + (dx + 1)) * 16);
 #pragma unroll
-        for (int dx = -1; dx <= 1; ++dx) {
-          const float4 *w4 = reinterpret_cast<const float4 *>(sw + ((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)) * 16);
+        for (int q = 0; q < 4; ++q) {
+          const float4 w = w4[q];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const float4 w = w4[q];
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-              const float a = s[j + dx + 1];
-              acc[j][4 * q] = fmaf(a, w.x, acc[j][4 * q]);
-              acc[j][4 * q + 1] = fmaf(a, w.y, acc[j][4 * q + 1]);
-              acc[j][4 * q + 2] = fmaf(a, w.z, acc[j][4 * q + 2]);
-              acc[j][4 * q + 3] = fmaf(a, w.w, acc[j][4 * q + 3]);
-            }
+          for (int j = 0; j < V; ++j) {
+            const float a = sl[j + dx + 1];
+            acc[j][4 * q] = fmaf(a, w.x, acc[j][4 * q]);
+            acc[j][4 * q + 1] = fmaf(a, w.y, acc[j][4 * q + 1]);
+            acc[j][4 * q + 2] = fmaf(a, w.z, acc[j][4 * q + 2]);
+            acc[j][4 * q + 3] = fmaf(a, w.w, acc[j][4 * q + 3]);
           }
         }
       }
@@ -214,18 +218,27 @@ __global__ void k_pool(const __nv_bfloat16 *in, __nv_bfloat16 *out, int nx, int 
     dst[e] = o;
   }
 }
-// Nearest-neighbour 2x upsampling: fine (nx,ny,nz) from coarse (nx/2,...).
+// Nearest-neighbour 2x upsampling: fine (nx,ny,nz) from coarse (nx/2,...).  One
+// thread per coarse 16-byte unit: one load, and its eight fine copies as two
+// adjacent units in each of the four fine rows (a warp writes 1 KB runs).
 __global__ void k_upsample(const __nv_bfloat16 *in, __nv_bfloat16 *out, int nx, int ny, int nz, int nb) {
   const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
-  const int64_t n = (int64_t)nx * ny * nz * nb * 2;
+  const int64_t n = (int64_t)cx * cy * cz * nb * 2;
   const uint4 *src = reinterpret_cast<const uint4 *>(in);
   uint4 *dst = reinterpret_cast<uint4 *>(out);
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
     int64_t row, b;
-    int h, x, z, y;
-    unit_coords(e, nx, &row, &h, &x);
-    row_coords(row, ny, nz, &b, &z, &y);
-    dst[e] = src[act_unit((b * cz + z / 2) * cy + y / 2, h, x / 2, cx)];
+    int h, xc, zc, yc;
+    unit_coords(e, cx, &row, &h, &xc);
+    row_coords(row, cy, cz, &b, &zc, &yc);
+    const uint4 v = src[e];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int64_t rf = (b * nz + 2 * zc + (k >> 1)) * ny + 2 * yc + (k & 1);
+      uint4 *d = dst + act_unit(rf, h, 2 * xc, nx);
+      d[0] = v;
+      d[1] = v;
+    }
   }
 }
 // Backward of pooling: d_fine += d_coarse / 8 (FP32 row-planar tensors).
