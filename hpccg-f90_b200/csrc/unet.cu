@@ -169,6 +169,9 @@ static int conv(hpccg_unet *u, int layer, int level, const __nv_bfloat16 *in0, c
     return launch_conv3_tc(nin, epi, a, u->num_sms, u->stream);
   }
   if (in_f32 && (epi == kEpiBiasRelu || epi == kEpiBias)) {  // the 1-channel input layer
+    if (Lv.nx % 128 == 0)  // tensor cores, 128-voxel row tiles
+      return launch_conv3_in1_tc(in_f32, W, bias, static_cast<__nv_bfloat16 *>(out), Lv.nx, Lv.ny, Lv.nz, u->nb,
+                                 epi == kEpiBiasRelu, u->d_err, u->num_sms, u->stream);
     if (Lv.nx % 4 == 0)
       k_conv3_in1x4<<<grid1d(u, Lv.nvox / 4), 256, 0, u->stream>>>(
           in_f32, W, bias, static_cast<__nv_bfloat16 *>(out), Lv.nx, Lv.ny, Lv.nz, u->nb, epi == kEpiBiasRelu);
@@ -535,8 +538,37 @@ extern "C" int hpccg_unet_time_forward(hpccg_unet *u, int32_t nx, int32_t ny, in
 extern "C" int hpccg_unet_conv3_layer(int32_t nx, int32_t ny, int32_t nz, int32_t nb, int32_t nin, const void *d_in0,
                                       const void *d_in1, const float *d_w, const float *d_bias, const float *d_proj,
                                       int32_t epi, int32_t path, void *d_out) {
-  if (nin < 1 || nin > 2 || !d_in0 || (nin == 2 && !d_in1) || !d_w || !d_out || epi < 0 || epi > 3)
+  if (nin < 0 || nin > 2 || !d_in0 || (nin == 2 && !d_in1) || !d_w || !d_out || epi < 0 || epi > 3)
     return HPCCG_ERR_INVALID_ARG;
+  if (nin == 0) {  // the 1-channel input layer: FP32 input [nb][nz][ny][nx], W [27][16]
+    if ((epi != kEpiBiasRelu && epi != kEpiBias) || !d_bias || (path != 0 && path != 1)) return HPCCG_ERR_INVALID_ARG;
+    int dev = 0, sms = 0;
+    HPCCG_CUDA(cudaGetDevice(&dev));
+    HPCCG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const float *in = static_cast<const float *>(d_in0);
+    __nv_bfloat16 *o = static_cast<__nv_bfloat16 *>(d_out);
+    const int relu = epi == kEpiBiasRelu;
+    int *d_err = nullptr;
+    HPCCG_CUDA(cudaMalloc(&d_err, sizeof(int)));
+    HPCCG_CUDA(cudaMemset(d_err, 0, sizeof(int)));
+    int rc = HPCCG_OK;
+    const int64_t nvox = (int64_t)nx * ny * nz * nb;
+    if (path == 0) {
+      rc = launch_conv3_in1_tc(in, d_w, d_bias, o, nx, ny, nz, nb, relu, d_err, sms, 0);
+    } else if (nx % 4 == 0) {
+      k_conv3_in1x4<<<(int)std::min<int64_t>((nvox / 4 + 255) / 256, (int64_t)sms * 16), 256>>>(in, d_w, d_bias, o,
+                                                                                              nx, ny, nz, nb, relu);
+    } else {
+      k_conv3_in1<<<(int)std::min<int64_t>((nvox + 255) / 256, (int64_t)sms * 16), 256>>>(in, d_w, d_bias, o, nx,
+                                                                                        ny, nz, nb, relu);
+    }
+    if (!rc && cudaDeviceSynchronize() != cudaSuccess) rc = set_cuda_error(cudaGetLastError(), "input layer", __FILE__, __LINE__);
+    int err = 0;
+    cudaMemcpy(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d_err);
+    if (!rc && err) rc = HPCCG_ERR_TIMEOUT;
+    return rc;
+  }
   if ((epi != kEpiRawF32 && !d_bias) || (epi == kEpiProject && !d_proj)) return HPCCG_ERR_INVALID_ARG;
   int dev = 0, sms = 0;
   HPCCG_CUDA(cudaGetDevice(&dev));

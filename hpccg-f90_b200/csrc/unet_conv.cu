@@ -482,6 +482,153 @@ __global__ void __launch_bounds__(kConvThreads * row_pipes(NIN, RX), 1) k_conv3_
   }
 }
 
+// ---- the 1-channel input layer on tcgen05 (nx a multiple of 128) -------------------------
+// An im2col GEMM per tile of 128 voxels of one x row: A[m][k] = in(x0+m+dx, y+dy, z+dz)
+// in BF16 for tap k = (dz+1)*9 + (dy+1)*3 + (dx+1) (k = 27..31 zero), B[c][k] = W[k][c];
+// two MMAs (M = 128, N = 16, K = 16) into a 16-column FP32 accumulator.  Thread m of
+// the CTA gathers its voxel's 27 inputs (for each tap the warp reads 32 consecutive
+// floats) into its A row; thread 0 issues the tile's MMAs; every warp then drains its
+// TMEM lane quarter of the PREVIOUS tile (bias, ReLU, BF16 stores), so a tile's MMAs
+// run while the next tile is gathered.  A and the accumulator are double-buffered.
+constexpr int kIn1Threads = 128;
+constexpr int kIn1ABytes = 4 * 128 * 16;  // [4 K chunks of 8 taps][128 rows][8 BF16]
+constexpr int kIn1BBytes = 4 * 16 * 16;   // [4 K chunks][16 output channels][8 BF16]
+
+__global__ void __launch_bounds__(kIn1Threads) k_conv3_in1_tc(const float *in, const float *W, const float *bias,
+                                                              __nv_bfloat16 *out, int nx, int ny, int nz, int nb,
+                                                              int relu, int *err) {
+  __shared__ __align__(1024) uint8_t sA[2][kIn1ABytes];
+  __shared__ __align__(128) uint8_t sB[kIn1BBytes];
+  __shared__ uint64_t done[2], fin;
+  __shared__ uint32_t slot;
+  __shared__ int s_fail;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int e = tid; e < 32 * 16; e += kIn1Threads) {  // B element (k, c): chunk k/8, row c, position k%8
+    const int k = e / 16, c = e % 16;
+    reinterpret_cast<__nv_bfloat16 *>(sB)[((k >> 3) * 16 + c) * 8 + (k & 7)] =
+        __float2bfloat16(k < 27 ? W[k * 16 + c] : 0.f);
+  }
+  float bc[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) bc[c] = bias[c];
+  if (tid == 0) {
+    mbar_init(&done[0], 1);
+    mbar_init(&done[1], 1);
+    mbar_init(&fin, 1);
+    fence_mbar_init();
+    s_fail = 0;
+  }
+  if (warp == 0) {
+    tmem_alloc(&slot, 32);
+    tmem_relinquish();
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = slot;
+  constexpr uint32_t idesc = idesc_bf16(128, 16);
+  const uint64_t bd = smem_desc(sB, 256, 128);
+  // tile t = ((b*nz + z)*ny + y)*tx + x-block; 32-bit indices (a grid has fewer than 2^31 tiles)
+  const int tx = nx / 128;
+  const int ntiles = tx * ny * nz * nb;
+  // the epilogue of tile t (buffer buf, its use u of that buffer): bias, ReLU, BF16 stores
+  auto drain = [&](int t, int buf, uint32_t use) {
+    if (!mbar_wait(&done[buf], use & 1u, err, 31)) s_fail = 1;
+    tc_fence_after();
+    float v[16];
+    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * 16), v);
+    tc_fence_before();
+    const int row = t / tx;
+    const int x = (t - row * tx) * 128 + tid;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      uint32_t w[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        float lo = v[8 * h + 2 * c] + bc[8 * h + 2 * c], hi = v[8 * h + 2 * c + 1] + bc[8 * h + 2 * c + 1];
+        if (relu) {
+          lo = fmaxf(lo, 0.f);
+          hi = fmaxf(hi, 0.f);
+        }
+        const __nv_bfloat162 pr = __floats2bfloat162_rn(lo, hi);
+        w[c] = *reinterpret_cast<const uint32_t *>(&pr);
+      }
+      *reinterpret_cast<uint4 *>(out + act_unit(row, h, x, nx) * 8) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  };
+  int it = 0, prev = -1;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+    const int buf = it & 1;
+    // gather this thread's voxel: 27 taps, zero outside the grid
+    const int row = t / tx;  // (b*nz + z)*ny + y
+    const int yz = row / ny, y = row - yz * ny;
+    const int bb = yz / nz, z = yz - bb * nz;
+    const int64_t bz = (int64_t)bb * nz;
+    const int x = (t - row * tx) * 128 + tid;
+    float v[32];
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy) {
+        const bool line = (unsigned)(z + dz) < (unsigned)nz && (unsigned)(y + dy) < (unsigned)ny;
+        const float *p = in + ((bz + z + dz) * ny + (y + dy)) * (int64_t)nx + x;
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx)
+          v[(dz + 1) * 9 + (dy + 1) * 3 + dx + 1] = (line && (unsigned)(x + dx) < (unsigned)nx) ? __ldg(p + dx) : 0.f;
+      }
+#pragma unroll
+    for (int k = 27; k < 32; ++k) v[k] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      uint32_t w[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const __nv_bfloat162 pr = __floats2bfloat162_rn(v[8 * c + 2 * j], v[8 * c + 2 * j + 1]);
+        w[j] = *reinterpret_cast<const uint32_t *>(&pr);
+      }
+      *reinterpret_cast<uint4 *>(sA[buf] + c * 2048 + (tid >> 3) * 128 + (tid & 7) * 16) =
+          make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    fence_proxy_async_smem();  // the A rows -> tensor-core proxy
+    tc_fence_before();
+    __syncthreads();  // every A row written; the drain of this buffer's last tile is done
+    tc_fence_after();
+    if (s_fail) break;  // read by every thread after the same barrier
+    if (tid == 0) {
+      const uint64_t ad = smem_desc(sA[buf], 2048, 128);
+      const uint32_t d = tmem + (uint32_t)(buf * 16);
+      mma_bf16(d, ad, bd, idesc, 0u);
+      mma_bf16(d, ad + (uint64_t)(4096 >> 4), bd + (uint64_t)(512 >> 4), idesc, 1u);
+      mma_commit(&done[buf]);
+    }
+    if (prev >= 0) drain(prev, buf ^ 1, (uint32_t)((it - 1) >> 1));
+    prev = t;
+  }
+  if (prev >= 0 && !s_fail) drain(prev, (it - 1) & 1, (uint32_t)((it - 1) >> 1));
+  if (tid == 0) {  // every MMA this thread issued has completed before TMEM is freed
+    mma_commit(&fin);
+    mbar_wait(&fin, 0, err, 32);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 32);
+  }
+}
+
+int launch_conv3_in1_tc(const float *in, const float *W, const float *bias, __nv_bfloat16 *out, int nx, int ny,
+                        int nz, int nb, int relu, int *err, int num_sms, cudaStream_t s) {
+  if (nx % 128 || ny < 1 || nz < 1 || nb < 1) return HPCCG_ERR_UNSUPPORTED;
+  const int64_t ntiles = (int64_t)(nx / 128) * ny * nz * nb;
+  if (ntiles >= ((int64_t)1 << 31)) return HPCCG_ERR_TOO_LARGE;
+  const int grid = (int)std::min<int64_t>(ntiles, (int64_t)num_sms * 8);
+  k_conv3_in1_tc<<<grid, kIn1Threads, 0, s>>>(in, W, bias, out, nx, ny, nz, nb, relu, err);
+  HPCCG_CUDA(cudaGetLastError());
+  return HPCCG_OK;
+}
+
 // RX = 0: brick tiles; 128 / 64: row tiles of that many voxels.
 template <int NIN, int EPI, int RX>
 static int launch_one(const ConvArgs &a, int num_sms, cudaStream_t s) {

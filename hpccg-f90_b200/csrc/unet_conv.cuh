@@ -137,5 +137,10 @@ inline bool conv_row64_geom(const ConvGeom &g, ConvGeom *r) {
 
 // Launches the tensor-core conv (row tiles when possible unless force_brick).
 int launch_conv3_tc(int nin, int epi, const ConvArgs &a, int num_sms, cudaStream_t s, bool force_brick = false);
+// The 1-channel input layer (FP32 input [nb][nz][ny][nx], W [27][16], bias [16])
+// on the tensor cores, BF16 operands, FP32 accumulation; nx a multiple of 128,
+// else HPCCG_ERR_UNSUPPORTED.
+int launch_conv3_in1_tc(const float *in, const float *W, const float *bias, __nv_bfloat16 *out, int nx, int ny,
+                        int nz, int nb, int relu, int *err, int num_sms, cudaStream_t s);
 
 }  // namespace hpccg

@@ -173,8 +173,17 @@ __global__ void __launch_bounds__(256, 2) k_conv3_in1x4(const float *in, const f
 }
 
 // ---- resampling (row-planar 16-channel tensors; fine dims nx, ny, nz even) -------------------
-// Decomposes a unit index of a row-planar tensor into (row, half, x).
+// Decomposes a unit index of a row-planar tensor into (row, half, x).  Indices
+// below 2^32 (every grid of fewer than 2^31 voxels) divide in 32 bits, several
+// times cheaper than the 64-bit division.
 __device__ __forceinline__ void unit_coords(int64_t u, int nx, int64_t *row, int *h, int *x) {
+  if ((uint64_t)u <= 0xFFFFFFFFull) {
+    const uint32_t uu = (uint32_t)u, t = uu / (uint32_t)nx;
+    *x = (int)(uu - t * (uint32_t)nx);
+    *h = (int)(t & 1u);
+    *row = (int64_t)(t >> 1);
+    return;
+  }
   *x = (int)(u % nx);
   const int64_t t = u / nx;
   *h = (int)(t & 1);
@@ -182,6 +191,13 @@ __device__ __forceinline__ void unit_coords(int64_t u, int nx, int64_t *row, int
 }
 // Row index of (b, z, y) and its inverse.
 __device__ __forceinline__ void row_coords(int64_t row, int ny, int nz, int64_t *b, int *z, int *y) {
+  if ((uint64_t)row <= 0xFFFFFFFFull) {
+    const uint32_t r = (uint32_t)row, t = r / (uint32_t)ny, bb = t / (uint32_t)nz;
+    *y = (int)(r - t * (uint32_t)ny);
+    *z = (int)(t - bb * (uint32_t)nz);
+    *b = (int64_t)bb;
+    return;
+  }
   *y = (int)(row % ny);
   const int64_t t = row / ny;
   *z = (int)(t % nz);

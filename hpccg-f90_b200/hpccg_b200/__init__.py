@@ -523,10 +523,12 @@ class Batch:
         return ms.value
 
 
-def conv3_layer(d_in0, d_in1, d_w, d_bias, d_proj, epi: int, path: int, d_out, nx, ny, nz, nb=1):
-    """One 3x3x3 conv with 16 outputs (test entry): torch device tensors, BF16 inputs."""
+def conv3_layer(d_in0, d_in1, d_w, d_bias, d_proj, epi: int, path: int, d_out, nx, ny, nz, nb=1, nin=None):
+    """One 3x3x3 conv with 16 outputs (test entry): torch device tensors, BF16 inputs;
+    nin = 0: the 1-channel input layer on an FP32 grid."""
     _sync_torch()
-    nin = 1 if d_in1 is None else 2
+    if nin is None:
+        nin = 1 if d_in1 is None else 2
     p = lambda t: None if t is None else _dptr(t)  # noqa: E731
     _check(_lib.hpccg_unet_conv3_layer(nx, ny, nz, nb, nin, p(d_in0), p(d_in1), p(d_w), p(d_bias), p(d_proj), epi,
                                        path, p(d_out)), "conv3_layer")

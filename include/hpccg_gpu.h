@@ -274,7 +274,10 @@ int hpccg_unet_time_forward(hpccg_unet *unet, int32_t nx, int32_t ny, int32_t nz
  * epi 0 = bias+ReLU (BF16 out), 1 = bias (BF16), 2 = bias+ReLU then the 16->1
  * projection d_proj (FP32 out), 3 = raw FP32 16-channel out; path 0 =
  * tcgen05 (row tiles when nx is a multiple of 128), 1 = CUDA cores,
- * 2 = tcgen05 with brick tiles (per-tap fetches). */
+ * 2 = tcgen05 with brick tiles (per-tap fetches).  nin = 0 is the network's
+ * 1-channel input layer: d_in0 an FP32 grid [b][z][y][x], weights FP32 [27][16],
+ * epi 0 or 1; path 0 = tcgen05 (nx a multiple of 128, else
+ * HPCCG_ERR_UNSUPPORTED), 1 = CUDA cores. */
 int hpccg_unet_conv3_layer(int32_t nx, int32_t ny, int32_t nz, int32_t nb, int32_t nin, const void *d_in0,
                            const void *d_in1, const float *d_w, const float *d_bias, const float *d_proj,
                            int32_t epi, int32_t path, void *d_out);

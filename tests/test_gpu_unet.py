@@ -77,6 +77,37 @@ def test_conv_layer_tc_and_cc(env, nx, ny, nz, nb, nin, epi):
         assert np.all(np.abs(got - want) <= tol), (path, np.abs(got - want).max(), scale)
 
 
+@pytest.mark.parametrize("nx,ny,nz,nb", [(128, 4, 2, 1), (256, 3, 5, 2), (128, 1, 1, 1), (64, 4, 4, 1)])
+@pytest.mark.parametrize("epi", [0, 1])
+def test_input_layer_tc_and_cc(env, nx, ny, nz, nb, epi):
+    """The 1-channel input layer: tcgen05 (BF16 input and weights rounded as the kernel rounds them,
+    FP32 accumulation; 128-voxel rows) and CUDA cores (FP32) against the oracle conv, within the
+    bars of the 16-channel layers; grids whose nx is not a multiple of 128 have no tensor-core path."""
+    torch, hp = env
+    rng = np.random.default_rng(nx * 7 + ny + epi)
+    x = rng.normal(0, 1, (nb, nz, ny, nx)).astype(np.float32)
+    W = rng.normal(0, 0.2, (27, 1, 16)).astype(np.float32)
+    b = rng.normal(0, 0.1, 16).astype(np.float32)
+    dW, db = torch.from_numpy(W).cuda(), torch.from_numpy(b).cuda()
+    din = torch.from_numpy(x).cuda()
+    for path in (0, 1):
+        xr, Wr = (uo.bf16_round(x), uo.bf16_round(W)) if path == 0 else (x, W)
+        want = uo.conv3(xr[..., None].astype(np.float64), Wr.astype(np.float64)) + b
+        if epi == 0:
+            want = np.maximum(want, 0)
+        out = torch.empty((nb, nz, ny, 2, nx, 8), dtype=torch.bfloat16, device="cuda")
+        if path == 0 and nx % 128:
+            with pytest.raises(hp.HpccgError) as e:
+                hp.conv3_layer(din, None, dW, db, None, epi, path, out, nx, ny, nz, nb, nin=0)
+            assert e.value.code == hp.HPCCG_ERR_UNSUPPORTED
+            continue
+        hp.conv3_layer(din, None, dW, db, None, epi, path, out, nx, ny, nz, nb, nin=0)
+        got = from_planar(out.float().cpu().numpy().astype(np.float64))
+        scale = np.abs(want).max() + 1e-30
+        tol = 1e-3 * scale + 2.0 ** -8 * np.abs(want)
+        assert np.all(np.abs(got - want) <= tol), (path, np.abs(got - want).max(), scale)
+
+
 def _net_and_params(hp, seed=3):
     net = hp.Unet(seed)
     p = net.get_params().astype(np.float64)
