@@ -485,20 +485,48 @@ __global__ void __launch_bounds__(kConvThreads * row_pipes(NIN, RX), 1) k_conv3_
 // ---- the 1-channel input layer on tcgen05 (nx a multiple of 128) -------------------------
 // An im2col GEMM per tile of 128 voxels of one x row: A[m][k] = in(x0+m+dx, y+dy, z+dz)
 // in BF16 for tap k = (dz+1)*9 + (dy+1)*3 + (dx+1) (k = 27..31 zero), B[c][k] = W[k][c];
-// two MMAs (M = 128, N = 16, K = 16) into a 16-column FP32 accumulator.  Thread m of
-// the CTA gathers its voxel's 27 inputs (for each tap the warp reads 32 consecutive
-// floats) into its A row; thread 0 issues the tile's MMAs; every warp then drains its
-// TMEM lane quarter of the PREVIOUS tile (bias, ReLU, BF16 stores), so a tile's MMAs
-// run while the next tile is gathered.  A and the accumulator are double-buffered.
+// two MMAs (M = 128, N = 16, K = 16) into a 16-column FP32 accumulator.  A CTA walks a
+// contiguous range of tiles.  The tile's nine input lines (dz, dy), x0-1 .. x0+128 with
+// zeros outside the grid, are staged once in shared memory: each thread loads one element
+// of every line a tile ahead into registers and stores them while the current tile is
+// built.  Thread m then reads its voxel's 27 taps from the staged lines into its A row;
+// thread 0 issues the tile's MMAs; every warp drains its TMEM lane quarter of the PREVIOUS
+// tile (bias, ReLU, BF16 stores), so a tile's MMAs run while the next tile is built.  The
+// staged lines, A and the accumulator are double-buffered: one barrier per tile.
 constexpr int kIn1Threads = 128;
 constexpr int kIn1ABytes = 4 * 128 * 16;  // [4 K chunks of 8 taps][128 rows][8 BF16]
 constexpr int kIn1BBytes = 4 * 16 * 16;   // [4 K chunks][16 output channels][8 BF16]
+constexpr int kIn1Line = 132;             // a staged line: x0-1+i at [i], i < 130
+
+// tile coordinates in tile order: row = (b*nz + z)*ny + y, x block xb (tile = row*tx + xb)
+struct In1Tile {
+  int row, xb, y, z;
+  __device__ __forceinline__ void at(int t, int tx, int ny, int nz) {
+    row = t / tx;
+    xb = t - row * tx;
+    const int yz = row / ny;
+    y = row - yz * ny;
+    z = yz % nz;
+  }
+  __device__ __forceinline__ void next(int tx, int ny, int nz) {
+    if (++xb == tx) {
+      xb = 0;
+      ++row;
+      if (++y == ny) {
+        y = 0;
+        if (++z == nz) z = 0;
+      }
+    }
+  }
+};
 
 __global__ void __launch_bounds__(kIn1Threads) k_conv3_in1_tc(const float *in, const float *W, const float *bias,
                                                               __nv_bfloat16 *out, int nx, int ny, int nz, int nb,
                                                               int relu, int *err) {
   __shared__ __align__(1024) uint8_t sA[2][kIn1ABytes];
   __shared__ __align__(128) uint8_t sB[kIn1BBytes];
+  __shared__ __align__(16) float sL[2][9 * kIn1Line];
+  __shared__ __align__(16) float sBias[16];
   __shared__ uint64_t done[2], fin;
   __shared__ uint32_t slot;
   __shared__ int s_fail;
@@ -508,9 +536,45 @@ __global__ void __launch_bounds__(kIn1Threads) k_conv3_in1_tc(const float *in, c
     reinterpret_cast<__nv_bfloat16 *>(sB)[((k >> 3) * 16 + c) * 8 + (k & 7)] =
         __float2bfloat16(k < 27 ? W[k * 16 + c] : 0.f);
   }
-  float bc[16];
+  if (tid < 16) sBias[tid] = bias[tid];
+  // tile t = ((b*nz + z)*ny + y)*tx + x-block; 32-bit indices (a grid has fewer than 2^31 tiles)
+  const int tx = nx / 128;
+  const int ntiles = tx * ny * nz * nb;
+  const int t_lo = (int)((int64_t)blockIdx.x * ntiles / gridDim.x);
+  const int t_hi = (int)((int64_t)(blockIdx.x + 1) * ntiles / gridDim.x);
+  // this thread's element of each staged line (x0 + tid), and for threads 0..8 / 32..40
+  // the left / right halo element (x0 - 1 / x0 + 128) of line hl
+  const int hl = tid < 9 ? tid : (tid >= 32 && tid < 41 ? tid - 32 : -1);
+  const int hx = tid < 32 ? -1 : 128;
+  float ld[9], lh = 0.f;
+  In1Tile L, D;  // the next tile to load, the next tile to drain
+  L.at(t_lo, tx, ny, nz);
+  D = L;
+  auto load = [&](bool live) {
+    const int x0 = L.xb * 128;
 #pragma unroll
-  for (int c = 0; c < 16; ++c) bc[c] = bias[c];
+    for (int l = 0; l < 9; ++l) {
+      const int dz = l / 3 - 1, dy = l % 3 - 1;
+      const bool ok = live && (unsigned)(L.z + dz) < (unsigned)nz && (unsigned)(L.y + dy) < (unsigned)ny;
+      ld[l] = ok ? __ldg(in + (int64_t)(L.row + dz * ny + dy) * nx + x0 + tid) : 0.f;
+    }
+    if (hl >= 0) {
+      const int dz = hl / 3 - 1, dy = hl % 3 - 1, xh = x0 + hx;
+      const bool ok = live && (unsigned)(L.z + dz) < (unsigned)nz && (unsigned)(L.y + dy) < (unsigned)ny &&
+                      (unsigned)xh < (unsigned)nx;
+      lh = ok ? __ldg(in + (int64_t)(L.row + dz * ny + dy) * nx + xh) : 0.f;
+    }
+    L.next(tx, ny, nz);
+  };
+  auto stage = [&](int sb) {
+    float *s = sL[sb];
+#pragma unroll
+    for (int l = 0; l < 9; ++l) s[l * kIn1Line + tid + 1] = ld[l];
+    if (hl >= 0) s[hl * kIn1Line + hx + 1] = lh;
+  };
+  load(t_lo < t_hi);
+  stage(0);
+  load(t_lo + 1 < t_hi);
   if (tid == 0) {
     mbar_init(&done[0], 1);
     mbar_init(&done[1], 1);
@@ -524,29 +588,28 @@ __global__ void __launch_bounds__(kIn1Threads) k_conv3_in1_tc(const float *in, c
   }
   fence_proxy_async_smem();
   tc_fence_before();
-  __syncthreads();
+  __syncthreads();  // B, the bias, the first tile's lines, the barriers and the TMEM slot
   tc_fence_after();
   const uint32_t tmem = slot;
   constexpr uint32_t idesc = idesc_bf16(128, 16);
   const uint64_t bd = smem_desc(sB, 256, 128);
-  // tile t = ((b*nz + z)*ny + y)*tx + x-block; 32-bit indices (a grid has fewer than 2^31 tiles)
-  const int tx = nx / 128;
-  const int ntiles = tx * ny * nz * nb;
-  // the epilogue of tile t (buffer buf, its use u of that buffer): bias, ReLU, BF16 stores
-  auto drain = [&](int t, int buf, uint32_t use) {
+  // the epilogue of tile D (buffer buf, its use u of that buffer): bias, ReLU, BF16 stores
+  auto drain = [&](int buf, uint32_t use) {
     if (!mbar_wait(&done[buf], use & 1u, err, 31)) s_fail = 1;
     tc_fence_after();
     float v[16];
     tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * 16), v);
     tc_fence_before();
-    const int row = t / tx;
-    const int x = (t - row * tx) * 128 + tid;
+    const int x = D.xb * 128 + tid;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
+      const float4 b0 = *reinterpret_cast<const float4 *>(sBias + 8 * h);
+      const float4 b1 = *reinterpret_cast<const float4 *>(sBias + 8 * h + 4);
+      const float bc[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
       uint32_t w[4];
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
-        float lo = v[8 * h + 2 * c] + bc[8 * h + 2 * c], hi = v[8 * h + 2 * c + 1] + bc[8 * h + 2 * c + 1];
+        float lo = v[8 * h + 2 * c] + bc[2 * c], hi = v[8 * h + 2 * c + 1] + bc[2 * c + 1];
         if (relu) {
           lo = fmaxf(lo, 0.f);
           hi = fmaxf(hi, 0.f);
@@ -554,29 +617,20 @@ __global__ void __launch_bounds__(kIn1Threads) k_conv3_in1_tc(const float *in, c
         const __nv_bfloat162 pr = __floats2bfloat162_rn(lo, hi);
         w[c] = *reinterpret_cast<const uint32_t *>(&pr);
       }
-      *reinterpret_cast<uint4 *>(out + act_unit(row, h, x, nx) * 8) = make_uint4(w[0], w[1], w[2], w[3]);
+      *reinterpret_cast<uint4 *>(out + act_unit(D.row, h, x, nx) * 8) = make_uint4(w[0], w[1], w[2], w[3]);
     }
+    D.next(tx, ny, nz);
   };
-  int it = 0, prev = -1;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+  int it = 0;
+  for (int t = t_lo; t < t_hi; ++t, ++it) {
     const int buf = it & 1;
-    // gather this thread's voxel: 27 taps, zero outside the grid
-    const int row = t / tx;  // (b*nz + z)*ny + y
-    const int yz = row / ny, y = row - yz * ny;
-    const int bb = yz / nz, z = yz - bb * nz;
-    const int64_t bz = (int64_t)bb * nz;
-    const int x = (t - row * tx) * 128 + tid;
+    // this thread's voxel: 27 taps from the staged lines
+    const float *s = sL[buf] + tid;
     float v[32];
 #pragma unroll
-    for (int dz = -1; dz <= 1; ++dz)
+    for (int l = 0; l < 9; ++l)
 #pragma unroll
-      for (int dy = -1; dy <= 1; ++dy) {
-        const bool line = (unsigned)(z + dz) < (unsigned)nz && (unsigned)(y + dy) < (unsigned)ny;
-        const float *p = in + ((bz + z + dz) * ny + (y + dy)) * (int64_t)nx + x;
-#pragma unroll
-        for (int dx = -1; dx <= 1; ++dx)
-          v[(dz + 1) * 9 + (dy + 1) * 3 + dx + 1] = (line && (unsigned)(x + dx) < (unsigned)nx) ? __ldg(p + dx) : 0.f;
-      }
+      for (int dx = 0; dx < 3; ++dx) v[l * 3 + dx] = s[l * kIn1Line + dx];
 #pragma unroll
     for (int k = 27; k < 32; ++k) v[k] = 0.f;
 #pragma unroll
@@ -590,9 +644,11 @@ __global__ void __launch_bounds__(kIn1Threads) k_conv3_in1_tc(const float *in, c
       *reinterpret_cast<uint4 *>(sA[buf] + c * 2048 + (tid >> 3) * 128 + (tid & 7) * 16) =
           make_uint4(w[0], w[1], w[2], w[3]);
     }
+    stage(buf ^ 1);        // tile t+1's lines: that buffer was last read before the previous barrier
+    load(t + 2 < t_hi);    // tile t+2's elements, in flight until the next iteration's stage
     fence_proxy_async_smem();  // the A rows -> tensor-core proxy
     tc_fence_before();
-    __syncthreads();  // every A row written; the drain of this buffer's last tile is done
+    __syncthreads();  // A and the next lines written; the drain of this buffer's last tile is done
     tc_fence_after();
     if (s_fail) break;  // read by every thread after the same barrier
     if (tid == 0) {
@@ -602,10 +658,9 @@ __global__ void __launch_bounds__(kIn1Threads) k_conv3_in1_tc(const float *in, c
       mma_bf16(d, ad + (uint64_t)(4096 >> 4), bd + (uint64_t)(512 >> 4), idesc, 1u);
       mma_commit(&done[buf]);
     }
-    if (prev >= 0) drain(prev, buf ^ 1, (uint32_t)((it - 1) >> 1));
-    prev = t;
+    if (it > 0) drain(buf ^ 1, (uint32_t)((it - 1) >> 1));
   }
-  if (prev >= 0 && !s_fail) drain(prev, (it - 1) & 1, (uint32_t)((it - 1) >> 1));
+  if (it > 0 && !s_fail) drain((it - 1) & 1, (uint32_t)((it - 1) >> 1));
   if (tid == 0) {  // every MMA this thread issued has completed before TMEM is freed
     mma_commit(&fin);
     mbar_wait(&fin, 0, err, 32);
