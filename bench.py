@@ -225,6 +225,24 @@ def cpu_reference_time(n: int, solves: int, warmup: int, solves_1thread: int = 1
             "per_solve_1thread_s": per_solve_1t, "iters_1thread": iters_1t}
 
 
+def _host_cpu():
+    """The host's CPU model, logical CPUs and the CPUs this process may run on."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        usable = os.cpu_count()
+    return {"cpu_model": model, "nproc": usable, "logical_cpus": os.cpu_count()}
+
+
 def _cpu_sample(r, n):
     s = (f"whole solves to FP64 rel-res 1e-8 of the C restatement of MPI/src CG at {n}^3 ({r['iters']} iterations, "
          f"true rel-res {r['relres']:.2e}): median of {len(r['per_solve_s'])} on {r['cores']} OpenMP threads")
@@ -255,7 +273,7 @@ def run_reference(args):
                    "reference_build": "unavailable (Fortran 90; no Fortran compiler in this image) -> C restatement of MPI/src",
                    "iterations": r["iters"], "per_solve_s": r["per_solve_s"]},
         "cpu_baseline": {"value": r["value"], "unit": "s", "cores": r["cores"], "kind": "port",
-                         "sample": _cpu_sample(r, args.n), "value_1thread": r["value_1thread"]},
+                         "sample": _cpu_sample(r, args.n), "value_1thread": r["value_1thread"], **_host_cpu()},
         "e2e": {"value": r["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -588,7 +606,8 @@ def run_ours(args):
     if not args.no_cpu_baseline and cubic:
         c = cpu_reference_time(n, 3, 1, args.ref_1thread_solves)
         cpu = {"value": c["value"], "unit": "s", "cores": c["cores"], "kind": "port",
-               "value_1thread": c["value_1thread"], "iterations": c["iters"], "sample": _cpu_sample(c, n)}
+               "value_1thread": c["value_1thread"], "iterations": c["iters"], "sample": _cpu_sample(c, n),
+               **_host_cpu()}
     hr = results[head]
     line = {
         "metric": METRIC, "value": hr["ms"] / 1e3, "unit": "s", "n_gpus": ws, "steps": args.steps,

@@ -22,6 +22,7 @@ def test_reference_arm_prints_one_contract_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == d["value"]
     assert cb["value_1thread"] > 0 and "whole solves" in cb["sample"]
+    assert cb["nproc"] >= 1 and cb["logical_cpus"] >= cb["nproc"] and "cpu_model" in cb
     assert d["e2e"] == {"value": d["value"], "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["config"]["iterations"] > 0
 
