@@ -34,6 +34,17 @@ def test_library_exports_every_declared_symbol():
     assert set(hp.exported_symbols()) <= set(declared)
 
 
+def test_integration_table_names_every_entry_point():
+    """The integration guide's entry-point table names every function the header
+    declares: by its exact name, as a call, or through a `prefix*` group."""
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    table = text[text.index("## Which reference interface"):text.index("## Fortran 90 host")]
+    named = set(re.findall(r"`(hpccg_\w+)[`(]", table))
+    groups = set(re.findall(r"`(hpccg_\w+?)\*`", table))
+    missing = [d for d in _declared_functions() if d not in named and not any(d.startswith(g) for g in groups)]
+    assert not missing, missing
+
+
 def test_library_is_sm100a_only():
     out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", hp.LIB_PATH], capture_output=True,
                          text=True).stdout
