@@ -14,7 +14,7 @@
 //         per system at ||r|| <= rel_tol ||b||), then an FP64 true residual.
 //   FP32 / BF16: per-system FP64 iterative refinement around an inner CG in
 //         FP32 vectors and FP32 / BF16 values (as hpccg_mixed.cu), with the
-//         FP64 true residual as the judge of every system.
+//         FP64 true residual as the stop test of every system.
 // Batches built by hpccg_batch_create_generated may switch to matrix-free
 // rows (hpccg_batch_set_spmv, HPCCG_SPMV_STENCIL): each row is formed from the
 // system's own grid with the reference's term order (hpccg_stencil.cuh), so

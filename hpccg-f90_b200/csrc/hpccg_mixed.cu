@@ -6,7 +6,7 @@
 // Inner CG (FP32 vectors; FP32 or BF16 copies of A's values; FP32 row sums;
 // FP64 dot-product accumulation) stops at ||r_in|| <= target ||r_in,0|| where
 // target = inner_rtol, or adaptively max(floor, 0.5 rel_tol ||b|| / ||r||).
-// The FP64 true residual is the judge: the solve only reports success when
+// The FP64 true residual decides: the solve only reports success when
 // the FP64 residual meets rel_tol.
 //
 // One CUDA graph: bnorm, residual64, while(outer){ start_inner,

@@ -4,7 +4,7 @@
 //
 // Outer loop, FP64 on the device: r = b - A x with the context's FP64 SpMV
 // (reference term order), stop when ||r|| <= rel_tol ||b|| -- the FP64 true
-// residual is the only judge -- else solve A d = r / ||r|| with the inner
+// residual alone decides -- else solve A d = r / ||r|| with the inner
 // solver and update x += ||r|| d in FP64.
 //
 // Inner solver, FP32 vectors (dot products accumulated in FP64): flexible CG

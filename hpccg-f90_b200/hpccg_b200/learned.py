@@ -124,7 +124,7 @@ def train_preconditioner(n: int = 64, seed: int = 1, rhs: int = 64, rounds: int 
                          batch: int = 4, lr: float = 2e-3, log=None):
     """Train the U-Net as an FCG preconditioner on n^3 grids.
 
-    Round 0 learns from plain-CG residual->error pairs of `rhs` Gaussian random
+    Training round 0 learns from plain-CG residual->error pairs of `rhs` Gaussian random
     field right-hand sides; each further round adds pairs from FCG runs with
     the current network.  Loss: energy norm of the HPCCG operator."""
     import torch

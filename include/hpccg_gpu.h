@@ -123,7 +123,7 @@ int hpccg_gpu_cg_device(hpccg_ctx *ctx, const double *d_b, double *d_x, int32_t 
  * residual instead of the reference's fixed iteration count.  The outer loop
  * is FP64 on the device: r = b - A x with the FP64 values (bit-exact
  * reference SpMV), stop when ||r||_2 <= rel_tol ||b||_2 (the FP64 true
- * residual is the only convergence judge), else solve A d = r/||r|| with an
+ * residual alone decides convergence), else solve A d = r/||r|| with an
  * inner CG in FP32 vectors and FP32 (HPCCG_PREC_FP32) or BF16
  * (HPCCG_PREC_BF16) copies of A's values, row sums accumulated in FP32, and
  * update x += ||r|| d in FP64.  The inner CG stops at ||r_in|| <= inner_rtol

@@ -83,7 +83,7 @@ int orc_cg_work(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
 /* MPI/src/numerics.F90:164-198 compute_residual: max_i |v1(i)-v2(i)|. */
 double orc_compute_residual(int32_t n, const double *v1, const double *v2);
 
-/* ||b - A x||_2 / ||b||_2 in sequential FP64 (the convergence judge). */
+/* ||b - A x||_2 / ||b||_2 in sequential FP64 (the convergence criterion). */
 double orc_true_relres(int32_t nrow, const int32_t *rowindex, const int32_t *colindex,
                        const double *values, const double *b, const double *x);
 

@@ -173,7 +173,7 @@ def test_trained_network_reduces_fcg_iterations(env):
             assert fcg.relres <= 1e-8 and plain.relres <= 1e-8
             assert fcg.iters <= 0.6 * plain.iters, (n, sd, fcg.iters, plain.iters)
             # the same network inside mixed precision: FP32 flexible CG in FP64 refinement,
-            # against plain FP32 CG through the same solver; the oracle judges the result
+            # against plain FP32 CG through the same solver; the oracle checks the result
             bh = b.cpu().numpy()
             runs = {}
             for name, nn in (("plain", None), ("learned", net)):
