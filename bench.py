@@ -620,7 +620,9 @@ def run_ours(args):
                    "method": head, "speedup_vs_plain_gpu_cg": plain_ms / hr["ms"],
                    "speedup_vs_plain_gpu_cg_stencil": results["fp64_cg_stencil"]["ms"] / hr["ms"],
                    "methods": results, "learned": learned_info, "batch": batch_info,
-                   "l2": "inputs (5.4 GB matrix) exceed the 126 MB L2; no flush",
+                   "l2": f"every pass streams more than the 126 MB L2 (the vectors alone: {N} rows x 8 B = "
+                         f"{8 * N / 1e6:.0f} MB in FP64; the matrix-free inner pass moves 24 B a row, the stored "
+                         f"matrix {(12 * nnz + 4 * (N + 1)) / 1e9:.1f} GB); no flush",
                    "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
                    "spmv_kernel": results[head]["spmv_kernel"]},
         "roofline": roofs[head], "roofline_all": roofs,
