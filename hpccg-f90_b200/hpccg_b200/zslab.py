@@ -269,18 +269,25 @@ class DistCG:
     dot products by an all-gather folded in rank order.  With the gloo backend the device
     vectors are staged through host memory."""
 
-    def __init__(self, slab: Slab, plan: SlabPlan, group=None, get_ranges=None):
+    def __init__(self, slab: Slab, plan: SlabPlan, group=None, get_ranges=None, device=None):
+        """device: where the slab's vectors live, by default the current CUDA device (the
+        library's Slab).  The transport works on any torch device: a slab object whose steps
+        keep their vectors in host memory passes device="cpu"."""
         import torch
         import torch.distributed as dist
 
         self.torch, self.dist = torch, dist
         self.slab, self.group = slab, group
-        self.dev = torch.device("cuda", torch.cuda.current_device())
-        self.host_staged = dist.get_backend(group) != "nccl"
+        self.dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.host_staged = self.dev.type == "cuda" and dist.get_backend(group) != "nccl"
         self.get_ranges = get_ranges or {}  # GET form: {requester: [(inmin, inmax), ..]}
         self.P = slab.nranks
         if slab.mode == HALO_MPI:
             self.sendbuf = torch.zeros(max(1, slab.nsend), dtype=torch.float64, device=self.dev)
+
+    def _sync(self):
+        if self.dev.type == "cuda":
+            self.torch.cuda.synchronize()
 
     def _xfer(self, sends, recvs):
         """sends: [(peer, tensor)], recvs: [(peer, tensor)]; device tensors, staged if needed."""
@@ -298,7 +305,7 @@ class DistCG:
                 w.wait()
         for t, buf in post:
             t.copy_(buf)
-        torch.cuda.synchronize()
+        self._sync()
 
     def exchange(self, d_p):
         s = self.slab
@@ -333,7 +340,7 @@ class DistCG:
         for q in range(1, self.P):
             s = s + out[q]
         d_state[GLOBAL:GLOBAL + 1].copy_(s.to(self.dev))
-        torch.cuda.synchronize()
+        self._sync()
 
     def solve(self, d_b, d_x, max_iter: int = 150, tolerance: float = 0.0):
         """Returns (niters, normr, hist); d_x is updated in place."""

@@ -11,6 +11,10 @@
   their requests through torch.distributed as the reference's ranks do
   through MPI.
 - The oracle's multi-rank CG against its single-rank CG on the stacked grid.
+- DistCG's transport (halo messages, rank-order sums of the dot products) on
+  gloo ranks of world sizes 2 and 3, each rank's CG steps in host memory
+  (HostSlab, a restatement of the step contract): the whole solve equals the
+  oracle's multi-rank CG bit for bit.
 - The reference's block-length count (:533-545), restated literally, is one
   too large for every block but the last: right for two ranks, off by one for
   the middle ranks of three -- the reason the plans use the block sizes.
@@ -189,3 +193,145 @@ def test_plans_over_gloo_ranks(tmp_path, nx, ny, nz, P, mode):
             want = sorted((q, int(lo), int(hi)) for q in range(P) for own, _s, lo, hi in ref.get(q, "blocks")
                           if own == r)
             np.testing.assert_array_equal(got["served"], np.array(want, np.int32).reshape(-1, 3))
+
+
+# ---- DistCG's transport on gloo ranks, with the CG steps in host memory -------
+
+class HostSlab:
+    """One rank's CG steps in host memory, restating the contract of hpccg_slab_cg_step,
+    hpccg_slab_pack and hpccg_slab_scatter_block (include/hpccg_gpu.h) with the operations of
+    MPI/src/numerics.F90:41-162 and vector_operations.F90:40-169: separately rounded products
+    and sums, row sums in CSR order and dot products in index order, both from 0.0.  With it,
+    DistCG's exchanges and rank-order sums run on gloo ranks without a GPU, and the whole
+    solve must equal the oracle's multi-rank CG bit for bit.  Test infrastructure only."""
+
+    def __init__(self, plan, rowindex, values):
+        info = plan.info()
+        self.nranks, self.mode = plan.nranks, plan.mode
+        self.nrow = len(rowindex) - 1
+        self.ncol = self.nrow + info["num_external"]
+        self.nsend = info["total_to_send"]
+        self.neighbors, self.recv_length = plan.neighbors()
+        if plan.mode == zslab.HALO_MPI:
+            self.send_length, idx = plan.sends()
+            self.send_idx = idx.astype(np.int64) - 1  # elements_to_send, 1-based local rows
+            self.blocks = np.zeros((0, 4), np.int32)
+        else:
+            self.send_length = np.zeros(0, np.int32)
+            self.blocks, remote = plan.blocks()
+            self.remote = remote.astype(np.int64)  # owner-local rows, 1-based
+        # the local CSR as rows padded at their ends with zero terms (which leave a row sum unchanged)
+        cl = plan.colindex_local().astype(np.int64) - 1
+        lens = np.diff(rowindex)
+        w = int(lens.max())
+        self.col = np.zeros((self.nrow, w), np.int64)
+        self.val = np.zeros((self.nrow, w))
+        for i in range(self.nrow):
+            a, e = rowindex[i] - 1, rowindex[i + 1] - 1
+            self.col[i, :e - a], self.val[i, :e - a] = cl[a:e], values[a:e]
+
+    def _spmv(self, x):
+        y = np.zeros(self.nrow)
+        for j in range(self.col.shape[1]):
+            y = y + self.val[:, j] * x[self.col[:, j]]
+        return y
+
+    @staticmethod
+    def _dot(a, b):
+        return float(np.add.accumulate(np.concatenate(([0.0], a * b)))[-1])
+
+    def pack(self, d_x, d_sendbuf):
+        d_sendbuf.numpy()[:self.nsend] = d_x.numpy()[self.send_idx]
+
+    def scatter_block(self, block, d_range, d_x):
+        _owner, first, inmin, _inmax = (int(v) for v in self.blocks[block])
+        end = int(self.blocks[block + 1][1]) if block + 1 < len(self.blocks) else self.ncol - self.nrow + 1
+        d_x.numpy()[self.nrow + first - 1:self.nrow + end - 1] = d_range.numpy()[self.remote[first - 1:end - 1] - inmin]
+
+    def step(self, step, k, d_b, d_x, d_p, d_r, d_Ap, d_state, d_hist=None):
+        st, x, p, r, Ap = d_state.numpy(), d_x.numpy(), d_p.numpy(), d_r.numpy(), d_Ap.numpy()
+        h = d_hist.numpy() if d_hist is not None else None
+        n = self.nrow
+        L, G, RT, NR, BE, DN, TL = (zslab.LOCAL, zslab.GLOBAL, zslab.RTRANS, zslab.NORMR, zslab.BETA, zslab.DONE,
+                                    zslab.TOL)
+        if step == zslab.START:
+            p[:n] = x
+        elif step == zslab.PREPARE:  # Ap = A p, r = 1 b + (-1) Ap (:96), local r.r
+            Ap[:] = self._spmv(p)
+            r[:] = 1.0 * d_b.numpy() + (-1.0) * Ap
+            st[L] = self._dot(r, r)
+        elif step == zslab.PREPARED:
+            st[RT] = st[G]
+            st[NR] = np.sqrt(st[RT])
+            st[DN] = 0.0
+            if h is not None:
+                h[0] = st[NR]
+        elif step == zslab.BEGIN:  # stop test on the previous normr; p = r, or beta and p = r + beta p
+            if st[DN] != 0.0:
+                return
+            if st[NR] < st[TL]:
+                st[DN] = 1.0
+                return
+            beta, rtrans = 0.0, st[RT]
+            if k > 1:
+                rtrans = st[G]
+                beta = rtrans / st[RT]
+            p[:n] = r if k == 1 else r + beta * p[:n]
+            st[BE] = beta
+            if h is not None:
+                h[k] = np.sqrt(rtrans)
+            if k > 1:
+                st[RT] = st[G]
+            st[NR] = np.sqrt(st[RT])
+        elif step == zslab.SPMV:
+            if st[DN] == 0.0:
+                Ap[:] = self._spmv(p)
+                st[L] = self._dot(p[:n], Ap)
+        elif step == zslab.UPDATE:  # alpha = rtrans / p.Ap; r -= alpha Ap; x += alpha p; local r.r
+            if st[DN] == 0.0:
+                alpha = st[RT] / st[G]
+                r[:] = r + (-alpha) * Ap
+                x[:] = x + alpha * p[:n]
+                st[L] = self._dot(r, r)
+
+
+def _dist_cg_main(rank, P, port, nx, ny, nz, mode, max_iter, tol, out_dir):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=P,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        rows, cols, vals, x, b, _ = zslab.generate_matrix_rank(nx, ny, nz, rank, P)
+        plan = zslab.SlabPlan(rows, cols, P, rank, zslab.first_rows_equal(nx * ny * nz, P), mode)
+        ranges = zslab.exchange_plans_dist(plan)
+        cg = zslab.DistCG(HostSlab(plan, rows, vals), plan, get_ranges=ranges, device="cpu")
+        d_b, d_x = torch.from_numpy(b.copy()), torch.zeros(len(b), dtype=torch.float64)
+        it, nr, h = cg.solve(d_b, d_x, max_iter, tol)
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), x=d_x.numpy(), it=it, nr=nr, h=h)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("mode", [zslab.HALO_MPI, zslab.HALO_GET])
+@pytest.mark.parametrize("nx,ny,nz,P,max_iter,tol", [(4, 3, 2, 2, 40, 0.0), (3, 4, 2, 3, 40, 0.0),
+                                                     (5, 3, 2, 3, 150, 1e-6)])
+def test_dist_cg_transport_over_gloo_ranks(tmp_path, nx, ny, nz, P, max_iter, tol, mode):
+    """DistCG (one rank per process, halos by point-to-point messages, dot products by an
+    all-gather folded in rank order) on gloo ranks, every rank's CG steps in host memory:
+    the iterates, iteration count, final normr and residual history equal the oracle's
+    multi-rank CG exactly, in the MPI and the CAF-V2 halo form, with tolerance 0 and with a
+    tolerance that stops the loop early."""
+    mp.start_processes(_dist_cg_main, args=(P, _free_port(), nx, ny, nz, mode, max_iter, tol, str(tmp_path)),
+                       nprocs=P, join=True, start_method="spawn")
+    _, x0, bg, _ = oracle.generate_matrix(nx, ny, nz * P)
+    rx, rit, rnr, rh = oracle.SlabPlan(nx, ny, nz, P, mode).cg(bg, x0, max_iter, tol)
+    if tol > 0:
+        assert rit < max_iter  # the tolerance ends the loop
+    res = [np.load(tmp_path / f"rank{r}.npz") for r in range(P)]
+    for r in res:
+        assert int(r["it"]) == rit and float(r["nr"]) == rnr
+        np.testing.assert_array_equal(r["h"], rh)
+    np.testing.assert_array_equal(np.concatenate([r["x"] for r in res]), rx)
