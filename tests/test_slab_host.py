@@ -295,13 +295,13 @@ class HostSlab:
                 st[L] = self._dot(r, r)
 
 
-def _dist_cg_main(rank, P, port, nx, ny, nz, mode, max_iter, tol, out_dir):
+def _dist_cg_main(rank, P, rdv, nx, ny, nz, mode, max_iter, tol, out_dir):
     import datetime
 
     import torch
     import torch.distributed as dist
 
-    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=P,
+    dist.init_process_group("gloo", init_method=f"file://{rdv}", rank=rank, world_size=P,
                             timeout=datetime.timedelta(seconds=60))
     try:
         rows, cols, vals, x, b, _ = zslab.generate_matrix_rank(nx, ny, nz, rank, P)
@@ -324,7 +324,7 @@ def test_dist_cg_transport_over_gloo_ranks(tmp_path, nx, ny, nz, P, max_iter, to
     the iterates, iteration count, final normr and residual history equal the oracle's
     multi-rank CG exactly, in the MPI and the CAF-V2 halo form, with tolerance 0 and with a
     tolerance that stops the loop early."""
-    mp.start_processes(_dist_cg_main, args=(P, _free_port(), nx, ny, nz, mode, max_iter, tol, str(tmp_path)),
+    mp.start_processes(_dist_cg_main, args=(P, str(tmp_path / "rdv"), nx, ny, nz, mode, max_iter, tol, str(tmp_path)),
                        nprocs=P, join=True, start_method="spawn")
     _, x0, bg, _ = oracle.generate_matrix(nx, ny, nz * P)
     rx, rit, rnr, rh = oracle.SlabPlan(nx, ny, nz, P, mode).cg(bg, x0, max_iter, tol)
@@ -335,3 +335,75 @@ def test_dist_cg_transport_over_gloo_ranks(tmp_path, nx, ny, nz, P, max_iter, to
         assert int(r["it"]) == rit and float(r["nr"]) == rnr
         np.testing.assert_array_equal(r["h"], rh)
     np.testing.assert_array_equal(np.concatenate([r["x"] for r in res]), rx)
+
+
+# ---- a rank that leaves between steps --------------------------------------------
+
+class _LeftEarly(Exception):
+    pass
+
+
+def _dist_cg_leaver_main(rank, P, rdv, how, out_dir):
+    import datetime
+    import json
+    import time
+
+    import torch
+    import torch.distributed as dist
+
+    timeout_s = 5
+    dist.init_process_group("gloo", init_method=f"file://{rdv}", rank=rank, world_size=P,
+                            timeout=datetime.timedelta(seconds=timeout_s))
+    nx, ny, nz = 4, 3, 2
+    rows, cols, vals, x, b, _ = zslab.generate_matrix_rank(nx, ny, nz, rank, P)
+    plan = zslab.SlabPlan(rows, cols, P, rank, zslab.first_rows_equal(nx * ny * nz, P), zslab.HALO_MPI)
+    ranges = zslab.exchange_plans_dist(plan)
+    slab = HostSlab(plan, rows, vals)
+    if rank == P - 1:  # the last rank leaves at the top of iteration 3, between two steps
+        inner = slab.step
+
+        def step(s, k, *a, **kw):
+            if s == zslab.BEGIN and k == 3:
+                raise _LeftEarly()
+            return inner(s, k, *a, **kw)
+
+        slab.step = step
+    cg = zslab.DistCG(slab, plan, get_ranges=ranges, device="cpu")
+    d_b, d_x = torch.from_numpy(b.copy()), torch.zeros(len(b), dtype=torch.float64)
+    t0, status = time.time(), "finished"
+    try:
+        cg.solve(d_b, d_x, 40, 0.0)
+    except _LeftEarly:
+        status = "left"
+        if how == "stay":  # alive, but takes no further part until the others' timeout has passed
+            time.sleep(timeout_s + 2)
+    except RuntimeError as e:
+        status = "error: " + str(e)[:200]
+    with open(os.path.join(out_dir, f"rank{rank}.json"), "w") as f:
+        json.dump({"status": status, "seconds": time.time() - t0}, f)
+    if status != "left" or how == "exit":
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("how", ["exit", "stay"])
+def test_dist_cg_rank_leaving_between_steps_raises_on_the_others(tmp_path, how):
+    """Failure detection on the host: one of three gloo ranks leaves DistCG at the top of
+    iteration 3, between two steps, and either exits or stays alive without taking part.  The
+    other ranks (its z neighbour and the rank beyond it) get an error from their next transfer
+    -- at once when the peer's connection closes; when it stays silent, the first of them to
+    give up does so on the process group's 5 s timeout, and the rest then on that timeout or
+    on the closed connection of the rank that gave up -- instead of waiting for ever."""
+    import json
+
+    P = 3
+    mp.start_processes(_dist_cg_leaver_main, args=(P, str(tmp_path / "rdv"), how, str(tmp_path)), nprocs=P, join=True,
+                       start_method="spawn")
+    res = [json.load(open(tmp_path / f"rank{r}.json")) for r in range(P)]
+    assert res[P - 1]["status"] == "left"
+    for r in res[:P - 1]:
+        assert r["status"].startswith("error"), r
+        assert r["seconds"] < 5 + 20, r
+        if how == "stay":
+            assert r["seconds"] >= 4.5, r
+    if how == "stay":
+        assert any("Timed out" in r["status"] for r in res[:P - 1]), res
