@@ -590,7 +590,8 @@ def run_ours(args):
         fms = learned_info["unet_forward_ms"]
         _, bf16_sust, bf16_kind = _bf16_sustained()
         conv = {"bound": "tensor", "kernel": "U-Net forward pass (k_conv3_row tcgen05 convolutions, BF16 in, "
-                "FP32 accumulate; plus the CUDA-core input layer, pooling and upsampling)",
+                "FP32 accumulate; the 1-channel input layer on tcgen05 too when nx % 128 == 0 "
+                "(k_conv3_in1_tc), else on CUDA cores; pooling and upsampling)",
                 "kernel_ms": fms, "flop_per_launch": flop, "achieved": flop / (fms * 1e-3) / 1e12,
                 "peak": bf16_sust, "unit": "TFLOP/s", "peak_source": bf16_kind, "traffic": None}
         conv["frac"] = conv["achieved"] / bf16_sust
