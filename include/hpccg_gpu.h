@@ -66,6 +66,8 @@ int hpccg_gpu_create(int32_t nrow, int64_t nnz, const int32_t *rowindex,
 int hpccg_gpu_create_generated(int32_t nx, int32_t ny, int32_t nz, double *d_x, double *d_b,
                                double *d_xexact, hpccg_ctx **ctx);
 
+/* Frees the context: its matrix copies, vectors, graphs, events and stream.
+ * NULL is ignored. */
 void hpccg_gpu_destroy(hpccg_ctx *ctx);
 
 /* Basic facts about the context: rows, stored nonzeros, ELL width. */
