@@ -317,10 +317,10 @@ def _dist_cg_main(rank, P, rdv, nx, ny, nz, mode, max_iter, tol, out_dir):
 
 @pytest.mark.parametrize("mode", [zslab.HALO_MPI, zslab.HALO_GET])
 @pytest.mark.parametrize("nx,ny,nz,P,max_iter,tol", [(4, 3, 2, 2, 40, 0.0), (3, 4, 2, 3, 40, 0.0),
-                                                     (5, 3, 2, 3, 150, 1e-6)])
+                                                     (3, 3, 1, 4, 40, 0.0), (5, 3, 2, 3, 150, 1e-6)])
 def test_dist_cg_transport_over_gloo_ranks(tmp_path, nx, ny, nz, P, max_iter, tol, mode):
     """DistCG (one rank per process, halos by point-to-point messages, dot products by an
-    all-gather folded in rank order) on gloo ranks, every rank's CG steps in host memory:
+    all-gather folded in rank order) on 2-4 gloo ranks (one-plane slabs among them), every rank's CG steps in host memory:
     the iterates, iteration count, final normr and residual history equal the oracle's
     multi-rank CG exactly, in the MPI and the CAF-V2 halo form, with tolerance 0 and with a
     tolerance that stops the loop early."""
